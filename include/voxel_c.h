@@ -1,0 +1,285 @@
+/*
+ * voxel_c.h - C ABI of the VoxelVM B200 backend (libvoxel_c.so).
+ *
+ * Drop-in replacement for the reference's bindings/voxel_c.h: every symbol the
+ * reference exports is declared here with the same signature (the comment
+ * gives the reference line it replaces), so existing callers (the Go cgo
+ * wrapper, the Java FFM wrapper, c_test.cpp) link unchanged.  Data work runs on
+ * the GPU; there is no CPU path, and calls that cannot run fail loudly through
+ * voxel_last_error().
+ *
+ * Additive symbols follow.  They never change a reference signature:
+ *   - engines for f32 / i32 / u32 / u64 columns, named like the _i64 set;
+ *   - status-returning variants (return 0 on success, a VOXEL_E* code otherwise);
+ *   - operator entry points for the hot path with host buffers, and "_dev"
+ *     variants that take device pointers and a cudaStream_t (as void*).
+ *
+ * Element-type codes: 0 f64, 1 f32, 2 i64, 3 i32, 4 u64, 5 u32.
+ * Comparison codes:   0 EQ, 1 NE, 2 LT, 3 LE, 4 GT, 5 GE, 6 BETWEEN.
+ */
+#pragma once
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define VOXEL_OK 0
+#define VOXEL_EINVAL 1
+#define VOXEL_EUNSUPPORTED 2
+#define VOXEL_ENONTERMINATING 3
+#define VOXEL_ECUDA 4
+#define VOXEL_ENOMEM 5
+#define VOXEL_ETIMEOUT 6
+#define VOXEL_EOVERFLOW 7
+#define VOXEL_ENODEVICE 8
+#define VOXEL_ECAPACITY 9
+
+/* ================================================================
+ * Engine (f64) - reference bindings/voxel_c.h:14-24
+ * ================================================================ */
+void*     voxel_engine_create_f64(void);                                             /* voxel_c.h:14 */
+void      voxel_engine_destroy(void* engine);                                        /* voxel_c.h:15 */
+size_t    voxel_engine_add_segment(void* engine, const double* data, size_t count);  /* voxel_c.h:16 */
+void      voxel_engine_load_program(void* engine, const uint32_t* code, size_t len); /* voxel_c.h:17 */
+void      voxel_engine_run(void* engine);                                            /* voxel_c.h:18 */
+void      voxel_engine_run_parallel(void* engine, size_t seg_id, uint32_t threads,
+                                    uint8_t result_reg);                             /* voxel_c.h:19 */
+void      voxel_engine_set_scalar(void* engine, size_t reg, uint64_t value);         /* voxel_c.h:20 */
+uint64_t  voxel_engine_get_scalar(void* engine, size_t reg);                         /* voxel_c.h:21 */
+void      voxel_engine_set_scalar_f64(void* engine, size_t reg, double value);       /* voxel_c.h:22 */
+double    voxel_engine_get_scalar_f64(void* engine, size_t reg);                     /* voxel_c.h:23 */
+size_t    voxel_engine_k_lanes(void);                                                /* voxel_c.h:24 */
+
+/* ================================================================
+ * Engine (i64) - reference bindings/voxel_c.h:29-35
+ * ================================================================ */
+void*     voxel_engine_create_i64(void);                                                 /* voxel_c.h:29 */
+void      voxel_engine_destroy_i64(void* engine);                                        /* voxel_c.h:30 */
+size_t    voxel_engine_add_segment_i64(void* engine, const int64_t* data, size_t count); /* voxel_c.h:31 */
+void      voxel_engine_load_program_i64(void* engine, const uint32_t* code, size_t len); /* voxel_c.h:32 */
+void      voxel_engine_run_i64(void* engine);                                            /* voxel_c.h:33 */
+void      voxel_engine_set_scalar_i64(void* engine, size_t reg, uint64_t value);         /* voxel_c.h:34 */
+uint64_t  voxel_engine_get_scalar_i64(void* engine, size_t reg);                         /* voxel_c.h:35 */
+
+/* ================================================================
+ * JIT - reference bindings/voxel_c.h:40-41 (fused filter+sum over one f64
+ * column with R0=0, R1=0, R2=data_len, R3=threshold; returns R0).
+ * ================================================================ */
+double    voxel_jit_run(const uint32_t* code, size_t code_len,
+                        const double* data, size_t data_len, double threshold);      /* voxel_c.h:40 */
+
+/* ================================================================
+ * Instruction encoding - reference bindings/voxel_c.h:46-65
+ * ================================================================ */
+uint32_t  voxel_instr_vload(uint8_t vd, uint8_t ra, uint8_t seg_id, uint8_t count);  /* voxel_c.h:46 */
+uint32_t  voxel_instr_vfilter_gt(uint8_t vd, uint8_t va, uint8_t rb);                /* voxel_c.h:47 */
+uint32_t  voxel_instr_vfilter_ge(uint8_t vd, uint8_t va, uint8_t rb);                /* voxel_c.h:48 */
+uint32_t  voxel_instr_vfilter_lt(uint8_t vd, uint8_t va, uint8_t rb);                /* voxel_c.h:49 */
+uint32_t  voxel_instr_vfilter_le(uint8_t vd, uint8_t va, uint8_t rb);                /* voxel_c.h:50 */
+uint32_t  voxel_instr_vsum(uint8_t rd, uint8_t va);                                  /* voxel_c.h:51 */
+uint32_t  voxel_instr_vred_min(uint8_t rd, uint8_t va);                              /* voxel_c.h:52 */
+uint32_t  voxel_instr_vred_max(uint8_t rd, uint8_t va);                              /* voxel_c.h:53 */
+uint32_t  voxel_instr_vcount(uint8_t rd, uint8_t va);                                /* voxel_c.h:54 */
+uint32_t  voxel_instr_addf(uint8_t rd, uint8_t ra, uint8_t rb);                      /* voxel_c.h:55 */
+uint32_t  voxel_instr_add(uint8_t rd, uint8_t ra, uint8_t rb);                       /* voxel_c.h:56 */
+uint32_t  voxel_instr_sub(uint8_t rd, uint8_t ra, uint8_t rb);                       /* voxel_c.h:57 */
+uint32_t  voxel_instr_mul(uint8_t rd, uint8_t ra, uint8_t rb);                       /* voxel_c.h:58 */
+uint32_t  voxel_instr_mov(uint8_t rd, int16_t imm);                                  /* voxel_c.h:59 */
+uint32_t  voxel_instr_movr(uint8_t rd, uint8_t ra);                                  /* voxel_c.h:60 */
+uint32_t  voxel_instr_cmp(uint8_t ra, uint8_t rb);                                   /* voxel_c.h:61 */
+uint32_t  voxel_instr_jnz(int16_t offset);                                           /* voxel_c.h:62 */
+uint32_t  voxel_instr_jz(int16_t offset);                                            /* voxel_c.h:63 */
+uint32_t  voxel_instr_jmp(int16_t offset);                                           /* voxel_c.h:64 */
+uint32_t  voxel_instr_halt(void);                                                    /* voxel_c.h:65 */
+
+/* ================================================================
+ * NullBitmap - reference bindings/voxel_c.h:70-76 (1 = null)
+ * ================================================================ */
+void*     voxel_null_create(size_t count);                      /* voxel_c.h:70 */
+void      voxel_null_destroy(void* bitmap);                     /* voxel_c.h:71 */
+int       voxel_null_is_null(const void* bitmap, size_t row);   /* voxel_c.h:72 */
+void      voxel_null_set_null(void* bitmap, size_t row);        /* voxel_c.h:73 */
+void      voxel_null_set_valid(void* bitmap, size_t row);       /* voxel_c.h:74 */
+size_t    voxel_null_null_count(const void* bitmap);            /* voxel_c.h:75 */
+size_t    voxel_null_valid_count(const void* bitmap);           /* voxel_c.h:76 */
+
+/* ================================================================
+ * HashAggregator<u32,f64> - reference bindings/voxel_c.h:81-85
+ * ================================================================ */
+void*     voxel_agg_create(void);                                                       /* voxel_c.h:81 */
+void      voxel_agg_destroy(void* agg);                                                 /* voxel_c.h:82 */
+void      voxel_agg_init(void* agg, size_t expected_groups);                            /* voxel_c.h:83 */
+void      voxel_agg_accumulate(void* agg, const uint32_t* keys, const double* values,
+                               size_t count);                                           /* voxel_c.h:84 */
+size_t    voxel_agg_group_count(const void* agg);                                       /* voxel_c.h:85 */
+
+/* ================================================================
+ * Sort & TopK - reference bindings/voxel_c.h:90-92
+ * ================================================================ */
+void      voxel_sort_ascending(const double* data, size_t count, uint32_t* indices_out);  /* voxel_c.h:90 */
+void      voxel_sort_descending(const double* data, size_t count, uint32_t* indices_out); /* voxel_c.h:91 */
+void      voxel_topk(const double* data, size_t count, size_t k, double* out, int largest);/* voxel_c.h:92 */
+
+/* ================================================================
+ * DictionaryEncoding<f64> - reference bindings/voxel_c.h:97-101
+ * ================================================================ */
+void*     voxel_dict_create(void);                                                    /* voxel_c.h:97 */
+void      voxel_dict_destroy(void* dict);                                             /* voxel_c.h:98 */
+void      voxel_dict_build(void* dict, const double* data, size_t count);             /* voxel_c.h:99 */
+size_t    voxel_dict_cardinality(const void* dict);                                   /* voxel_c.h:100 */
+void      voxel_dict_decode_batch(void* dict, double* out, size_t offset, size_t count); /* voxel_c.h:101 */
+
+/* ================================================================
+ * ThreadPool - reference bindings/voxel_c.h:106-109 (host worker pool)
+ * ================================================================ */
+void*     voxel_pool_create(uint32_t threads);           /* voxel_c.h:106 */
+void      voxel_pool_destroy(void* pool);                /* voxel_c.h:107 */
+void      voxel_pool_wait_all(void* pool);               /* voxel_c.h:108 */
+size_t    voxel_pool_thread_count(const void* pool);     /* voxel_c.h:109 */
+
+/* ================================================================
+ * Error handling - reference bindings/voxel_c.h:114.  Unlike the reference
+ * (whose buffer is never written, voxel_c.cpp:7,227) this returns the calling
+ * thread's last failure message, or "" after a success.
+ * ================================================================ */
+const char* voxel_last_error(void);                      /* voxel_c.h:114 */
+
+/* ================================================================
+ * Additive: engines for the other column types (north-star EngineF32/I32/
+ * U32/U64), following the _i64 naming.  voxel_engine_destroy accepts any
+ * engine handle.  f32 engines keep scalar registers as f64 values.
+ * ================================================================ */
+void*     voxel_engine_create(int dtype);
+int       voxel_engine_dtype(const void* engine);
+size_t    voxel_engine_k_lanes_of(const void* engine);
+void*     voxel_engine_create_f32(void);
+void*     voxel_engine_create_i32(void);
+void*     voxel_engine_create_u32(void);
+void*     voxel_engine_create_u64(void);
+size_t    voxel_engine_add_segment_f32(void* engine, const float* data, size_t count);
+size_t    voxel_engine_add_segment_i32(void* engine, const int32_t* data, size_t count);
+size_t    voxel_engine_add_segment_u32(void* engine, const uint32_t* data, size_t count);
+size_t    voxel_engine_add_segment_u64(void* engine, const uint64_t* data, size_t count);
+/* a column already resident in device memory (not copied; must outlive runs) */
+size_t    voxel_engine_add_segment_device(void* engine, const void* device_data, size_t count);
+int       voxel_engine_run_status(void* engine);
+int       voxel_engine_run_parallel_status(void* engine, size_t seg_id, uint32_t threads,
+                                           uint8_t result_reg);
+/* the schedule the last run executed, as text (for diagnostics and tests) */
+size_t    voxel_engine_explain(void* engine, char* buf, size_t cap);
+/* lower the loaded program without running it (no device needed); the
+ * schedules are then available from voxel_engine_explain */
+int       voxel_engine_plan(void* engine);
+void      voxel_engine_reset(void* engine);
+/* milliseconds of device time of the last run's kernels (CUDA events) */
+double    voxel_engine_last_device_ms(const void* engine);
+int       voxel_last_status(void);
+
+/* ================================================================
+ * Additive: VectorFilter / ColumnFilter / SelectionVector on the GPU
+ * (reference include/voxel/ops/filter.hpp:42-399).  Host buffers.
+ * ================================================================ */
+/* bitmap: ceil(n/64) words, bit i&63 of word i>>6 set iff row i passes.
+ * Returns PassCount, or (size_t)-1 on failure. */
+size_t    voxel_vfilter(int dtype, int op, const void* data, size_t n, uint64_t lo_bits,
+                        uint64_t hi_bits, uint64_t* bitmap);
+size_t    voxel_bitmap_and(const uint64_t* const* bitmaps, size_t nbitmaps, size_t rows,
+                           uint64_t* out);
+size_t    voxel_selection_from_bitmap(const uint64_t* bitmap, size_t rows, uint32_t* out);
+/* device variants (stream may be NULL for the calling thread's stream) */
+int       voxel_vfilter_dev(int dtype, int op, const void* d_data, size_t n, uint64_t lo_bits,
+                            uint64_t hi_bits, uint64_t* d_bitmap, uint64_t* d_count, void* stream);
+int       voxel_selection_from_bitmap_dev(const uint64_t* d_bitmap, size_t rows, uint32_t* d_out,
+                                          uint64_t* d_count, void* stream);
+
+/* ================================================================
+ * Additive: decoders (reference include/voxel/data/encoding.hpp)
+ * ================================================================ */
+/* BitPackedEncoding::DecodeBatch (encoding.hpp:397-422) */
+int       voxel_bitpack_decode(const uint64_t* words, size_t nwords, uint32_t width,
+                               size_t value_count, size_t offset, size_t count, uint32_t* out);
+/* DictionaryEncoding<i32>::DecodeBatch over packed indices: out[i] = dict[unpack(i)] */
+int       voxel_dict_bitpack_decode_i32(const uint64_t* words, size_t nwords, uint32_t width,
+                                        const int32_t* dict, size_t card, size_t value_count,
+                                        size_t offset, size_t count, int32_t* out);
+/* DictionaryEncoding<T>::DecodeBatch (encoding.hpp:156-167), dtype 0 or 3 */
+int       voxel_dict_decode(int dtype, const void* dict, size_t card, const uint32_t* indices,
+                            size_t n, size_t offset, size_t count, void* out);
+/* RLEEncoding<i64>::DecodeBatch (encoding.hpp:231-257) */
+int       voxel_rle_decode_i64(const int64_t* values, const uint32_t* runs, size_t nruns,
+                               size_t offset, size_t count, int64_t* out);
+int       voxel_bitpack_decode_dev(const uint64_t* d_words, size_t nwords, uint32_t width,
+                                   size_t value_count, size_t offset, size_t count, uint32_t* d_out,
+                                   void* stream);
+int       voxel_rle_decode_i64_dev(const int64_t* d_values, const uint32_t* d_runs, size_t nruns,
+                                   size_t offset, size_t count, int64_t* d_out, void* stream);
+
+/* ================================================================
+ * Additive: fused scan + group-by (decode key, two predicates, group SUM of a
+ * product, COUNT, MIN, MAX).  Groups come out sorted by key; returns the
+ * group count or (size_t)-1.
+ *   key = dict[unpack(packed_key)], WHERE price > price_gt AND
+ *   qty BETWEEN qty_lo AND qty_hi, GROUP BY key:
+ *   SUM(price*qty) (one rounded multiply), COUNT(*), MIN(price), MAX(price)
+ * ================================================================ */
+size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t width,
+                             const int32_t* dict, size_t card, const double* price,
+                             const int32_t* qty, size_t n, double price_gt, int32_t qty_lo,
+                             int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
+                             double* out_max, uint64_t* out_count);
+int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,
+                                 const int32_t* d_dict, size_t card, const double* d_price,
+                                 const int32_t* d_qty, size_t n, double price_gt, int32_t qty_lo,
+                                 int32_t qty_hi, int32_t* d_keys, double* d_sum, double* d_min,
+                                 double* d_max, uint64_t* d_count, uint64_t* d_ngroups,
+                                 void* stream);
+
+/* ================================================================
+ * Additive: GROUP BY over explicit keys (HashAggregator semantics,
+ * aggregate.hpp:159-301): per key SUM (compensated f64), MIN, MAX, COUNT,
+ * groups sorted by key.  Returns the group count or (size_t)-1.
+ * ================================================================ */
+size_t    voxel_groupby_i32_f64(const int32_t* keys, const double* values, size_t n,
+                                size_t expected_groups, int32_t* out_keys, double* out_sum,
+                                double* out_min, double* out_max, uint64_t* out_count);
+size_t    voxel_groupby_u32_f64(const uint32_t* keys, const double* values, size_t n,
+                                size_t expected_groups, uint32_t* out_keys, double* out_sum,
+                                double* out_min, double* out_max, uint64_t* out_count);
+/* GroupedAggregator over pre-sorted keys (aggregate.hpp:665-706) */
+size_t    voxel_grouped_sorted_i32_f64(const int32_t* sorted_keys, const double* values,
+                                       size_t n, int32_t* out_keys, double* out_sum,
+                                       double* out_min, double* out_max, uint64_t* out_count);
+
+/* ================================================================
+ * Additive: stable LSD radix sort of keys with a u32 payload
+ * (RadixSort<T>::Sort, sort.hpp:83-160).  keys and idx are sorted in place.
+ * dtype in {2 i64, 3 i32, 4 u64, 5 u32}.
+ * ================================================================ */
+int       voxel_radix_sort(int dtype, void* keys, uint32_t* idx, size_t n);
+int       voxel_radix_sort_dev(int dtype, void* d_keys, uint32_t* d_idx, size_t n,
+                               void* d_tmp, size_t tmp_bytes, void* stream);
+size_t    voxel_radix_sort_tmp_bytes(int dtype, size_t n);
+
+/* ================================================================
+ * Additive: hash join on i64 keys (HashJoin<TKey>, join.hpp:36-165).
+ * Pairs (probe_idx, build_idx) in ascending probe order; for equal build
+ * keys the newest build row comes first (the reference's LIFO chains).
+ * all=0 keeps the first match only (Probe), all=1 every match
+ * (ProbeAllMatches).  Returns the pair count or (size_t)-1.
+ * ================================================================ */
+size_t    voxel_hashjoin_i64(const int64_t* build, size_t nb, const int64_t* probe, size_t np,
+                             uint32_t* left, uint32_t* right, size_t max_matches, int all);
+/* count + u64 SUM(build payload) + pairs, device pointers */
+int       voxel_hashjoin_i64_dev(const int64_t* d_build, const uint64_t* d_payload, size_t nb,
+                                 const int64_t* d_probe, size_t np, uint32_t* d_left,
+                                 uint32_t* d_right, size_t max_matches, int all,
+                                 uint64_t* d_count_sum, void* stream);
+
+#ifdef __cplusplus
+}
+#endif

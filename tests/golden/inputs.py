@@ -1,0 +1,137 @@
+"""Deterministic input generators shared by the golden-vector script and tests.
+
+All generators use numpy's PCG64 (stable across numpy versions for the calls
+used here), except mt_uniform, which reproduces the reference's own
+std::mt19937_64 + uniform_real_distribution column (examples/validate.cpp:22-25)
+through the backend's C++ data generator.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from voxel_b200 import templates as T  # noqa: E402
+
+
+def column(dtype: int, n: int, seed: int) -> np.ndarray:
+    return T.make_column(dtype, n, np.random.default_rng(seed))
+
+
+def mt_uniform(seed: int, n: int, lo: float = 0.0, hi: float = 1000.0) -> np.ndarray:
+    from voxel_b200 import capi
+
+    x = np.empty(n, np.float64)
+    capi.datagen().vgen_uniform_f64_mt(seed, n, lo, hi, x.ctypes.data)
+    return x
+
+
+def bitmap(n: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    words = max((n + 63) // 64, 1)
+    bm = rng.integers(0, 2**63, size=words, dtype=np.int64).astype(np.uint64)
+    bm ^= rng.integers(0, 2, size=words, dtype=np.int64).astype(np.uint64) << np.uint64(63)
+    if n % 64:
+        bm[-1] &= np.uint64((1 << (n % 64)) - 1)
+    if n == 0:
+        bm[:] = 0
+    return bm
+
+
+def u32_values(n: int, maxv: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    v = rng.integers(0, maxv, size=n, dtype=np.int64).astype(np.uint32)
+    if n:
+        v[0] = np.uint32(maxv - 1)
+    return v
+
+
+def i32_values(n: int, card: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    pool = rng.integers(-(2**31), 2**31, size=card, dtype=np.int64).astype(np.int32)
+    return pool[rng.integers(0, card, size=n)]
+
+
+def rle_i64(n: int, seed: int) -> np.ndarray:
+    """Strictly increasing run values, runs of 1..64 (the ts column's shape)."""
+    rng = np.random.default_rng(seed)
+    out = np.empty(n, np.int64)
+    i, v = 0, int(rng.integers(0, 1000))
+    while i < n:
+        r = int(rng.integers(1, 65))
+        out[i:i + r] = v
+        i += r
+        v += int(rng.integers(1, 6))
+    return out
+
+
+def group_input(n: int, card: int, seed: int):
+    rng = np.random.default_rng(seed)
+    keys = rng.integers(0, card, size=n).astype(np.int32) * 7 - 100
+    vals = rng.random(n) * 100.0
+    return keys, vals
+
+
+def sort_keys(dtype: int, n: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    if dtype == T.U64:
+        k = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64) * np.uint64(2)
+        k += rng.integers(0, 2, size=n, dtype=np.int64).astype(np.uint64)
+        if n > 4:
+            k[: n // 4] = k[n // 2: n // 2 + n // 4]  # duplicates exercise stability
+        return k
+    if dtype == T.U32:
+        k = rng.integers(0, 2**32, size=n, dtype=np.int64).astype(np.uint32)
+    elif dtype == T.I64:
+        k = rng.integers(-(2**62), 2**62, size=n, dtype=np.int64)
+    else:
+        k = rng.integers(-(2**31), 2**31, size=n, dtype=np.int64).astype(np.int32)
+    if n > 4:
+        k[: n // 4] = k[n // 2: n // 2 + n // 4]
+    return k
+
+
+def join_input(nb: int, np_: int, dup: bool, seed: int):
+    rng = np.random.default_rng(seed)
+    if dup:
+        pool = rng.integers(-(2**40), 2**40, size=max(nb // 4, 1), dtype=np.int64)
+        b = pool[rng.integers(0, pool.size, size=nb)]
+    else:
+        b = rng.permutation(rng.integers(-(2**40), 2**40, size=nb * 2, dtype=np.int64))
+        b = np.unique(b)[:nb]
+        b = rng.permutation(b)
+    hit = rng.random(np_) < 0.9
+    p = np.where(hit, b[rng.integers(0, b.size, size=np_)], rng.integers(2**41, 2**42, size=np_, dtype=np.int64))
+    return b.astype(np.int64), p.astype(np.int64)
+
+
+def zipf_alias_keys(n: int, card: int, s: float, rng: np.random.Generator) -> np.ndarray:
+    """Ranks 0..card-1 drawn with P(k) ~ (k+1)^-s (inverse-CDF on the exact pmf)."""
+    w = np.arange(1, card + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w / w.sum())
+    cdf[-1] = 1.0
+    return np.searchsorted(cdf, rng.random(n), side="right").astype(np.int64)
+
+
+def config2(n: int, seed: int, card: int = 1000) -> dict:
+    """The scan + group-by columns: key i32 Zipf(1.1) over `card` values,
+    dictionary-encoded and bit-packed; price LogNormal(3,1); qty U[1,100];
+    ts strictly increasing in runs of 1-64 (RLE)."""
+    from voxel_b200 import encode
+
+    rng = np.random.default_rng(seed)
+    values = np.sort(rng.choice(np.arange(-50000, 50000, dtype=np.int64), size=card, replace=False)).astype(np.int32)
+    rank = zipf_alias_keys(n, card, 1.1, rng)
+    perm = rng.permutation(card)
+    key = values[perm[rank]]
+    price = rng.lognormal(3.0, 1.0, n)
+    qty = rng.integers(1, 101, size=n).astype(np.int32)
+    dict_, idx = encode.dict_build_i32(key)
+    width = encode.bit_width(idx)
+    packed = encode.bitpack(idx, width)
+    return dict(n=n, key=key, dict=dict_, idx=idx, width=width, packed=packed, price=price, qty=qty)

@@ -1,0 +1,181 @@
+"""ctypes view of ``include/voxel_c.h`` (the backend's C ABI).
+
+The library is the in-tree ``voxel_b200/lib/libvoxel_c.so``.  Loading fails
+loudly when it has not been built: there is no Python or CPU stand-in.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "lib", "libvoxel_c.so")
+DATAGEN_PATH = os.path.join(HERE, "lib", "libvoxel_datagen.so")
+HEADER = os.path.join(ROOT, "include", "voxel_c.h")
+
+F64, F32, I64, I32, U64, U32 = range(6)
+EQ, NE, LT, LE, GT, GE, BETWEEN = range(7)
+
+_lib = None
+_datagen = None
+
+vp = C.c_void_p
+sz = C.c_size_t
+u8, u32, u64, i16, i32, i64 = C.c_uint8, C.c_uint32, C.c_uint64, C.c_int16, C.c_int32, C.c_int64
+dbl = C.c_double
+P = C.POINTER
+
+_SIGS = {
+    "voxel_engine_create": (vp, [C.c_int]),
+    "voxel_engine_create_f64": (vp, []),
+    "voxel_engine_create_f32": (vp, []),
+    "voxel_engine_create_i64": (vp, []),
+    "voxel_engine_create_i32": (vp, []),
+    "voxel_engine_create_u64": (vp, []),
+    "voxel_engine_create_u32": (vp, []),
+    "voxel_engine_destroy": (None, [vp]),
+    "voxel_engine_destroy_i64": (None, [vp]),
+    "voxel_engine_dtype": (C.c_int, [vp]),
+    "voxel_engine_k_lanes": (sz, []),
+    "voxel_engine_k_lanes_of": (sz, [vp]),
+    "voxel_engine_add_segment": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_i64": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_f32": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_i32": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_u32": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_u64": (sz, [vp, vp, sz]),
+    "voxel_engine_add_segment_device": (sz, [vp, vp, sz]),
+    "voxel_engine_load_program": (None, [vp, vp, sz]),
+    "voxel_engine_load_program_i64": (None, [vp, vp, sz]),
+    "voxel_engine_run": (None, [vp]),
+    "voxel_engine_run_i64": (None, [vp]),
+    "voxel_engine_run_status": (C.c_int, [vp]),
+    "voxel_engine_run_parallel": (None, [vp, sz, u32, u8]),
+    "voxel_engine_run_parallel_status": (C.c_int, [vp, sz, u32, u8]),
+    "voxel_engine_set_scalar": (None, [vp, sz, u64]),
+    "voxel_engine_get_scalar": (u64, [vp, sz]),
+    "voxel_engine_set_scalar_f64": (None, [vp, sz, dbl]),
+    "voxel_engine_get_scalar_f64": (dbl, [vp, sz]),
+    "voxel_engine_set_scalar_i64": (None, [vp, sz, u64]),
+    "voxel_engine_get_scalar_i64": (u64, [vp, sz]),
+    "voxel_engine_explain": (sz, [vp, C.c_char_p, sz]),
+    "voxel_engine_reset": (None, [vp]),
+    "voxel_engine_plan": (C.c_int, [vp]),
+    "voxel_engine_last_device_ms": (dbl, [vp]),
+    "voxel_jit_run": (dbl, [vp, sz, vp, sz, dbl]),
+    "voxel_last_error": (C.c_char_p, []),
+    "voxel_last_status": (C.c_int, []),
+    "voxel_instr_vload": (u32, [u8, u8, u8, u8]),
+    "voxel_instr_vfilter_gt": (u32, [u8, u8, u8]),
+    "voxel_instr_vfilter_ge": (u32, [u8, u8, u8]),
+    "voxel_instr_vfilter_lt": (u32, [u8, u8, u8]),
+    "voxel_instr_vfilter_le": (u32, [u8, u8, u8]),
+    "voxel_instr_vsum": (u32, [u8, u8]),
+    "voxel_instr_vred_min": (u32, [u8, u8]),
+    "voxel_instr_vred_max": (u32, [u8, u8]),
+    "voxel_instr_vcount": (u32, [u8, u8]),
+    "voxel_instr_addf": (u32, [u8, u8, u8]),
+    "voxel_instr_add": (u32, [u8, u8, u8]),
+    "voxel_instr_sub": (u32, [u8, u8, u8]),
+    "voxel_instr_mul": (u32, [u8, u8, u8]),
+    "voxel_instr_mov": (u32, [u8, i16]),
+    "voxel_instr_movr": (u32, [u8, u8]),
+    "voxel_instr_cmp": (u32, [u8, u8]),
+    "voxel_instr_jnz": (u32, [i16]),
+    "voxel_instr_jz": (u32, [i16]),
+    "voxel_instr_jmp": (u32, [i16]),
+    "voxel_instr_halt": (u32, []),
+    "voxel_null_create": (vp, [sz]),
+    "voxel_null_destroy": (None, [vp]),
+    "voxel_null_is_null": (C.c_int, [vp, sz]),
+    "voxel_null_set_null": (None, [vp, sz]),
+    "voxel_null_set_valid": (None, [vp, sz]),
+    "voxel_null_null_count": (sz, [vp]),
+    "voxel_null_valid_count": (sz, [vp]),
+    "voxel_agg_create": (vp, []),
+    "voxel_agg_destroy": (None, [vp]),
+    "voxel_agg_init": (None, [vp, sz]),
+    "voxel_agg_accumulate": (None, [vp, vp, vp, sz]),
+    "voxel_agg_group_count": (sz, [vp]),
+    "voxel_sort_ascending": (None, [vp, sz, vp]),
+    "voxel_sort_descending": (None, [vp, sz, vp]),
+    "voxel_topk": (None, [vp, sz, sz, vp, C.c_int]),
+    "voxel_dict_create": (vp, []),
+    "voxel_dict_destroy": (None, [vp]),
+    "voxel_dict_build": (None, [vp, vp, sz]),
+    "voxel_dict_cardinality": (sz, [vp]),
+    "voxel_dict_decode_batch": (None, [vp, vp, sz, sz]),
+    "voxel_pool_create": (vp, [u32]),
+    "voxel_pool_destroy": (None, [vp]),
+    "voxel_pool_wait_all": (None, [vp]),
+    "voxel_pool_thread_count": (sz, [vp]),
+    "voxel_vfilter": (sz, [C.c_int, C.c_int, vp, sz, u64, u64, vp]),
+    "voxel_bitmap_and": (sz, [vp, sz, sz, vp]),
+    "voxel_selection_from_bitmap": (sz, [vp, sz, vp]),
+    "voxel_vfilter_dev": (C.c_int, [C.c_int, C.c_int, vp, sz, u64, u64, vp, vp, vp]),
+    "voxel_selection_from_bitmap_dev": (C.c_int, [vp, sz, vp, vp, vp]),
+    "voxel_bitpack_decode": (C.c_int, [vp, sz, u32, sz, sz, sz, vp]),
+    "voxel_dict_bitpack_decode_i32": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp]),
+    "voxel_dict_decode": (C.c_int, [C.c_int, vp, sz, vp, sz, sz, sz, vp]),
+    "voxel_rle_decode_i64": (C.c_int, [vp, vp, sz, sz, sz, vp]),
+    "voxel_bitpack_decode_dev": (C.c_int, [vp, sz, u32, sz, sz, sz, vp, vp]),
+    "voxel_rle_decode_i64_dev": (C.c_int, [vp, vp, sz, sz, sz, vp, vp]),
+    "voxel_scan_groupby": (sz, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32, vp, vp, vp, vp, vp]),
+    "voxel_scan_groupby_dev": (C.c_int, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32,
+                                          vp, vp, vp, vp, vp, vp, vp]),
+    "voxel_groupby_i32_f64": (sz, [vp, vp, sz, sz, vp, vp, vp, vp, vp]),
+    "voxel_groupby_u32_f64": (sz, [vp, vp, sz, sz, vp, vp, vp, vp, vp]),
+    "voxel_grouped_sorted_i32_f64": (sz, [vp, vp, sz, vp, vp, vp, vp, vp]),
+    "voxel_radix_sort": (C.c_int, [C.c_int, vp, vp, sz]),
+    "voxel_radix_sort_dev": (C.c_int, [C.c_int, vp, vp, sz, vp, sz, vp]),
+    "voxel_radix_sort_tmp_bytes": (sz, [C.c_int, sz]),
+    "voxel_hashjoin_i64": (sz, [vp, sz, vp, sz, vp, vp, sz, C.c_int]),
+    "voxel_hashjoin_i64_dev": (C.c_int, [vp, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
+}
+
+
+def header_symbols() -> list[str]:
+    """Every function name declared in include/voxel_c.h."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(voxel_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> C.CDLL:
+    """The loaded backend library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"voxel_b200 native library not built ({LIB_PATH}); run __graft_entry__.build()")
+        _lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(_lib, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def datagen() -> C.CDLL:
+    global _datagen
+    if _datagen is None:
+        _datagen = C.CDLL(DATAGEN_PATH)
+        _datagen.vgen_uniform_f64_mt.restype = None
+        _datagen.vgen_uniform_f64_mt.argtypes = [u64, sz, dbl, dbl, vp]
+    return _datagen
+
+
+def last_error() -> str:
+    msg = lib().voxel_last_error()
+    return msg.decode() if msg else ""
+
+
+def ptr(a) -> int:
+    """Address of a numpy array (or 0 for None)."""
+    if a is None:
+        return 0
+    return a.ctypes.data

@@ -1,0 +1,516 @@
+// Fused filter/compare/aggregate scan kernel (the lowered bytecode loop).
+//
+// One launch runs every iteration of a lowered loop.  Iteration j of the
+// reference loop reads the kLanes rows [off0 + j*kLanes, ...) of each column
+// (a "group": 32 bytes per column, VLOAD in include/voxel/exec/engine.hpp:
+// 1947-1968), evaluates the predicate atoms per lane, forms each reduction's
+// lane values, reduces them over the group in T exactly like VSUM / VCOUNT /
+// VRED_MIN / VRED_MAX (engine.hpp:2980-3110), and folds the group result into
+// its accumulator register (ADD / ADDF / MIN / MAX, engine.hpp:1286-1400).
+// Groups are independent, so threads take them grid-stride with 128-bit loads;
+// integer / min / max folds are exact in any order, f64 folds use Neumaier
+// compensation, and blocks combine in a fixed order in the last block to
+// finish, so results are deterministic for a given grid.
+#include <cstdio>
+
+#include "scan.h"
+#include "vx_common.cuh"
+#include "vx_runtime.h"
+
+namespace vx {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBlocks = 148 * 8;
+
+struct ScanPartial {
+    uint64_t u[kMaxRed];
+    double s[kMaxRed];
+    double c[kMaxRed];
+};
+
+struct Acc {
+    uint64_t u;
+    KSum k;
+};
+
+template <typename T>
+__device__ __forceinline__ bool acc_is_float(uint8_t op) {
+    return op == kAccAddF || (op == kAccTAdd && Traits<T>::kFloat);
+}
+
+__device__ __forceinline__ uint64_t acc_identity(uint8_t op) {
+    if (op == kAccMin) return 0x7FFFFFFFFFFFFFFFull;
+    if (op == kAccMax) return 0x8000000000000000ull;
+    return 0;
+}
+
+template <typename T>
+__device__ __forceinline__ void acc_fold(Acc& a, uint8_t op, uint64_t r) {
+    switch (op) {
+    case kAccAdd:
+    case kAccSub: a.u += r; break;
+    case kAccAddF: ksum_add(a.k, __longlong_as_double(static_cast<long long>(r))); break;
+    case kAccTAdd:
+        if constexpr (Traits<T>::kFloat) ksum_add(a.k, __longlong_as_double(static_cast<long long>(r)));
+        else a.u += r;
+        break;
+    case kAccMin: if (static_cast<int64_t>(r) < static_cast<int64_t>(a.u)) a.u = r; break;
+    case kAccMax: if (static_cast<int64_t>(r) > static_cast<int64_t>(a.u)) a.u = r; break;
+    default: break;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void acc_merge(Acc& a, uint8_t op, const Acc& b) {
+    if (acc_is_float<T>(op)) {
+        a.k = ksum_merge(a.k, b.k);
+    } else if (op == kAccMin) {
+        if (static_cast<int64_t>(b.u) < static_cast<int64_t>(a.u)) a.u = b.u;
+    } else if (op == kAccMax) {
+        if (static_cast<int64_t>(b.u) > static_cast<int64_t>(a.u)) a.u = b.u;
+    } else {
+        a.u += b.u;
+    }
+}
+
+template <typename T, int NC>
+__device__ __forceinline__ T col_val(const T (&v)[NC][32 / sizeof(T)], int c, int l) {
+    T x = v[0][l];
+#pragma unroll
+    for (int k = 1; k < NC; ++k)
+        if (c == k) x = v[k][l];
+    return x;
+}
+
+template <typename T, int NC>
+__device__ __forceinline__ T opnd_val(const Opnd& o, const T (&v)[NC][32 / sizeof(T)], int l) {
+    if (o.kind == kOpCol) return col_val<T, NC>(v, o.col, l);
+    if (o.kind == kOpConst) return from_bits<T>(o.bits);
+    return T(0);
+}
+
+// Evaluate every reduction of one group; res[r] is the register image.
+template <typename T, int NC, int NR>
+__device__ __forceinline__ void eval_group(const ScanParams& p, const T (&v)[NC][32 / sizeof(T)],
+                                           uint64_t (&res)[NR]) {
+    constexpr int KL = 32 / sizeof(T);
+    uint32_t ab[KL];
+#pragma unroll
+    for (int l = 0; l < KL; ++l) {
+        uint32_t b = 0;
+#pragma unroll
+        for (int a = 0; a < kMaxAtoms; ++a) {
+            if (a < p.natoms) {
+                const Atom& at = p.atom[a];
+                if (t_cmp<T>(col_val<T, NC>(v, at.col, l), from_bits<T>(at.thr), at.op)) b |= 1u << a;
+            }
+        }
+        ab[l] = b;
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        if (r >= p.nred) break;
+        const Red& rd = p.red[r];
+        T x[KL];
+#pragma unroll
+        for (int l = 0; l < KL; ++l) {
+            bool pass = !(rd.pmask & kMaskFalse) && ((ab[l] & rd.pmask) == rd.pmask);
+            x[l] = pass ? opnd_val<T, NC>(rd.a, v, l) : opnd_val<T, NC>(rd.b, v, l);
+        }
+        uint64_t out;
+        switch (rd.kind) {
+        case kRedSum: {
+            T s = T(0);
+#pragma unroll
+            for (int l = 0; l < KL; ++l) s = t_add<T>(s, x[l]);
+            out = set_scalar<T>(s);
+            break;
+        }
+        case kRedCount: {
+            uint64_t c = 0;
+#pragma unroll
+            for (int l = 0; l < KL; ++l) c += (!t_isnan<T>(x[l]) && x[l] != T(0)) ? 1 : 0;
+            out = c;
+            break;
+        }
+        case kRedMin: {
+            T m = x[0];
+#pragma unroll
+            for (int l = 1; l < KL; ++l)
+                if (x[l] < m || t_isnan<T>(x[l])) m = x[l];
+            out = set_scalar<T>(m);
+            break;
+        }
+        default: {
+            T m = x[0];
+#pragma unroll
+            for (int l = 1; l < KL; ++l)
+                if (x[l] > m || t_isnan<T>(m)) m = x[l];
+            out = set_scalar<T>(m);
+            break;
+        }
+        }
+        res[r] = out;
+    }
+}
+
+template <typename T, int NC>
+__device__ __forceinline__ void load_group(const ScanParams& p, uint64_t j, bool vec,
+                                           T (&v)[NC][32 / sizeof(T)]) {
+    constexpr int KL = 32 / sizeof(T);
+    uint64_t r0 = p.off0 + j * KL;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        if (c >= p.ncols) {
+#pragma unroll
+            for (int l = 0; l < KL; ++l) v[c][l] = T(0);
+            continue;
+        }
+        const T* base = static_cast<const T*>(p.col[c]);
+        if (vec && r0 + KL <= p.count[c]) {
+            const uint4* q = reinterpret_cast<const uint4*>(base + r0);
+            uint4 a = __ldcs(q);
+            uint4 b = __ldcs(q + 1);
+            T tmp[KL];
+            *reinterpret_cast<uint4*>(&tmp[0]) = a;
+            *reinterpret_cast<uint4*>(&tmp[KL / 2]) = b;
+#pragma unroll
+            for (int l = 0; l < KL; ++l) v[c][l] = tmp[l];
+        } else {
+#pragma unroll
+            for (int l = 0; l < KL; ++l) {
+                uint64_t idx = r0 + l;
+                v[c][l] = (idx >= r0 && idx < p.count[c]) ? base[idx] : T(0);
+            }
+        }
+    }
+}
+
+template <typename T, int NR>
+__device__ void block_reduce(const ScanParams& p, Acc (&acc)[NR], Acc* smem_out) {
+    __shared__ Acc sh[kThreads / 32][NR];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        if (r >= p.nred) break;
+        uint8_t op = p.red[r].acc;
+        for (int d = 16; d > 0; d >>= 1) {
+            Acc o;
+            o.u = shfl_down_u64(acc[r].u, d);
+            o.k.s = shfl_down_f64(acc[r].k.s, d);
+            o.k.c = shfl_down_f64(acc[r].k.c, d);
+            acc_merge<T>(acc[r], op, o);
+        }
+        if (lane == 0) sh[warp][r] = acc[r];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            if (r >= p.nred) break;
+            uint8_t op = p.red[r].acc;
+            Acc a;
+            a.u = acc_identity(op);
+            a.k = {0.0, 0.0};
+            if (lane < kThreads / 32) a = sh[lane][r];
+            for (int d = 16; d > 0; d >>= 1) {
+                Acc o;
+                o.u = shfl_down_u64(a.u, d);
+                o.k.s = shfl_down_f64(a.k.s, d);
+                o.k.c = shfl_down_f64(a.k.c, d);
+                acc_merge<T>(a, op, o);
+            }
+            if (lane == 0) smem_out[r] = a;
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int NC, int NR, int UNROLL>
+__global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ ScanParams p, int vec,
+                                                        ScanPartial* part, unsigned int* done,
+                                                        ScanResult* out) {
+    constexpr int KL = 32 / sizeof(T);
+    Acc acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
+        acc[r].k = {0.0, 0.0};
+    }
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t lastj = p.ngroups - 1;
+    for (uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j0 < p.ndata;
+         j0 += stride * UNROLL) {
+        T v[UNROLL][NC][KL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            uint64_t j = j0 + u * stride;
+            if (j < p.ndata) load_group<T, NC>(p, j, vec != 0, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            uint64_t j = j0 + u * stride;
+            if (j < p.ndata) {
+                uint64_t res[NR];
+                eval_group<T, NC, NR>(p, v[u], res);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    if (r >= p.nred) break;
+                    acc_fold<T>(acc[r], p.red[r].acc, res[r]);
+                    if (j == lastj) out->last[r] = res[r];
+                }
+            }
+        }
+    }
+
+    __shared__ Acc blk[NR];
+    block_reduce<T, NR>(p, acc, blk);
+    if (threadIdx.x < NR && threadIdx.x < p.nred) {
+        int r = threadIdx.x;
+        part[blockIdx.x].u[r] = blk[r].u;
+        part[blockIdx.x].s[r] = blk[r].k.s;
+        part[blockIdx.x].c[r] = blk[r].k.c;
+    }
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+
+    // Last block: fold the per-block partials in block order.
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
+        acc[r].k = {0.0, 0.0};
+    }
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            if (r >= p.nred) break;
+            Acc o;
+            o.u = __ldcg(&part[b].u[r]);
+            o.k.s = __ldcg(&part[b].s[r]);
+            o.k.c = __ldcg(&part[b].c[r]);
+            acc_merge<T>(acc[r], p.red[r].acc, o);
+        }
+    }
+    block_reduce<T, NR>(p, acc, blk);
+    if (threadIdx.x == 0) {
+        *done = 0;
+        // groups past the data are all-zero lanes: identical results
+        uint64_t npad = p.ngroups - p.ndata;
+        uint64_t res0[NR];
+        if (npad) {
+            T z[NC][KL];
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+#pragma unroll
+                for (int l = 0; l < KL; ++l) z[c][l] = T(0);
+            eval_group<T, NC, NR>(p, z, res0);
+        }
+        for (int r = 0; r < p.nred && r < NR; ++r) {
+            uint8_t op = p.red[r].acc;
+            Acc a = blk[r];
+            if (npad) {
+                out->last[r] = res0[r];
+                if (acc_is_float<T>(op)) {
+                    double g = __longlong_as_double(static_cast<long long>(res0[r]));
+                    double hi = __dmul_rn(static_cast<double>(npad), g);
+                    double lo = fma(static_cast<double>(npad), g, -hi);
+                    ksum_add(a.k, hi);
+                    a.k.c = __dadd_rn(a.k.c, lo);
+                } else if (op == kAccMin || op == kAccMax) {
+                    Acc o;
+                    o.u = res0[r];
+                    acc_merge<T>(a, op, o);
+                } else {
+                    a.u += npad * res0[r];
+                }
+            }
+            uint64_t a0 = p.acc0[r];
+            uint64_t fin = a0;
+            switch (op) {
+            case kAccAdd: fin = a0 + a.u; break;
+            case kAccSub: fin = a0 - a.u; break;
+            case kAccAddF: {
+                KSum k{__longlong_as_double(static_cast<long long>(a0)), 0.0};
+                k = ksum_merge(k, a.k);
+                fin = static_cast<uint64_t>(__double_as_longlong(ksum_value(k)));
+                break;
+            }
+            case kAccTAdd:
+                if constexpr (Traits<T>::kFloat) {
+                    KSum k{__longlong_as_double(static_cast<long long>(a0)), 0.0};
+                    k = ksum_merge(k, a.k);
+                    fin = static_cast<uint64_t>(__double_as_longlong(ksum_value(k)));
+                } else {
+                    fin = set_scalar<T>(static_cast<T>(a0 + a.u));
+                }
+                break;
+            case kAccMin: fin = static_cast<int64_t>(a.u) < static_cast<int64_t>(a0) ? a.u : a0; break;
+            case kAccMax: fin = static_cast<int64_t>(a.u) > static_cast<int64_t>(a0) ? a.u : a0; break;
+            default: break;
+            }
+            out->acc[r] = fin;
+        }
+        out->status = kOk;
+    }
+}
+
+template <typename T, int NC, int NR, int UNROLL>
+int launch_t(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    ScanPartial* part = static_cast<ScanPartial*>(scratch);
+    unsigned int* done = reinterpret_cast<unsigned int*>(static_cast<char*>(scratch) + kMaxBlocks * sizeof(ScanPartial));
+    bool vec = true;
+    for (int c = 0; c < p.ncols; ++c) {
+        uintptr_t a = reinterpret_cast<uintptr_t>(p.col[c]) + p.off0 * sizeof(T);
+        if (a % 16) vec = false;
+    }
+    scan_kernel<T, NC, NR, UNROLL><<<grid, kThreads, 0, s>>>(p, vec ? 1 : 0, part, done, d_out);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int dispatch(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    if (p.ncols <= 1 && p.nred <= 2) return launch_t<T, 1, 2, 4>(p, grid, d_out, scratch, s);
+    if (p.ncols <= 1) return launch_t<T, 1, kMaxRed, 2>(p, grid, d_out, scratch, s);
+    return launch_t<T, kMaxCols, kMaxRed, 1>(p, grid, d_out, scratch, s);
+}
+
+// ---- segment aggregates (AGG_* opcodes) -------------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) seg_agg_kernel(const T* col, uint64_t begin, uint64_t end,
+                                                          int kind, uint64_t init_bits, ScanPartial* part,
+                                                          unsigned int* done, uint64_t* out3) {
+    // kind 0: count nonzero; 1: sum (ints widened to i64, floats in f64);
+    // 3: min, 4: max, folded with < and > from the slot's current value, as
+    // HandleAggregate does (NaN never replaces the running value).
+    uint64_t cnt = 0, isum = 0;
+    KSum k{0.0, 0.0};
+    T m = from_bits<T>(init_bits);
+    for (uint64_t i = begin + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < end;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        T x = col[i];
+        if (kind == 0) cnt += (x != T(0)) ? 1 : 0;
+        else if (kind == 1) {
+            if constexpr (Traits<T>::kFloat) ksum_add(k, static_cast<double>(x));
+            else isum += static_cast<uint64_t>(static_cast<int64_t>(x));
+        } else if (kind == 3) {
+            if (x < m) m = x;
+        } else {
+            if (x > m) m = x;
+        }
+    }
+    __shared__ uint64_t su[kThreads];
+    __shared__ double ss[kThreads], sc[kThreads];
+    __shared__ T sm[kThreads];
+    int t = threadIdx.x;
+    su[t] = kind == 0 ? cnt : isum;
+    ss[t] = k.s;
+    sc[t] = k.c;
+    sm[t] = m;
+    __syncthreads();
+    for (int d = kThreads / 2; d > 0; d >>= 1) {
+        if (t < d) {
+            su[t] += su[t + d];
+            KSum a{ss[t], sc[t]}, b{ss[t + d], sc[t + d]};
+            a = ksum_merge(a, b);
+            ss[t] = a.s;
+            sc[t] = a.c;
+            if (kind == 3 ? (sm[t + d] < sm[t]) : (sm[t + d] > sm[t])) sm[t] = sm[t + d];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        part[blockIdx.x].u[0] = su[0];
+        part[blockIdx.x].s[0] = ss[0];
+        part[blockIdx.x].c[0] = sc[0];
+        part[blockIdx.x].u[1] = to_bits<T>(sm[0]);
+    }
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (t == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last || t != 0) return;
+    __threadfence();
+    uint64_t u = 0;
+    KSum a{0.0, 0.0};
+    T mm = from_bits<T>(init_bits);
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+        u += __ldcg(&part[b].u[0]);
+        KSum o{__ldcg(&part[b].s[0]), __ldcg(&part[b].c[0])};
+        a = ksum_merge(a, o);
+        T bm = from_bits<T>(__ldcg(&part[b].u[1]));
+        if (kind == 3 ? (bm < mm) : (bm > mm)) mm = bm;
+    }
+    *done = 0;
+    out3[0] = kind >= 3 ? to_bits<T>(mm) : u;
+    out3[1] = static_cast<uint64_t>(__double_as_longlong(a.s));
+    out3[2] = static_cast<uint64_t>(__double_as_longlong(a.c));
+}
+
+}  // namespace
+
+size_t scan_scratch_bytes() { return kMaxBlocks * sizeof(ScanPartial) + 256; }
+
+int scan_scratch_init(void* scratch, cudaStream_t s) {
+    VX_CUDA(cudaMemsetAsync(static_cast<char*>(scratch) + kMaxBlocks * sizeof(ScanPartial), 0, 256, s));
+    return kOk;
+}
+
+int scan_grid(int dtype, uint64_t ndata, int ncols, int nred) {
+    int sms = sm_count();
+    if (sms <= 0) sms = 148;
+    int unroll = (ncols <= 1 && nred <= 2) ? 4 : (ncols <= 1 ? 2 : 1);
+    uint64_t need = (ndata + static_cast<uint64_t>(kThreads) * unroll - 1) / (static_cast<uint64_t>(kThreads) * unroll);
+    int per_sm = 8;
+    uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
+    if (cap > kMaxBlocks) cap = kMaxBlocks;
+    uint64_t g = need < cap ? need : cap;
+    (void)dtype;
+    return g < 1 ? 1 : static_cast<int>(g);
+}
+
+int launch_scan(const ScanParams& p, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    int grid = scan_grid(p.dtype, p.ndata, p.ncols, p.nred);
+    switch (p.dtype) {
+    case F64: return dispatch<double>(p, grid, d_out, scratch, s);
+    case F32: return dispatch<float>(p, grid, d_out, scratch, s);
+    case I64: return dispatch<int64_t>(p, grid, d_out, scratch, s);
+    case I32: return dispatch<int32_t>(p, grid, d_out, scratch, s);
+    case U64: return dispatch<uint64_t>(p, grid, d_out, scratch, s);
+    case U32: return dispatch<uint32_t>(p, grid, d_out, scratch, s);
+    default: set_error(kErrInvalidArg, "unknown element type %d", p.dtype); return kErrInvalidArg;
+    }
+}
+
+int launch_segment_agg(int dtype, const void* col, uint64_t begin, uint64_t end, int kind,
+                       uint64_t init_bits, uint64_t* d_out3, void* scratch, cudaStream_t s) {
+    ScanPartial* part = static_cast<ScanPartial*>(scratch);
+    unsigned int* done = reinterpret_cast<unsigned int*>(static_cast<char*>(scratch) + kMaxBlocks * sizeof(ScanPartial));
+    uint64_t n = end > begin ? end - begin : 0;
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t need = (n + kThreads * 4 - 1) / (kThreads * 4);
+    uint64_t cap = static_cast<uint64_t>(sms) * 4;
+    int grid = static_cast<int>(need < 1 ? 1 : (need < cap ? need : cap));
+    switch (dtype) {
+    case F64: seg_agg_kernel<double><<<grid, kThreads, 0, s>>>(static_cast<const double*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    case F32: seg_agg_kernel<float><<<grid, kThreads, 0, s>>>(static_cast<const float*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    case I64: seg_agg_kernel<int64_t><<<grid, kThreads, 0, s>>>(static_cast<const int64_t*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    case I32: seg_agg_kernel<int32_t><<<grid, kThreads, 0, s>>>(static_cast<const int32_t*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    case U64: seg_agg_kernel<uint64_t><<<grid, kThreads, 0, s>>>(static_cast<const uint64_t*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    case U32: seg_agg_kernel<uint32_t><<<grid, kThreads, 0, s>>>(static_cast<const uint32_t*>(col), begin, end, kind, init_bits, part, done, d_out3); break;
+    default: set_error(kErrInvalidArg, "unknown element type %d", dtype); return kErrInvalidArg;
+    }
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+}  // namespace vx
