@@ -181,6 +181,18 @@ double    voxel_engine_last_device_ms(const void* engine);
 int       voxel_last_status(void);
 
 /* ================================================================
+ * Additive: memory helpers for callers that keep columns resident
+ * ================================================================ */
+void*     voxel_device_alloc(size_t bytes);
+void      voxel_device_free(void* d_ptr);
+int       voxel_copy_to_device(void* d_dst, const void* src, size_t bytes, void* stream);
+int       voxel_copy_to_host(void* dst, const void* d_src, size_t bytes, void* stream);
+int       voxel_stream_sync(void* stream);
+/* page-lock an existing host buffer so the H2D copies of host entry points run at full speed */
+int       voxel_host_register(void* ptr, size_t bytes);
+int       voxel_host_unregister(void* ptr);
+
+/* ================================================================
  * Additive: VectorFilter / ColumnFilter / SelectionVector on the GPU
  * (reference include/voxel/ops/filter.hpp:42-399).  Host buffers.
  * ================================================================ */
@@ -191,7 +203,7 @@ size_t    voxel_vfilter(int dtype, int op, const void* data, size_t n, uint64_t 
 size_t    voxel_bitmap_and(const uint64_t* const* bitmaps, size_t nbitmaps, size_t rows,
                            uint64_t* out);
 size_t    voxel_selection_from_bitmap(const uint64_t* bitmap, size_t rows, uint32_t* out);
-/* device variants (stream may be NULL for the calling thread's stream) */
+/* device variants: asynchronous on `stream` (NULL = the CUDA default stream) */
 int       voxel_vfilter_dev(int dtype, int op, const void* d_data, size_t n, uint64_t lo_bits,
                             uint64_t hi_bits, uint64_t* d_bitmap, uint64_t* d_count, void* stream);
 int       voxel_selection_from_bitmap_dev(const uint64_t* d_bitmap, size_t rows, uint32_t* d_out,
@@ -232,6 +244,8 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              const int32_t* qty, size_t n, double price_gt, int32_t qty_lo,
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
+/* rows each thread of the fused scan handles per tile (4, 8 or 16; tuning knob) */
+int       voxel_scan_groupby_tune(int rows_per_thread);
 int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,
                                  const int32_t* d_dict, size_t card, const double* d_price,
                                  const int32_t* d_qty, size_t n, double price_gt, int32_t qty_lo,
@@ -250,6 +264,13 @@ size_t    voxel_groupby_i32_f64(const int32_t* keys, const double* values, size_
 size_t    voxel_groupby_u32_f64(const uint32_t* keys, const double* values, size_t n,
                                 size_t expected_groups, uint32_t* out_keys, double* out_sum,
                                 double* out_min, double* out_max, uint64_t* out_count);
+/* the voxel_agg_* object: device-pointer accumulate, and its groups sorted by key */
+int       voxel_agg_accumulate_dev(void* agg, const uint32_t* d_keys, const double* d_values, size_t count,
+                                   void* stream);
+size_t    voxel_agg_results(void* agg, uint32_t* keys, double* sum, double* min, double* max,
+                            uint64_t* count);
+/* the voxel_dict_* object's sorted dictionary (returns the cardinality) */
+size_t    voxel_dict_values(const void* dict, double* out);
 /* GroupedAggregator over pre-sorted keys (aggregate.hpp:665-706) */
 size_t    voxel_grouped_sorted_i32_f64(const int32_t* sorted_keys, const double* values,
                                        size_t n, int32_t* out_keys, double* out_sum,

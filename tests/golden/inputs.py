@@ -128,10 +128,15 @@ def config2(n: int, seed: int, card: int = 1000) -> dict:
     values = np.sort(rng.choice(np.arange(-50000, 50000, dtype=np.int64), size=card, replace=False)).astype(np.int32)
     rank = zipf_alias_keys(n, card, 1.1, rng)
     perm = rng.permutation(card)
-    key = values[perm[rank]]
+    code = perm[rank]                      # position of each row's key in the sorted value list
+    key = values[code]
     price = rng.lognormal(3.0, 1.0, n)
     qty = rng.integers(1, 101, size=n).astype(np.int32)
-    dict_, idx = encode.dict_build_i32(key)
+    # the reference dictionary: sorted unique values present, u32 indices into it
+    present = np.bincount(code, minlength=card) > 0
+    remap = (np.cumsum(present) - 1).astype(np.uint32)
+    dict_ = values[present]
+    idx = remap[code]
     width = encode.bit_width(idx)
     packed = encode.bitpack(idx, width)
     return dict(n=n, key=key, dict=dict_, idx=idx, width=width, packed=packed, price=price, qty=qty)

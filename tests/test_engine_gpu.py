@@ -122,7 +122,7 @@ def test_templates_match_sql_and_interpreter():
             prog = T.random_program(dt, rng, agg=agg)
             got, _ = run_gpu(dt, prog.code, [col], prog.registers(n))
             sql = T.sql_reference(prog, col)
-            v = T.image_value(dt, got[0])
+            v = got[0] if agg == "COUNT" else T.image_value(dt, got[0])
             if agg == "SUM" and dt in (0, 1):
                 assert abs(v - sql) <= (F64_RTOL if dt == 0 else F32_RTOL) * max(abs(sql), 1.0)
             elif agg in ("MIN", "MAX") and dt == T.F32:

@@ -1,0 +1,187 @@
+"""Operator kernels on the GPU against the oracle: VectorFilter / selection
+vectors, decoders, radix sort and hash join.  Small cases reproduce the
+reference's own outputs (golden fixtures); large cases check size-independent
+properties (round trips, sortedness + stability, counts, pair order)."""
+import hashlib
+import struct
+
+import numpy as np
+import pytest
+
+import inputs
+import oracle
+from voxel_b200 import capi, encode
+from voxel_b200 import templates as T
+
+pytestmark = pytest.mark.gpu
+FAIL = (1 << 64) - 1
+
+
+def digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def bits(dt, v):
+    if dt == T.F32:
+        return struct.unpack("<I", struct.pack("<f", v))[0]
+    return T.reg_image(dt, v)
+
+
+def vfilter(dt, op, col, a, b):
+    n = col.size
+    bm = np.zeros(max((n + 63) // 64, 1), np.uint64)
+    c = capi.lib().voxel_vfilter(dt, op, col.ctypes.data, n, bits(dt, a), bits(dt, b), bm.ctypes.data)
+    assert c != FAIL, capi.last_error()
+    return c, bm[: (n + 63) // 64]
+
+
+def test_vfilter_golden(golden):
+    k = golden["ops"]["vfilter_kat"]
+    c, bm = vfilter(T.F64, 4, np.asarray(k["data"]), 4.0, 0.0)
+    assert c == 4 and int(bm[0]) == k["bitmap"]  # bits 2,3,6,7 (test_suite.cpp:410-427)
+    for case in golden["ops"]["vfilter"]:
+        col = inputs.column(case["dtype"], case["n"], case["seed"])
+        c, bm = vfilter(case["dtype"], case["op"], col, case["a"], case["b"])
+        assert c == case["count"] and digest(bm) == case["digest"], case
+
+
+def test_vfilter_full_size():
+    rng = np.random.default_rng(21)
+    n = (1 << 25) + 17
+    for dt in (T.F64, T.I32):
+        col = T.make_column(dt, n, rng)
+        c, bm = vfilter(dt, 6, col, 10, 50) if dt == T.I32 else vfilter(dt, 4, col, 20.0, 0.0)
+        m = (col >= 10) & (col <= 50) if dt == T.I32 else col > 20.0
+        assert c == int(m.sum())
+        want = np.packbits(m, bitorder="little")
+        got = bm.view(np.uint8)[: want.size]
+        assert (got == want).all()
+
+
+def test_selection_and_bitmap_and(golden):
+    L = capi.lib()
+    for case in golden["ops"]["selection"]:
+        bm = inputs.bitmap(case["n"], case["seed"])
+        out = np.zeros(max(case["n"], 1), np.uint32)
+        c = L.voxel_selection_from_bitmap(bm.ctypes.data, case["n"], out.ctypes.data)
+        assert c == case["count"] and digest(out[:c]) == case["digest"]
+    rng = np.random.default_rng(22)
+    for n in (1, 63, 64, 65, 1000, 65536 * 3 + 5, 1 << 25):
+        a = inputs.bitmap(n, int(rng.integers(1 << 30)))
+        b = inputs.bitmap(n, int(rng.integers(1 << 30)))
+        words = (n + 63) // 64
+        out = np.zeros(words, np.uint64)
+        arr = (C_ptrs := (__import__("ctypes").c_void_p * 2)(a.ctypes.data, b.ctypes.data))
+        c = L.voxel_bitmap_and(arr, 2, n, out.ctypes.data)
+        want = np.zeros(words, np.uint64)
+        wc = oracle.port().vo_bitmap_and(arr, 2, n, want.ctypes.data)
+        assert c == wc and (out == want).all()
+        sel = np.zeros(max(int(c), 1), np.uint32)
+        cs = L.voxel_selection_from_bitmap(out.ctypes.data, n, sel.ctypes.data)
+        assert cs == c
+        ref = np.zeros(max(n, 1), np.uint32)
+        rc = oracle.port().vo_selection_from_bitmap(want.ctypes.data, n, ref.ctypes.data)
+        assert rc == cs and (sel[:cs] == ref[:rc]).all()
+        del C_ptrs
+
+
+def test_decoders_golden_and_round_trip(golden):
+    L = capi.lib()
+    for case in golden["ops"]["bitpack"]:
+        v = inputs.u32_values(case["n"], case["maxv"], case["seed"])
+        w = encode.bit_width(v)
+        words = encode.bitpack(v, w)
+        assert w == case["width"] and words.size == case["nwords"] and digest(words) == case["words_digest"]
+        out = np.zeros(v.size, np.uint32)
+        assert L.voxel_bitpack_decode(words.ctypes.data, words.size, w, v.size, 0, v.size, out.ctypes.data) == 0
+        assert (out == v).all()
+        if v.size > 10:  # offset window, past-the-end count clipped like DecodeBatch
+            out2 = np.zeros(v.size, np.uint32)
+            off = v.size // 3
+            assert L.voxel_bitpack_decode(words.ctypes.data, words.size, w, v.size, off, v.size, out2.ctypes.data) == 0
+            assert (out2[: v.size - off] == v[off:]).all()
+    for case in golden["ops"]["rle"]:
+        v = inputs.rle_i64(case["n"], case["seed"])
+        vals, runs = encode.rle_build(v)
+        assert vals.size == case["runs"] and digest(vals) == case["values_digest"]
+        for dc in case["decodes"]:
+            out = np.zeros(dc["count"], np.int64)
+            assert L.voxel_rle_decode_i64(vals.ctypes.data, runs.ctypes.data, vals.size, dc["offset"], dc["count"],
+                                          out.ctypes.data) == 0
+            assert digest(out) == dc["digest"], dc
+    # dictionary + bit-packed key column of the scan workload, full size
+    d = inputs.config2(1 << 25, 2002)
+    out = np.zeros(d["n"], np.int32)
+    assert L.voxel_dict_bitpack_decode_i32(d["packed"].ctypes.data, d["packed"].size, d["width"], d["dict"].ctypes.data,
+                                           d["dict"].size, d["n"], 0, d["n"], out.ctypes.data) == 0
+    assert (out == d["key"]).all()
+    o2 = np.zeros(1000, np.int32)
+    assert L.voxel_dict_decode(T.I32, d["dict"].ctypes.data, d["dict"].size, d["idx"].ctypes.data, d["n"], 12345, 1000,
+                               o2.ctypes.data) == 0
+    assert (o2 == d["key"][12345:13345]).all()
+    # ts column: strictly increasing, runs of 1..64, RLE round trip at full size
+    ts = inputs.rle_i64(1 << 25, 2004)
+    vals, runs = encode.rle_build(ts)
+    out = np.zeros(ts.size + 100, np.int64)
+    assert L.voxel_rle_decode_i64(vals.ctypes.data, runs.ctypes.data, vals.size, 0, out.size, out.ctypes.data) == 0
+    assert (out[: ts.size] == ts).all() and (out[ts.size:] == 0).all()
+
+
+def test_radix_sort_golden_and_properties(golden):
+    L = capi.lib()
+    for case in golden["ops"]["radix"]:
+        k = inputs.sort_keys(case["dtype"], case["n"], case["seed"])
+        idx = np.arange(case["n"], dtype=np.uint32)
+        assert L.voxel_radix_sort(case["dtype"], k.ctypes.data, idx.ctypes.data, case["n"]) == 0, capi.last_error()
+        assert digest(k) == case["keys_digest"] and digest(idx) == case["idx_digest"], case
+    rng = np.random.default_rng(23)
+    for dt, n in ((T.U64, 1 << 24), (T.I64, (1 << 22) + 3), (T.U32, (1 << 23) + 1), (T.I32, 100_001)):
+        k0 = inputs.sort_keys(dt, n, int(rng.integers(1 << 30)))
+        k = k0.copy()
+        idx = np.arange(n, dtype=np.uint32)
+        assert L.voxel_radix_sort(dt, k.ctypes.data, idx.ctypes.data, n) == 0, capi.last_error()
+        order = np.argsort(k0, kind="stable")  # stable ascending = the reference's permutation
+        assert (idx == order).all() and (k == k0[order]).all()
+
+
+def test_hashjoin_golden_and_properties(golden):
+    L = capi.lib()
+    for case in golden["ops"]["hashjoin"]:
+        if case["seed"] == 0:
+            b = np.array([1, 2, 3, 4], np.int64)
+            p = np.array([2, 4, 6], np.int64)
+        else:
+            b, p = inputs.join_input(case["nb"], case["np"], case["dup"], case["seed"])
+        cap = case["np"] * (8 if case["dup"] else 1) + 8
+        l = np.zeros(cap, np.uint32)
+        r = np.zeros(cap, np.uint32)
+        m = L.voxel_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, l.ctypes.data, r.ctypes.data, cap,
+                                 case["all"])
+        assert m == case["matches"] and digest(l[:m], r[:m]) == case["digest"], case
+    rng = np.random.default_rng(24)
+    for nb, np_, dup in ((1 << 20, 1 << 23, False), (50_000, 400_000, True)):
+        b, p = inputs.join_input(nb, np_, dup, int(rng.integers(1 << 30)))
+        cap = np_ * (16 if dup else 1)
+        l = np.zeros(cap, np.uint32)
+        r = np.zeros(cap, np.uint32)
+        m = L.voxel_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, l.ctypes.data, r.ctypes.data, cap, 1)
+        assert m != FAIL, capi.last_error()
+        wl = np.zeros(cap, np.uint32)
+        wr = np.zeros(cap, np.uint32)
+        wm = oracle.port().vo_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, wl.ctypes.data,
+                                           wr.ctypes.data, cap, 1)
+        assert m == wm and (l[:m] == wl[:m]).all() and (r[:m] == wr[:m]).all()
+        assert (np.diff(l[:m].astype(np.int64)) >= 0).all() and (b[r[:m]] == p[l[:m]]).all()
+    # capped probe: the first max_matches pairs in probe order
+    b, p = inputs.join_input(1000, 5000, False, 77)
+    l = np.zeros(100, np.uint32)
+    r = np.zeros(100, np.uint32)
+    m = L.voxel_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, l.ctypes.data, r.ctypes.data, 100, 1)
+    wl = np.zeros(100, np.uint32)
+    wr = np.zeros(100, np.uint32)
+    wm = oracle.port().vo_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, wl.ctypes.data, wr.ctypes.data,
+                                       100, 1)
+    assert m == wm == 100 and (l == wl).all() and (r == wr).all()

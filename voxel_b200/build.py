@@ -43,6 +43,7 @@ CORE_SOURCES = [
     "groupby.cu",
     "radix.cu",
     "join.cu",
+    "ops.cu",
     "estimator.cu",
     "batch.cu",
     "serve.cpp",

@@ -111,6 +111,13 @@ _SIGS = {
     "voxel_pool_destroy": (None, [vp]),
     "voxel_pool_wait_all": (None, [vp]),
     "voxel_pool_thread_count": (sz, [vp]),
+    "voxel_device_alloc": (vp, [sz]),
+    "voxel_device_free": (None, [vp]),
+    "voxel_copy_to_device": (C.c_int, [vp, vp, sz, vp]),
+    "voxel_copy_to_host": (C.c_int, [vp, vp, sz, vp]),
+    "voxel_stream_sync": (C.c_int, [vp]),
+    "voxel_host_register": (C.c_int, [vp, sz]),
+    "voxel_host_unregister": (C.c_int, [vp]),
     "voxel_vfilter": (sz, [C.c_int, C.c_int, vp, sz, u64, u64, vp]),
     "voxel_bitmap_and": (sz, [vp, sz, sz, vp]),
     "voxel_selection_from_bitmap": (sz, [vp, sz, vp]),

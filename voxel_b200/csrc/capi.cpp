@@ -225,6 +225,36 @@ void voxel_pool_destroy(void* p) { delete static_cast<Pool*>(p); }
 void voxel_pool_wait_all(void* p) { static_cast<Pool*>(p)->wait_all(); }
 size_t voxel_pool_thread_count(const void* p) { return static_cast<const Pool*>(p)->size(); }
 
+// ---- memory helpers ------------------------------------------------------------------
+void* voxel_device_alloc(size_t bytes) {
+    vx::clear_error();
+    if (vx::ensure_device()) return nullptr;
+    return vx::dev_alloc(bytes);
+}
+void voxel_device_free(void* p) { vx::dev_free(p); }
+int voxel_copy_to_device(void* dst, const void* src, size_t bytes, void* stream) {
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : vx::thread_stream();
+    int st = vx::h2d(dst, src, bytes, s);
+    return st ? st : (stream ? vx::kOk : vx::sync(s));
+}
+int voxel_copy_to_host(void* dst, const void* src, size_t bytes, void* stream) {
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : vx::thread_stream();
+    int st = vx::d2h(dst, src, bytes, s);
+    return st ? st : (stream ? vx::kOk : vx::sync(s));
+}
+int voxel_stream_sync(void* stream) {
+    return vx::sync(stream ? static_cast<cudaStream_t>(stream) : vx::thread_stream());
+}
+int voxel_host_register(void* ptr, size_t bytes) {
+    if (vx::ensure_device()) return vx::kErrNoDevice;
+    VX_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    return vx::kOk;
+}
+int voxel_host_unregister(void* ptr) {
+    VX_CUDA(cudaHostUnregister(ptr));
+    return vx::kOk;
+}
+
 // ---- errors --------------------------------------------------------------------------
 const char* voxel_last_error(void) { return vx::last_error(); }
 int voxel_last_status(void) { return vx::last_status(); }

@@ -1,0 +1,379 @@
+// Column decoders (reference include/voxel/data/encoding.hpp).
+//
+//   BitPackedEncoding::Decode / DecodeBatch (397-422): value i lives at bit i*w
+//     of little-endian u64 words, LSB first, straddling into the next word.
+//   DictionaryEncoding<T>::DecodeBatch (156-167): out[i] = Dictionary[Indices[i]].
+//   RLEEncoding<T>::DecodeBatch (231-257): (value, run length) pairs expanded
+//     from row `offset`; rows past the last run decode to T{}.
+// Outputs are written once, coalesced; the packed words are read through L1
+// (neighbouring threads share words); the RLE decode scans the run lengths
+// into row starts (decoupled look-back) and each block expands the runs that
+// cover its row range from shared memory.
+#include "decode.h"
+#include "voxel_c.h"
+#include "vx_common.cuh"
+#include "vx_runtime.h"
+#include "vx_scan.cuh"
+
+namespace vx {
+
+namespace {
+
+constexpr int kDThreads = 256;
+
+__device__ __forceinline__ uint32_t unpack_row(const uint64_t* __restrict__ words, uint64_t nwords, uint64_t row,
+                                               uint32_t w, uint64_t mask) {
+    uint64_t bit = row * w;
+    uint64_t wi = bit >> 6;
+    uint32_t sh = static_cast<uint32_t>(bit & 63);
+    uint64_t v = __ldg(words + wi) >> sh;
+    if (sh + w > 64 && wi + 1 < nwords) v |= __ldg(words + wi + 1) << (64 - sh);
+    return static_cast<uint32_t>(v & mask);
+}
+
+__global__ void bitunpack_kernel(const uint64_t* __restrict__ words, uint64_t nwords, uint32_t w, uint64_t offset,
+                                 uint64_t count, uint32_t* __restrict__ out) {
+    const uint64_t mask = w >= 64 ? ~0ull : ((1ull << w) - 1);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = unpack_row(words, nwords, offset + i, w, mask);
+}
+
+template <typename T>
+__global__ void dict_bitunpack_kernel(const uint64_t* __restrict__ words, uint64_t nwords, uint32_t w,
+                                      const T* __restrict__ dict, uint32_t card, uint64_t offset, uint64_t count,
+                                      T* __restrict__ out, int* err) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    T* sd = reinterpret_cast<T*>(sm);
+    const bool in_smem = card <= 8192;
+    if (in_smem)
+        for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) sd[i] = dict[i];
+    __syncthreads();
+    const uint64_t mask = w >= 64 ? ~0ull : ((1ull << w) - 1);
+    bool bad = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t k = unpack_row(words, nwords, offset + i, w, mask);
+        if (k >= card) { bad = true; out[i] = T(0); continue; }
+        out[i] = in_smem ? sd[k] : __ldg(dict + k);
+    }
+    if (bad) atomicOr(err, 2);
+}
+
+template <typename T>
+__global__ void dict_gather_kernel(const T* __restrict__ dict, uint32_t card, const uint32_t* __restrict__ idx,
+                                   uint64_t count, T* __restrict__ out, int* err) {
+    bool bad = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t k = __ldcs(idx + i);
+        if (k >= card) { bad = true; out[i] = T(0); continue; }
+        out[i] = __ldg(dict + k);
+    }
+    if (bad) atomicOr(err, 2);
+}
+
+// exclusive prefix of u32 run lengths -> u64 row starts (single pass)
+constexpr int kRunsPerTile = kDThreads * 8;
+
+__global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* __restrict__ runs, uint64_t nruns,
+                                                               uint64_t* __restrict__ starts,
+                                                               unsigned long long* status, unsigned int* ctr,
+                                                               int* err) {
+    __shared__ uint64_t s_tile, s_base;
+    __shared__ uint64_t s_warp[kDThreads / 32];
+    const uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        uint64_t tile = s_tile;
+        if (tile >= ntiles) break;
+        uint64_t r0 = tile * kRunsPerTile + threadIdx.x * 8;
+        uint64_t v[8];
+        uint64_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            v[k] = r0 + k < nruns ? runs[r0 + k] : 0;
+            c += v[k];
+        }
+        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint64_t inc = c;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += y;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            uint64_t x = lane < kDThreads / 32 ? s_warp[lane] : 0, t = x;
+            for (int d = 1; d < 32; d <<= 1) {
+                uint64_t y = __shfl_up_sync(0xffffffffu, t, d);
+                if (lane >= d) t += y;
+            }
+            if (lane < kDThreads / 32) s_warp[lane] = t - x;
+            if (lane == kDThreads / 32 - 1) s_base = lookback_exclusive(status, tile, t, err);
+        }
+        __syncthreads();
+        uint64_t pos = s_base + s_warp[warp] + (inc - c);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (r0 + k < nruns) starts[r0 + k] = pos;
+            pos += v[k];
+        }
+        if (r0 < nruns && r0 + 8 >= nruns) starts[nruns] = pos;  // the thread holding the last run: total rows
+        __syncthreads();
+    }
+}
+
+// rows [offset, offset+count): block b expands rows [b*R, (b+1)*R) of the output
+constexpr int kRleRows = 4096;
+
+template <typename T>
+__global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restrict__ values,
+                                                               const uint64_t* __restrict__ starts, uint64_t nruns,
+                                                               uint64_t offset, uint64_t count, T* __restrict__ out) {
+    __shared__ uint64_t s_lo;
+    const uint64_t total = starts[nruns];
+    for (uint64_t blk = blockIdx.x; blk * kRleRows < count; blk += gridDim.x) {
+        const uint64_t row0 = offset + blk * kRleRows;
+        if (threadIdx.x == 0) {
+            // last run whose start <= row0 (upper_bound - 1)
+            uint64_t lo = 0, hi = nruns;
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) >> 1;
+                if (starts[mid] <= row0) lo = mid + 1; else hi = mid;
+            }
+            s_lo = lo ? lo - 1 : 0;
+        }
+        __syncthreads();
+        const uint64_t k0 = s_lo;
+        for (uint32_t j = threadIdx.x; j < kRleRows; j += blockDim.x) {
+            uint64_t i = blk * kRleRows + j;
+            if (i >= count) break;
+            uint64_t row = offset + i;
+            if (row >= total) { out[i] = T(0); continue; }
+            // runs are >= 1 row long, so the covering run is within j+1 runs of k0
+            uint64_t lo = k0, hi = k0 + j + 2 < nruns ? k0 + j + 2 : nruns;
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) >> 1;
+                if (__ldg(starts + mid) <= row) lo = mid + 1; else hi = mid;
+            }
+            out[i] = __ldg(values + (lo - 1));
+        }
+        __syncthreads();
+    }
+}
+
+int grid_for(uint64_t n, int per_sm = 8) {
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = (n + kDThreads - 1) / kDThreads;
+    uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : static_cast<int>(b);
+}
+
+}  // namespace
+
+int launch_bitunpack(const uint64_t* words, uint64_t nwords, uint32_t w, uint64_t value_count, uint64_t offset,
+                     uint64_t count, uint32_t* out, cudaStream_t s) {
+    if (w == 0 || w > 32) {
+        set_error(kErrInvalidArg, "bit width %u outside 1..32", w);
+        return kErrInvalidArg;
+    }
+    if (offset >= value_count) return kOk;
+    if (count > value_count - offset) count = value_count - offset;  // reference stops at ValueCount
+    if (!count) return kOk;
+    bitunpack_kernel<<<grid_for(count), kDThreads, 0, s>>>(words, nwords, w, offset, count, out);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int launch_dict_bitunpack_i32(const uint64_t* words, uint64_t nwords, uint32_t w, const int32_t* dict, uint32_t card,
+                              uint64_t value_count, uint64_t offset, uint64_t count, int32_t* out, int* err,
+                              cudaStream_t s) {
+    if (w == 0 || w > 32) {
+        set_error(kErrInvalidArg, "bit width %u outside 1..32", w);
+        return kErrInvalidArg;
+    }
+    if (offset >= value_count) return kOk;
+    if (count > value_count - offset) count = value_count - offset;
+    if (!count) return kOk;
+    size_t smem = card <= 8192 ? card * sizeof(int32_t) : 0;
+    dict_bitunpack_kernel<int32_t><<<grid_for(count), kDThreads, smem, s>>>(words, nwords, w, dict, card, offset,
+                                                                           count, out, err);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int launch_dict_gather(int dtype, const void* dict, uint32_t card, const uint32_t* idx, uint64_t count, void* out,
+                       int* err, cudaStream_t s) {
+    if (!count) return kOk;
+    if (dtype == F64)
+        dict_gather_kernel<double><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const double*>(dict), card, idx,
+                                                                         count, static_cast<double*>(out), err);
+    else if (dtype == I32)
+        dict_gather_kernel<int32_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const int32_t*>(dict), card,
+                                                                          idx, count, static_cast<int32_t*>(out), err);
+    else if (dtype == I64 || dtype == U64)
+        dict_gather_kernel<uint64_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const uint64_t*>(dict), card,
+                                                                           idx, count, static_cast<uint64_t*>(out),
+                                                                           err);
+    else
+        dict_gather_kernel<uint32_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const uint32_t*>(dict), card,
+                                                                           idx, count, static_cast<uint32_t*>(out),
+                                                                           err);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+size_t rle_scratch_bytes(uint64_t nruns) {
+    uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
+    return (nruns + 1) * 8 + (ntiles + 1) * 8 + 64;
+}
+
+int launch_rle_decode_i64(const int64_t* values, const uint32_t* runs, uint64_t nruns, uint64_t offset,
+                          uint64_t count, int64_t* out, void* scratch, int* err, cudaStream_t s) {
+    if (!count) return kOk;
+    if (nruns == 0) {
+        VX_CUDA(cudaMemsetAsync(out, 0, count * 8, s));
+        return kOk;
+    }
+    uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
+    uint64_t* starts = static_cast<uint64_t*>(scratch);
+    unsigned long long* status = reinterpret_cast<unsigned long long*>(starts + nruns + 1);
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(status + ntiles);
+    VX_CUDA(cudaMemsetAsync(status, 0, (ntiles + 1) * 8, s));
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = ntiles < static_cast<uint64_t>(sms) * 4 ? ntiles : static_cast<uint64_t>(sms) * 4;
+    run_starts_kernel<<<static_cast<unsigned>(b), kDThreads, 0, s>>>(runs, nruns, starts, status, ctr, err);
+    VX_CUDA(cudaGetLastError());
+    uint64_t blocks = (count + kRleRows - 1) / kRleRows;
+    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    rle_expand_kernel<int64_t><<<static_cast<unsigned>(blocks), kDThreads, 0, s>>>(values, starts, nruns, offset,
+                                                                                  count, out);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+namespace {
+thread_local DevBuf t_derr;
+int* derr(cudaStream_t s) {
+    if (!t_derr.p) {
+        t_derr = DevBuf(16);
+        if (t_derr.p) cudaMemsetAsync(t_derr.p, 0, 16, s);
+    }
+    return t_derr.as<int>();
+}
+int check(int* e, cudaStream_t s) {
+    int h = 0;
+    if (int st = d2h(&h, e, 4, s)) return st;
+    if (int st = sync(s)) return st;
+    if (h) {
+        cudaMemsetAsync(e, 0, 4, s);
+        if (h & 4) { set_error(kErrDeviceTimeout, "a device-side wait ran out of budget"); return kErrDeviceTimeout; }
+        set_error(kErrInvalidArg, "an index is outside the dictionary");
+        return kErrInvalidArg;
+    }
+    return kOk;
+}
+}  // namespace
+
+extern "C" {
+
+int voxel_bitpack_decode_dev(const uint64_t* d_words, size_t nwords, uint32_t width, size_t value_count,
+                             size_t offset, size_t count, uint32_t* d_out, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    return launch_bitunpack(d_words, nwords, width, value_count, offset, count, d_out, s);
+}
+
+int voxel_bitpack_decode(const uint64_t* words, size_t nwords, uint32_t width, size_t value_count, size_t offset,
+                         size_t count, uint32_t* out) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = thread_stream();
+    uint64_t n = offset < value_count ? (count < value_count - offset ? count : value_count - offset) : 0;
+    DevBuf dw(nwords * 8), o(n * 4);
+    if (!dw.ok(nwords * 8) || !o.ok(n * 4)) return kErrOutOfMemory;
+    if (int st = h2d(dw.p, words, nwords * 8, s)) return st;
+    if (int st = launch_bitunpack(dw.as<uint64_t>(), nwords, width, value_count, offset, count, o.as<uint32_t>(), s))
+        return st;
+    if (int st = d2h(out, o.p, n * 4, s)) return st;
+    return sync(s);
+}
+
+int voxel_dict_bitpack_decode_i32(const uint64_t* words, size_t nwords, uint32_t width, const int32_t* dict,
+                                  size_t card, size_t value_count, size_t offset, size_t count, int32_t* out) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = thread_stream();
+    uint64_t n = offset < value_count ? (count < value_count - offset ? count : value_count - offset) : 0;
+    DevBuf dw(nwords * 8), dd(card * 4), o(n * 4);
+    if (!dw.ok(nwords * 8) || !dd.ok(card * 4) || !o.ok(n * 4)) return kErrOutOfMemory;
+    if (int st = h2d(dw.p, words, nwords * 8, s)) return st;
+    if (int st = h2d(dd.p, dict, card * 4, s)) return st;
+    int* e = derr(s);
+    if (int st = launch_dict_bitunpack_i32(dw.as<uint64_t>(), nwords, width, dd.as<int32_t>(),
+                                           static_cast<uint32_t>(card), value_count, offset, count, o.as<int32_t>(),
+                                           e, s))
+        return st;
+    if (int st = d2h(out, o.p, n * 4, s)) return st;
+    return check(e, s);
+}
+
+int voxel_dict_decode(int dtype, const void* dict, size_t card, const uint32_t* indices, size_t n, size_t offset,
+                      size_t count, void* out) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = thread_stream();
+    uint64_t m = offset < n ? (count < n - offset ? count : n - offset) : 0;  // encoding.hpp:163-166
+    size_t es = dtype_size(dtype);
+    DevBuf dd(card * es), di(m * 4), o(m * es);
+    if (!dd.ok(card * es) || !di.ok(m * 4) || !o.ok(m * es)) return kErrOutOfMemory;
+    if (int st = h2d(dd.p, dict, card * es, s)) return st;
+    if (int st = h2d(di.p, indices + offset, m * 4, s)) return st;
+    int* e = derr(s);
+    if (int st = launch_dict_gather(dtype, dd.p, static_cast<uint32_t>(card), di.as<uint32_t>(), m, o.p, e, s))
+        return st;
+    if (int st = d2h(out, o.p, m * es, s)) return st;
+    return check(e, s);
+}
+
+int voxel_rle_decode_i64_dev(const int64_t* d_values, const uint32_t* d_runs, size_t nruns, size_t offset,
+                             size_t count, int64_t* d_out, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    static thread_local DevBuf scratch;
+    size_t need = rle_scratch_bytes(nruns);
+    if (scratch.n < need) {
+        scratch = DevBuf(need);
+        if (!scratch.p) return kErrOutOfMemory;
+    }
+    int* e = derr(s);
+    if (int st = launch_rle_decode_i64(d_values, d_runs, nruns, offset, count, d_out, scratch.p, e, s)) return st;
+    return kOk;
+}
+
+int voxel_rle_decode_i64(const int64_t* values, const uint32_t* runs, size_t nruns, size_t offset, size_t count,
+                         int64_t* out) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = thread_stream();
+    DevBuf dv(nruns * 8), dr(nruns * 4), o(count * 8);
+    if (!dv.ok(nruns * 8) || !dr.ok(nruns * 4) || !o.ok(count * 8)) return kErrOutOfMemory;
+    if (int st = h2d(dv.p, values, nruns * 8, s)) return st;
+    if (int st = h2d(dr.p, runs, nruns * 4, s)) return st;
+    if (int st = voxel_rle_decode_i64_dev(dv.as<int64_t>(), dr.as<uint32_t>(), nruns, offset, count, o.as<int64_t>(),
+                                          s))
+        return st;
+    if (int st = d2h(out, o.p, count * 8, s)) return st;
+    return check(derr(s), s);
+}
+
+}  // extern "C"

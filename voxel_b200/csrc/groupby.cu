@@ -1,0 +1,478 @@
+// Fused scan + group-by over a dictionary-encoded, bit-packed key column.
+//
+// Reference composition this replaces (all single-threaded CPU operators):
+//   BitPackedEncoding::DecodeBatch -> DictionaryEncoding lookup
+//     (include/voxel/data/encoding.hpp:397-422, 156-167)
+//   VectorFilter<f64>::ApplyGT, VectorFilter<i32>::ApplyBetween, ColumnFilter::AndWith
+//     (include/voxel/ops/filter.hpp:42-78, 255-288, 526-547)
+//   SelectionVector::BuildFromBitmap + gather (filter.hpp:378-399)
+//   HashAggregator<i32,f64>::Accumulate / Finalize (include/voxel/ops/aggregate.hpp:159-261)
+//
+// B200 design: one pass over the three columns, nothing materialised.  The
+// reference's dictionary is sorted and unique, so a row's dictionary index is
+// already a dense group id in key order: no hash table is needed.  Each block
+// keeps a shared-memory table of per-group state and runs barrier-free over
+// its tiles (each thread reads its rows' key bits straight through L1).  A
+// passing row costs two shared atomics in the common case: its exact
+// fixed-point value (LSB 2^-76) shifted left 20 bits with the row count in the
+// low 20 bits goes into a 192-bit accumulator, so SUM and COUNT share words;
+// MIN/MAX (as order keys) are only touched when they improve.  Blocks flush to
+// a global table (exact 192-bit sums, u64 counts) before 2^20 rows could wrap
+// the embedded count, and the last block to finish converts the global table
+// to sorted output rows and resets it for the next launch.
+#include <cstdio>
+
+#include "fixedpoint.cuh"
+#include "groupby.h"
+#include "voxel_c.h"
+#include "vx_common.cuh"
+#include "vx_runtime.h"
+
+namespace vx {
+
+namespace {
+
+constexpr int kGbThreads = 512;
+constexpr int kCountBits = 20;
+constexpr int kFixScale = 76;  // LSB weight 2^-76 of the group sums
+constexpr int kMaxWidth = 32;
+
+struct GlobalGroups {
+    unsigned long long* sum;  // 3 words per group, LSB 2^-76
+    unsigned long long* cnt;
+    unsigned long long* mn;   // order keys
+    unsigned long long* mx;
+};
+
+// x -> 192-bit fixed point with LSB 2^-S (|x| < 2^63); *bad on NaN / inf / overflow
+template <int S>
+__device__ __forceinline__ Fix3 fix_from_double_s(double x, bool* bad) {
+    uint64_t b = static_cast<uint64_t>(__double_as_longlong(x));
+    int ex = static_cast<int>((b >> 52) & 0x7FF);
+    Fix3 r{0, 0, 0};
+    if (ex == 0x7FF) { *bad = true; return r; }
+    if (ex == 0) return r;
+    uint64_t m = (b & ((1ull << 52) - 1)) | (1ull << 52);
+    int s = ex - 1075 + S;
+    if (ex >= 1023 + 63) { *bad = true; return r; }
+    if (s < 0) {
+        if (s > -64) r.w0 = m >> (-s);
+    } else if (s < 64) {
+        r.w0 = m << s;
+        r.w1 = s ? (m >> (64 - s)) : 0;
+    } else if (s < 128) {
+        int t = s - 64;
+        r.w1 = m << t;
+        r.w2 = t ? (m >> (64 - t)) : 0;
+    } else {
+        r.w2 = m << (s - 128);
+    }
+    if (b >> 63) {
+        r.w0 = ~r.w0; r.w1 = ~r.w1; r.w2 = ~r.w2;
+        r.w0 += 1;
+        if (r.w0 == 0) { r.w1 += 1; if (r.w1 == 0) r.w2 += 1; }
+    }
+    return r;
+}
+
+// (F << 20) | 1 : the value and one row, packed for a single 192-bit add
+__device__ __forceinline__ Fix3 pack_row(const Fix3& f) {
+    Fix3 v;
+    v.w0 = (f.w0 << kCountBits) | 1ull;
+    v.w1 = (f.w1 << kCountBits) | (f.w0 >> (64 - kCountBits));
+    v.w2 = (f.w2 << kCountBits) | (f.w1 >> (64 - kCountBits));
+    return v;
+}
+
+// accumulator -> (value with LSB 2^-76, count)
+__device__ __forceinline__ Fix3 unpack_sum(Fix3 x, unsigned int* count) {
+    *count = static_cast<unsigned int>(x.w0 & ((1ull << kCountBits) - 1));
+    x.w0 -= *count;
+    Fix3 f;
+    f.w0 = (x.w0 >> kCountBits) | (x.w1 << (64 - kCountBits));
+    f.w1 = (x.w1 >> kCountBits) | (x.w2 << (64 - kCountBits));
+    f.w2 = static_cast<uint64_t>(static_cast<int64_t>(x.w2) >> kCountBits);
+    return f;
+}
+
+__device__ __forceinline__ uint32_t key_bits(const uint64_t* __restrict__ packed, uint64_t row, uint32_t w,
+                                             uint64_t mask) {
+    uint64_t bit = row * w;
+    uint64_t wi = bit >> 6;
+    uint32_t sh = static_cast<uint32_t>(bit & 63);
+    uint64_t v = __ldg(packed + wi) >> sh;
+    if (sh + w > 64) v |= __ldg(packed + wi + 1) << (64 - sh);
+    return static_cast<uint32_t>(v & mask);
+}
+
+// Per-warp queue of passing rows (ballot compaction): the atomic path then runs
+// with all 32 lanes converged instead of once per 32-row slice with ~6 lanes.
+constexpr int kQueue = 64;
+struct WarpQueue {
+    uint32_t gid[kQueue];
+    double val[kQueue];
+    double price[kQueue];
+};
+
+template <int RPT>
+__global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
+    const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
+    const double* __restrict__ price, const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo,
+    int32_t qhi, GlobalGroups g, unsigned int* done, int32_t* out_keys, double* out_sum, double* out_min,
+    double* out_max, uint64_t* out_count, uint64_t* out_ngroups, int* status) {
+    constexpr int kTile = kGbThreads * RPT;
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem);  // 3 words per group
+    unsigned long long* s_mn = s_acc + 3 * card;
+    unsigned long long* s_mx = s_mn + card;
+
+    auto reset_table = [&]() {
+        for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+            s_acc[3 * i] = 0;
+            s_acc[3 * i + 1] = 0;
+            s_acc[3 * i + 2] = 0;
+            s_mn[i] = ~0ull;
+            s_mx[i] = 0;
+        }
+    };
+    auto flush_table = [&]() {
+        for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+            Fix3 x{s_acc[3 * i], s_acc[3 * i + 1], s_acc[3 * i + 2]};
+            unsigned int c;
+            Fix3 f = unpack_sum(x, &c);
+            if (!c) continue;
+            fix_atomic_add(&g.sum[3 * i], f);
+            atomicAdd(&g.cnt[i], static_cast<unsigned long long>(c));
+            atomicMin(&g.mn[i], s_mn[i]);
+            atomicMax(&g.mx[i], s_mx[i]);
+        }
+    };
+
+    reset_table();
+    __syncthreads();
+    const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    // embedded counts stay below 2^20 per group between flushes
+    const uint64_t tiles_per_flush = ((1ull << kCountBits) - 1) / kTile;
+    bool bad_value = false, bad_key = false;
+    uint64_t since_flush = 0;
+
+    __shared__ WarpQueue s_queue[kGbThreads / 32];
+    const int lane = threadIdx.x & 31;
+    const unsigned lanemask_lt = (1u << lane) - 1;
+    WarpQueue& Q = s_queue[threadIdx.x >> 5];
+    int qn = 0;  // warp-uniform fill of Q
+    // lanes < cnt fold queue entry `lane` into the block table, converged
+    auto consume = [&](int cnt) {
+        if (lane < cnt) {
+            uint32_t gi = Q.gid[lane];
+            if (gi >= card) {
+                bad_key = true;
+            } else {
+                double p = Q.price[lane];
+                fix_atomic_add(&s_acc[3 * gi], pack_row(fix_from_double_s<kFixScale>(Q.val[lane], &bad_value)));
+                uint64_t ok = f64_order_key(p);
+                if (ok < s_mn[gi]) atomicMin(&s_mn[gi], static_cast<unsigned long long>(ok));
+                if (ok > s_mx[gi]) atomicMax(&s_mx[gi], static_cast<unsigned long long>(ok));
+            }
+        }
+    };
+
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (since_flush == tiles_per_flush) {
+            __syncwarp();
+            consume(qn);
+            qn = 0;
+            __syncthreads();
+            flush_table();
+            __syncthreads();
+            reset_table();
+            __syncthreads();
+            since_flush = 0;
+        }
+        ++since_flush;
+        const uint64_t r0 = t * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
+        double pv[RPT];
+        int32_t qv[RPT];
+        if (r0 + RPT <= n) {
+#pragma unroll
+            for (int k = 0; k < RPT; k += 4) {
+                const double2* pp = reinterpret_cast<const double2*>(price + r0 + k);
+                double2 a = __ldcs(pp), b = __ldcs(pp + 1);
+                int4 q = __ldcs(reinterpret_cast<const int4*>(qty + r0 + k));
+                pv[k] = a.x; pv[k + 1] = a.y; pv[k + 2] = b.x; pv[k + 3] = b.y;
+                qv[k] = q.x; qv[k + 1] = q.y; qv[k + 2] = q.z; qv[k + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                bool in = r0 + k < n;
+                pv[k] = in ? price[r0 + k] : 0.0;
+                qv[k] = in ? qty[r0 + k] : 0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            uint64_t r = r0 + k;
+            double p = pv[k];
+            int32_t q = qv[k];
+            bool pass = r < n && p > pthr && q >= qlo && q <= qhi;
+            unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) {
+                uint32_t gi = key_bits(packed, r, width, mask);
+                int pos = qn + __popc(m & lanemask_lt);
+                Q.gid[pos] = gi;
+                // one rounded multiply, as the reference materialises price*qty
+                Q.val[pos] = __dmul_rn(p, static_cast<double>(q));
+                Q.price[pos] = p;
+            }
+            qn += __popc(m);
+            if (qn >= 32) {
+                __syncwarp();
+                consume(32);
+                __syncwarp();
+                if (lane < qn - 32) {
+                    Q.gid[lane] = Q.gid[32 + lane];
+                    Q.val[lane] = Q.val[32 + lane];
+                    Q.price[lane] = Q.price[32 + lane];
+                }
+                __syncwarp();
+                qn -= 32;
+            }
+        }
+    }
+    __syncwarp();
+    consume(qn);
+    if (bad_value) atomicOr(status, 1);
+    if (bad_key) atomicOr(status, 2);
+    __syncthreads();
+    flush_table();
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+
+    // last block: compact non-empty groups in key (= dictionary index) order
+    __shared__ unsigned int s_scan[kGbThreads];
+    uint32_t per = (card + blockDim.x - 1) / blockDim.x;
+    uint32_t lo = threadIdx.x * per < card ? threadIdx.x * per : card;
+    uint32_t hi = lo + per < card ? lo + per : card;
+    unsigned int mine = 0;
+    for (uint32_t i = lo; i < hi; ++i) mine += __ldcg(&g.cnt[i]) ? 1 : 0;
+    s_scan[threadIdx.x] = mine;
+    __syncthreads();
+    for (int d = 1; d < kGbThreads; d <<= 1) {
+        unsigned int v = threadIdx.x >= static_cast<unsigned>(d) ? s_scan[threadIdx.x - d] : 0;
+        __syncthreads();
+        s_scan[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned int pos = s_scan[threadIdx.x] - mine;
+    for (uint32_t i = lo; i < hi; ++i) {
+        unsigned long long c = __ldcg(&g.cnt[i]);
+        if (c) {
+            Fix3 f{__ldcg(&g.sum[3 * i]), __ldcg(&g.sum[3 * i + 1]), __ldcg(&g.sum[3 * i + 2])};
+            out_keys[pos] = dict[i];
+            out_sum[pos] = fix_to_double_s<kFixScale>(f);
+            out_min[pos] = f64_from_order_key(__ldcg(&g.mn[i]));
+            out_max[pos] = f64_from_order_key(__ldcg(&g.mx[i]));
+            out_count[pos] = c;
+            ++pos;
+        }
+        g.sum[3 * i] = 0;
+        g.sum[3 * i + 1] = 0;
+        g.sum[3 * i + 2] = 0;
+        g.cnt[i] = 0;
+        g.mn[i] = ~0ull;
+        g.mx[i] = 0;
+    }
+    if (threadIdx.x == blockDim.x - 1) {
+        *out_ngroups = s_scan[threadIdx.x];
+        *done = 0;
+    }
+}
+
+__global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* done) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < card; i += gridDim.x * blockDim.x) {
+        g.sum[3 * i] = 0;
+        g.sum[3 * i + 1] = 0;
+        g.sum[3 * i + 2] = 0;
+        g.cnt[i] = 0;
+        g.mn[i] = ~0ull;
+        g.mx[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *done = 0;
+}
+
+size_t table_bytes(uint32_t card) { return static_cast<size_t>(card) * 6 * 8 + 256; }
+
+template <int RPT>
+int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+               const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+               int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
+    constexpr int kTile = kGbThreads * RPT;
+    size_t smem = scan_groupby_smem_bytes(card);
+    static thread_local uint32_t attr_set_for = 0;
+    if (attr_set_for < card) {
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
+        attr_set_for = kMaxGroups;
+    }
+    int per_sm = 0;
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_groupby_kernel<RPT>, kGbThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t ntiles = (n + kTile - 1) / kTile;
+    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (grid < 1) grid = 1;
+    GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
+    scan_groupby_kernel<RPT><<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
+        packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, S.g_done, ok, os, omn, omx, oc, ong,
+        static_cast<int*>(S.status.p));
+    VX_CUDA(cudaGetLastError());
+    S.last_grid = static_cast<int>(grid);
+    return kOk;
+}
+
+}  // namespace
+
+size_t scan_groupby_smem_bytes(uint32_t card) { return static_cast<size_t>(card) * 5 * 8 + 16; }
+
+int ScanGroupBy::prepare(uint32_t card, cudaStream_t s) {
+    if (card == 0 || card > kMaxGroups) {
+        set_error(kErrInvalidArg, "dictionary cardinality %u outside 1..%u", card, kMaxGroups);
+        return kErrInvalidArg;
+    }
+    if (card_ != card) {
+        table = DevBuf(table_bytes(card));
+        status = DevBuf(16);
+        if (!table.p || !status.p) return kErrOutOfMemory;
+        card_ = card;
+        char* b = static_cast<char*>(table.p);
+        g_sum = reinterpret_cast<unsigned long long*>(b);
+        g_cnt = g_sum + 3 * card;
+        g_mn = g_cnt + card;
+        g_mx = g_mn + card;
+        g_done = reinterpret_cast<unsigned int*>(g_mx + card);
+        GlobalGroups g{g_sum, g_cnt, g_mn, g_mx};
+        init_groups_kernel<<<(card + 255) / 256, 256, 0, s>>>(g, card, g_done);
+        VX_CUDA(cudaGetLastError());
+        VX_CUDA(cudaMemsetAsync(status.p, 0, 16, s));
+    }
+    return kOk;
+}
+
+int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+                        const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo,
+                        int32_t qhi, int32_t* out_keys, double* out_sum, double* out_min, double* out_max,
+                        uint64_t* out_count, uint64_t* out_ngroups, cudaStream_t s) {
+    if (width == 0 || width > kMaxWidth) {
+        set_error(kErrInvalidArg, "bit width %u outside 1..%d", width, kMaxWidth);
+        return kErrInvalidArg;
+    }
+    if ((reinterpret_cast<uintptr_t>(price) | reinterpret_cast<uintptr_t>(qty)) & 15) {
+        set_error(kErrInvalidArg, "price / qty columns must be 16-byte aligned");
+        return kErrInvalidArg;
+    }
+    int st = prepare(card, s);
+    if (st) return st;
+    switch (rows_per_thread) {
+    case 8:
+        return launch_rpt<8>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
+                             out_min, out_max, out_count, out_ngroups, s);
+    case 16:
+        return launch_rpt<16>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
+                              out_min, out_max, out_count, out_ngroups, s);
+    default:
+        return launch_rpt<4>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
+                             out_min, out_max, out_count, out_ngroups, s);
+    }
+}
+
+int ScanGroupBy::check_status(cudaStream_t s) {
+    int h = 0;
+    int st = d2h(&h, status.p, sizeof(int), s);
+    if (st) return st;
+    st = sync(s);
+    if (st) return st;
+    if (h) {
+        cudaMemsetAsync(status.p, 0, 16, s);
+        if (h & 2) {
+            set_error(kErrInvalidArg, "a packed key index is outside the dictionary");
+            return kErrInvalidArg;
+        }
+        set_error(kErrOverflow, "a price*qty product is not finite or exceeds 2^63 in magnitude");
+        return kErrOverflow;
+    }
+    return kOk;
+}
+
+ScanGroupBy& scan_groupby_state() {
+    static thread_local ScanGroupBy s;
+    return s;
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t width, const int32_t* d_dict,
+                           size_t card, const double* d_price, const int32_t* d_qty, size_t n, double pthr,
+                           int32_t qlo, int32_t qhi, int32_t* d_keys, double* d_sum, double* d_min, double* d_max,
+                           uint64_t* d_count, uint64_t* d_ngroups, void* stream) {
+    clear_error();
+    int st = ensure_device();
+    if (st) return st;
+    if (nwords * 64 < n * static_cast<uint64_t>(width)) {
+        set_error(kErrInvalidArg, "packed key column has %zu words, %zu rows of %u bits need more", nwords, n, width);
+        return kErrInvalidArg;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    return scan_groupby_state().launch(d_packed, width, d_dict, static_cast<uint32_t>(card), d_price, d_qty, n, pthr,
+                                       qlo, qhi, d_keys, d_sum, d_min, d_max, d_count, d_ngroups, s);
+}
+
+int voxel_scan_groupby_tune(int rows_per_thread) {
+    if (rows_per_thread != 4 && rows_per_thread != 8 && rows_per_thread != 16) return kErrInvalidArg;
+    scan_groupby_state().rows_per_thread = rows_per_thread;
+    return kOk;
+}
+
+size_t voxel_scan_groupby(const uint64_t* packed, size_t nwords, uint32_t width, const int32_t* dict, size_t card,
+                          const double* price, const int32_t* qty, size_t n, double pthr, int32_t qlo, int32_t qhi,
+                          int32_t* out_keys, double* out_sum, double* out_min, double* out_max,
+                          uint64_t* out_count) {
+    clear_error();
+    if (ensure_device()) return static_cast<size_t>(-1);
+    cudaStream_t s = thread_stream();
+    size_t bytes_words = nwords * 8, bytes_price = n * 8, bytes_qty = n * 4, bytes_dict = card * 4;
+    DevBuf dw(bytes_words), dd(bytes_dict), dp(bytes_price), dq(bytes_qty);
+    DevBuf ok(card * 4), os(card * 8), omn(card * 8), omx(card * 8), oc(card * 8), ong(8);
+    if (!dw.ok(bytes_words) || !dd.ok(bytes_dict) || !dp.ok(bytes_price) || !dq.ok(bytes_qty) || !ok.p || !os.p ||
+        !omn.p || !omx.p || !oc.p || !ong.p)
+        return static_cast<size_t>(-1);
+    if (h2d(dw.p, packed, bytes_words, s) || h2d(dd.p, dict, bytes_dict, s) || h2d(dp.p, price, bytes_price, s) ||
+        h2d(dq.p, qty, bytes_qty, s))
+        return static_cast<size_t>(-1);
+    int st = voxel_scan_groupby_dev(dw.as<uint64_t>(), nwords, width, dd.as<int32_t>(), card, dp.as<double>(),
+                                    dq.as<int32_t>(), n, pthr, qlo, qhi, ok.as<int32_t>(), os.as<double>(),
+                                    omn.as<double>(), omx.as<double>(), oc.as<uint64_t>(), ong.as<uint64_t>(), s);
+    if (st) return static_cast<size_t>(-1);
+    if (scan_groupby_state().check_status(s)) return static_cast<size_t>(-1);
+    uint64_t ng = 0;
+    if (d2h(&ng, ong.p, 8, s) || sync(s)) return static_cast<size_t>(-1);
+    if (ng) {
+        if (d2h(out_keys, ok.p, ng * 4, s) || d2h(out_sum, os.p, ng * 8, s) || d2h(out_min, omn.p, ng * 8, s) ||
+            d2h(out_max, omx.p, ng * 8, s) || d2h(out_count, oc.p, ng * 8, s) || sync(s))
+            return static_cast<size_t>(-1);
+    }
+    return static_cast<size_t>(ng);
+}
+
+}  // extern "C"

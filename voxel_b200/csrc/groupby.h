@@ -1,0 +1,36 @@
+// Fused scan + group-by state (global group table, status word).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vx_runtime.h"
+
+namespace vx {
+
+// Largest dictionary the shared-memory group table holds.
+constexpr uint32_t kMaxGroups = 4096;
+
+size_t scan_groupby_smem_bytes(uint32_t card);
+
+struct ScanGroupBy {
+    DevBuf table, status;
+    uint32_t card_ = 0;
+    unsigned long long *g_sum = nullptr, *g_cnt = nullptr, *g_mn = nullptr, *g_mx = nullptr;
+    unsigned int* g_done = nullptr;
+    int rows_per_thread = 8;  // autotuned per shape: 4, 8 or 16
+    int last_grid = 0;
+
+    int prepare(uint32_t card, cudaStream_t s);
+    int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
+               const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi, int32_t* out_keys,
+               double* out_sum, double* out_min, double* out_max, uint64_t* out_count, uint64_t* out_ngroups,
+               cudaStream_t s);
+    // reads (and clears) the kernel's status word; synchronises the stream
+    int check_status(cudaStream_t s);
+};
+
+ScanGroupBy& scan_groupby_state();
+
+}  // namespace vx

@@ -1,0 +1,727 @@
+// Remaining reference operators behind the C ABI, on the GPU:
+//
+//   HashAggregator<u32,f64> (include/voxel/ops/aggregate.hpp:159-301) as the
+//     voxel_agg_* object and the one-shot voxel_groupby_*: a device
+//     open-addressing table keyed by 64-bit slot words (key << 32 | 1, claimed
+//     with one CAS, so a key is published atomically), grown by doubling when a
+//     batch would push the load past 0.75 (the reference's limit); per-group
+//     state is an exact fixed-point SUM, COUNT, MIN/MAX.  A batch first inserts
+//     its keys (idempotent, retried after a grow), then accumulates its values.
+//   GroupedAggregator::AccumulateSorted / FinalizeGroups (aggregate.hpp:665-706):
+//     runs of equal keys are reduced with a warp segmented scan and one set of
+//     atomics per warp segment.
+//   SortOperator::SortAscending / SortDescending (sort.hpp:504-541, a stable
+//     merge sort on f64 returning indices) and TopKSelect (490-502): the radix
+//     sort on order-preserving u64 images of the values (-0.0 folded into +0.0 so
+//     equal values keep their input order).
+//   DictionaryEncoding<f64>::Build / DecodeBatch (encoding.hpp:113-167).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "fixedpoint.cuh"
+#include "radix.h"
+#include "voxel_c.h"
+#include "vx_common.cuh"
+#include "vx_runtime.h"
+#include "vx_scan.cuh"
+
+namespace vx {
+
+namespace {
+
+constexpr int kOThreads = 256;
+
+int ogrid(uint64_t n, int per_sm = 8) {
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = (n + kOThreads - 1) / kOThreads;
+    uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : static_cast<int>(b);
+}
+
+__device__ __forceinline__ uint32_t hash32(uint32_t k) {
+    // murmur3 fmix64 on the widened key, the mixer HashValue<u32> uses (ops/hash.hpp:334-339)
+    uint64_t x = k;
+    x = (x ^ (x >> 33)) * 0xff51afd7ed558ccdull;
+    x = (x ^ (x >> 33)) * 0xc4ceb9fe1a85ec53ull;
+    return static_cast<uint32_t>(x ^ (x >> 33));
+}
+
+struct Table {
+    unsigned long long* slot;  // 0 = empty, else (key << 32) | 1
+    unsigned long long* sum;   // 3 words per slot
+    unsigned long long* cnt;
+    unsigned long long* mn;
+    unsigned long long* mx;
+    uint64_t mask;
+};
+
+__global__ void table_init_kernel(Table t) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= t.mask;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        t.slot[i] = 0;
+        t.sum[3 * i] = 0;
+        t.sum[3 * i + 1] = 0;
+        t.sum[3 * i + 2] = 0;
+        t.cnt[i] = 0;
+        t.mn[i] = ~0ull;
+        t.mx[i] = 0;
+    }
+}
+
+// phase 1: make sure every key has a slot; counts new groups; flags overflow
+__global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, uint64_t n,
+                                   unsigned long long* groups, uint64_t limit, int* overflow) {
+    unsigned int added = 0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t k = keys[i];
+        unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
+        uint64_t h = hash32(k) & t.mask;
+        for (uint64_t p = 0;; ++p) {
+            unsigned long long cur = t.slot[h];
+            if (cur == want) break;
+            if (cur == 0) {
+                unsigned long long old = atomicCAS(&t.slot[h], 0ull, want);
+                if (old == 0) { ++added; break; }
+                if (old == want) break;
+            }
+            h = (h + 1) & t.mask;
+            if (p > t.mask) { atomicOr(overflow, 1); break; }
+        }
+    }
+    if (added) {
+        unsigned long long g = atomicAdd(groups, static_cast<unsigned long long>(added)) + added;
+        if (g > limit) atomicOr(overflow, 1);
+    }
+}
+
+__device__ __forceinline__ uint64_t find_slot(const Table& t, uint32_t k) {
+    unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
+    uint64_t h = hash32(k) & t.mask;
+    for (uint64_t p = 0; p <= t.mask; ++p) {
+        unsigned long long cur = __ldg(t.slot + h);
+        if (cur == want) return h;
+        if (cur == 0) return ~0ull;
+        h = (h + 1) & t.mask;
+    }
+    return ~0ull;
+}
+
+// phase 2: fold values into their groups (keys all present)
+__global__ void accumulate_kernel(Table t, const uint32_t* __restrict__ keys, const double* __restrict__ vals,
+                                  uint64_t n, int* err) {
+    bool bad = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t s = find_slot(t, keys[i]);
+        if (s == ~0ull) { bad = true; continue; }
+        double v = vals[i];
+        fix_atomic_add(&t.sum[3 * s], fix_from_double(v, &bad));
+        atomicAdd(&t.cnt[s], 1ull);
+        uint64_t ok = f64_order_key(v);
+        if (ok < t.mn[s]) atomicMin(&t.mn[s], static_cast<unsigned long long>(ok));
+        if (ok > t.mx[s]) atomicMax(&t.mx[s], static_cast<unsigned long long>(ok));
+    }
+    if (bad) atomicOr(err, 1);
+}
+
+// move every occupied slot of `from` into `to` (a grow)
+__global__ void rehash_kernel(Table from, Table to) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= from.mask;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        unsigned long long w = from.slot[i];
+        if (!w) continue;
+        uint32_t k = static_cast<uint32_t>(w >> 32);
+        uint64_t h = hash32(k) & to.mask;
+        for (;;) {
+            if (atomicCAS(&to.slot[h], 0ull, w) == 0ull) break;
+            h = (h + 1) & to.mask;
+        }
+        to.sum[3 * h] = from.sum[3 * i];
+        to.sum[3 * h + 1] = from.sum[3 * i + 1];
+        to.sum[3 * h + 2] = from.sum[3 * i + 2];
+        to.cnt[h] = from.cnt[i];
+        to.mn[h] = from.mn[i];
+        to.mx[h] = from.mx[i];
+    }
+}
+
+// occupied slots -> (key image for sorting, slot id)
+__global__ void collect_kernel(Table t, int key_signed, uint32_t* out_key, uint32_t* out_slot,
+                               unsigned long long* n) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= t.mask;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        unsigned long long w = t.slot[i];
+        if (!w) continue;
+        unsigned long long p = atomicAdd(n, 1ull);
+        out_key[p] = static_cast<uint32_t>(w >> 32);
+        out_slot[p] = static_cast<uint32_t>(i);
+    }
+    (void)key_signed;
+}
+
+__global__ void emit_groups_kernel(Table t, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sslot,
+                                   uint64_t g, uint32_t* okeys, double* osum, double* omin, double* omax,
+                                   uint64_t* ocount) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < g;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t s = sslot[j];
+        okeys[j] = skey[j];
+        Fix3 f{t.sum[3 * s], t.sum[3 * s + 1], t.sum[3 * s + 2]};
+        osum[j] = fix_to_double(f);
+        omin[j] = f64_from_order_key(t.mn[s]);
+        omax[j] = f64_from_order_key(t.mx[s]);
+        ocount[j] = t.cnt[s];
+    }
+}
+
+// ---- sorted (run-based) group-by ----------------------------------------------------
+
+__global__ void grouped_sorted_kernel(const int32_t* __restrict__ keys, const double* __restrict__ vals, uint64_t n,
+                                      const uint32_t* __restrict__ run_of, unsigned long long* sum,
+                                      unsigned long long* cnt, unsigned long long* mn, unsigned long long* mx,
+                                      int* err) {
+    const int lane = threadIdx.x & 31;
+    bool bad = false;
+    // warps take 32 consecutive rows; runs inside a warp are contiguous lane ranges
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ull; base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t i = base + lane;
+        bool in = i < n;
+        uint32_t r = in ? run_of[i] : 0xFFFFFFFFu;
+        double v = in ? vals[i] : 0.0;
+        Fix3 f = in ? fix_from_double(v, &bad) : Fix3{0, 0, 0};
+        uint64_t c = in ? 1 : 0;
+        uint64_t okey = f64_order_key(v);
+        uint64_t lo = in ? okey : ~0ull, hi = in ? okey : 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t rr = __shfl_up_sync(0xffffffffu, r, d);
+            Fix3 g;
+            g.w0 = __shfl_up_sync(0xffffffffu, f.w0, d);
+            g.w1 = __shfl_up_sync(0xffffffffu, f.w1, d);
+            g.w2 = __shfl_up_sync(0xffffffffu, f.w2, d);
+            uint64_t cc = __shfl_up_sync(0xffffffffu, c, d);
+            uint64_t l2 = __shfl_up_sync(0xffffffffu, lo, d);
+            uint64_t h2 = __shfl_up_sync(0xffffffffu, hi, d);
+            if (lane >= d && rr == r) {
+                fix_add(f, g);
+                c += cc;
+                lo = l2 < lo ? l2 : lo;
+                hi = h2 > hi ? h2 : hi;
+            }
+        }
+        uint32_t rn = __shfl_down_sync(0xffffffffu, r, 1);
+        bool tail = in && (lane == 31 || rn != r);
+        if (tail) {
+            fix_atomic_add(&sum[3 * static_cast<uint64_t>(r)], f);
+            atomicAdd(&cnt[r], static_cast<unsigned long long>(c));
+            atomicMin(&mn[r], static_cast<unsigned long long>(lo));
+            atomicMax(&mx[r], static_cast<unsigned long long>(hi));
+        }
+    }
+    if (bad) atomicOr(err, 1);
+    (void)keys;
+}
+
+__global__ void run_flags_kernel(const int32_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ flag) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        flag[i] = (i > 0 && keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+// inclusive scan of 0/1 flags -> run id per row (single pass, look-back)
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kOThreads * kScanItems;
+__global__ void __launch_bounds__(kOThreads) run_ids_kernel(const uint32_t* __restrict__ flag, uint64_t n,
+                                                            uint32_t* __restrict__ run, unsigned long long* status,
+                                                            unsigned int* ctr, int* err) {
+    __shared__ uint64_t s_tile, s_base;
+    __shared__ uint32_t s_warp[kOThreads / 32];
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        uint64_t tile = s_tile;
+        if (tile >= ntiles) break;
+        uint64_t r0 = tile * kScanTile + threadIdx.x * kScanItems;
+        uint32_t v[kScanItems], c = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            v[k] = r0 + k < n ? flag[r0 + k] : 0;
+            c += v[k];
+        }
+        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        uint32_t inc = c;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += y;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t x = lane < kOThreads / 32 ? s_warp[lane] : 0, t = x;
+            for (int d = 1; d < 32; d <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, t, d);
+                if (lane >= d) t += y;
+            }
+            if (lane < kOThreads / 32) s_warp[lane] = t - x;
+            if (lane == kOThreads / 32 - 1) s_base = lookback_exclusive(status, tile, t, err);
+        }
+        __syncthreads();
+        uint64_t pos = s_base + s_warp[warp] + (inc - c);
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            pos += v[k];
+            if (r0 + k < n) run[r0 + k] = static_cast<uint32_t>(pos);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void emit_runs_kernel(const int32_t* __restrict__ keys, const uint32_t* __restrict__ run, uint64_t n,
+                                 const unsigned long long* sum, const unsigned long long* cnt,
+                                 const unsigned long long* mn, const unsigned long long* mx, int32_t* okeys,
+                                 double* osum, double* omin, double* omax, uint64_t* ocount) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (i > 0 && run[i] == run[i - 1]) continue;
+        uint32_t r = run[i];
+        okeys[r] = keys[i];
+        Fix3 f{sum[3 * r], sum[3 * r + 1], sum[3 * r + 2]};
+        osum[r] = fix_to_double(f);
+        omin[r] = f64_from_order_key(mn[r]);
+        omax[r] = f64_from_order_key(mx[r]);
+        ocount[r] = cnt[r];
+    }
+}
+
+__global__ void init_runs_kernel(unsigned long long* sum, unsigned long long* cnt, unsigned long long* mn,
+                                 unsigned long long* mx, uint64_t g) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < g;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        sum[3 * i] = 0;
+        sum[3 * i + 1] = 0;
+        sum[3 * i + 2] = 0;
+        cnt[i] = 0;
+        mn[i] = ~0ull;
+        mx[i] = 0;
+    }
+}
+
+// ---- f64 sort keys -----------------------------------------------------------------
+
+__global__ void f64_sort_keys_kernel(const double* __restrict__ x, uint64_t n, int descending,
+                                     uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        double v = x[i];
+        if (v == 0.0) v = 0.0;  // -0.0 and +0.0 compare equal in the reference's merge
+        uint64_t k = f64_order_key(v);
+        key[i] = descending ? ~k : k;
+        idx[i] = static_cast<uint32_t>(i);
+    }
+}
+
+__global__ void gather_f64_kernel(const double* __restrict__ x, const uint32_t* __restrict__ idx, uint64_t k,
+                                  double* __restrict__ out) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < k;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = x[idx[i]];
+}
+
+// dictionary build: sorted (key, row) -> dictionary values + per-row indices
+__global__ void dict_heads_kernel(const uint64_t* __restrict__ skey, uint64_t n, uint32_t* __restrict__ flag) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        // NaN images never compare equal, like std::unordered_map<double> keys
+        uint64_t k = skey[i];
+        bool nan = (k >> 63) ? ((~k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull)
+                             : ((k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull);
+        flag[i] = (i > 0 && (skey[i] != skey[i - 1] || nan)) ? 1u : 0u;
+    }
+}
+
+__global__ void dict_emit_kernel(const double* __restrict__ x, const uint32_t* __restrict__ srow,
+                                 const uint32_t* __restrict__ run, uint64_t n, double* __restrict__ dict,
+                                 uint32_t* __restrict__ indices) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t r = run[i];
+        if (i == 0 || run[i - 1] != r) dict[r] = x[srow[i]];  // first occurrence's representation
+        indices[srow[i]] = r;
+    }
+}
+
+__global__ void f64_dict_gather_kernel(const double* __restrict__ dict, const uint32_t* __restrict__ idx,
+                                       uint64_t count, double* __restrict__ out) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = dict[idx[i]];
+}
+
+thread_local DevBuf t_oerr;
+int* oerr(cudaStream_t s) {
+    if (!t_oerr.p) {
+        t_oerr = DevBuf(16);
+        if (t_oerr.p) cudaMemsetAsync(t_oerr.p, 0, 16, s);
+    }
+    return t_oerr.as<int>();
+}
+int ocheck(cudaStream_t s, const char* what) {
+    int h = 0;
+    if (int st = d2h(&h, oerr(s), 4, s)) return st;
+    if (int st = sync(s)) return st;
+    if (h) {
+        cudaMemsetAsync(oerr(s), 0, 4, s);
+        if (h & 4) { set_error(kErrDeviceTimeout, "%s: a device-side wait ran out of budget", what); return kErrDeviceTimeout; }
+        set_error(kErrOverflow, "%s: a value is not finite or exceeds 2^63 in magnitude", what);
+        return kErrOverflow;
+    }
+    return kOk;
+}
+
+// sorted run ids for n rows of keys (flags + scan); returns #runs
+int run_ids(const int32_t* keys, uint64_t n, DevBuf& run, cudaStream_t s, uint64_t* nruns) {
+    DevBuf flag(n * 4 + 4);
+    run = DevBuf(n * 4 + 4);
+    uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    DevBuf scratch((ntiles + 1) * 8 + 64);
+    if (!flag.p || !run.p || !scratch.p) return kErrOutOfMemory;
+    run_flags_kernel<<<ogrid(n), kOThreads, 0, s>>>(keys, n, flag.as<uint32_t>());
+    VX_CUDA(cudaMemsetAsync(scratch.p, 0, scratch.n, s));
+    unsigned long long* status = scratch.as<unsigned long long>();
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(status + ntiles);
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = ntiles < static_cast<uint64_t>(sms) * 4 ? ntiles : static_cast<uint64_t>(sms) * 4;
+    run_ids_kernel<<<static_cast<unsigned>(b), kOThreads, 0, s>>>(flag.as<uint32_t>(), n, run.as<uint32_t>(), status,
+                                                                 ctr, oerr(s));
+    VX_CUDA(cudaGetLastError());
+    uint32_t last = 0;
+    if (int st = d2h(&last, run.as<uint32_t>() + (n - 1), 4, s)) return st;
+    if (int st = ocheck(s, "run scan")) return st;
+    *nruns = static_cast<uint64_t>(last) + 1;
+    return kOk;
+}
+
+}  // namespace
+
+// ---- device hash aggregator object ------------------------------------------------
+
+class HashAgg {
+public:
+    DevBuf mem;
+    Table t{};
+    uint64_t cap = 0, groups = 0;
+    DevBuf groups_d, flag_d;
+
+    int alloc_table(uint64_t c, Table& out, DevBuf& m, cudaStream_t s) {
+        size_t bytes = c * (8 + 24 + 8 + 8 + 8);
+        m = DevBuf(bytes);
+        if (!m.p) return kErrOutOfMemory;
+        char* b = static_cast<char*>(m.p);
+        out.slot = reinterpret_cast<unsigned long long*>(b);
+        out.sum = out.slot + c;
+        out.cnt = out.sum + 3 * c;
+        out.mn = out.cnt + c;
+        out.mx = out.mn + c;
+        out.mask = c - 1;
+        table_init_kernel<<<ogrid(c), kOThreads, 0, s>>>(out);
+        VX_CUDA(cudaGetLastError());
+        return kOk;
+    }
+
+    int init(uint64_t expected, cudaStream_t s) {
+        uint64_t c = 16;
+        while (c < expected * 2) c <<= 1;  // nextpow2(max(2*expected, 16)) (aggregate.hpp:160)
+        cap = c;
+        groups = 0;
+        if (!groups_d.p) groups_d = DevBuf(16);
+        if (!flag_d.p) flag_d = DevBuf(16);
+        if (!groups_d.p || !flag_d.p) return kErrOutOfMemory;
+        VX_CUDA(cudaMemsetAsync(groups_d.p, 0, 16, s));
+        return alloc_table(c, t, mem, s);
+    }
+
+    int grow(cudaStream_t s) {
+        Table nt{};
+        DevBuf nm;
+        if (int st = alloc_table(cap * 2, nt, nm, s)) return st;
+        rehash_kernel<<<ogrid(cap), kOThreads, 0, s>>>(t, nt);
+        VX_CUDA(cudaGetLastError());
+        mem = std::move(nm);
+        t = nt;
+        cap *= 2;
+        return kOk;
+    }
+
+    int accumulate(const uint32_t* dk, const double* dv, uint64_t n, cudaStream_t s) {
+        if (!mem.p) if (int st = init(16, s)) return st;
+        if (!n) return kOk;
+        // phase 1: insert keys, growing until every key fits under load 0.75
+        for (int attempt = 0; attempt < 40; ++attempt) {
+            VX_CUDA(cudaMemsetAsync(flag_d.p, 0, 4, s));
+            uint64_t limit = cap * 3 / 4;
+            insert_keys_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, n, groups_d.as<unsigned long long>(), limit,
+                                                              flag_d.as<int>());
+            VX_CUDA(cudaGetLastError());
+            int ovf = 0;
+            uint64_t g = 0;
+            if (int st = d2h(&ovf, flag_d.p, 4, s)) return st;
+            if (int st = d2h(&g, groups_d.p, 8, s)) return st;
+            if (int st = sync(s)) return st;
+            groups = g;
+            if (!ovf) break;
+            if (int st = grow(s)) return st;
+        }
+        accumulate_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, dv, n, oerr(s));
+        VX_CUDA(cudaGetLastError());
+        return ocheck(s, "group-by");
+    }
+
+    // groups sorted by key (key_signed: order as i32)
+    int results(int key_signed, void* okeys, double* osum, double* omin, double* omax, uint64_t* ocount,
+                cudaStream_t s) {
+        if (!groups) return kOk;
+        DevBuf k(groups * 4 + 4), sl(groups * 4 + 4), n(8);
+        DevBuf ok(groups * 4), os(groups * 8), omn(groups * 8), omx(groups * 8), oc(groups * 8);
+        if (!k.p || !sl.p || !n.p || !ok.p || !os.p || !omn.p || !omx.p || !oc.p) return kErrOutOfMemory;
+        VX_CUDA(cudaMemsetAsync(n.p, 0, 8, s));
+        collect_kernel<<<ogrid(cap), kOThreads, 0, s>>>(t, key_signed, k.as<uint32_t>(), sl.as<uint32_t>(),
+                                                        n.as<unsigned long long>());
+        VX_CUDA(cudaGetLastError());
+        size_t tb = radix_tmp_bytes(key_signed ? I32 : U32, groups);
+        DevBuf tmp(tb);
+        if (!tmp.p) return kErrOutOfMemory;
+        if (int st = launch_radix_sort(key_signed ? I32 : U32, k.p, sl.as<uint32_t>(), groups, tmp.p, tb, radix_err(s),
+                                       s, nullptr))
+            return st;
+        emit_groups_kernel<<<ogrid(groups), kOThreads, 0, s>>>(t, k.as<uint32_t>(), sl.as<uint32_t>(), groups,
+                                                              ok.as<uint32_t>(), os.as<double>(), omn.as<double>(),
+                                                              omx.as<double>(), oc.as<uint64_t>());
+        VX_CUDA(cudaGetLastError());
+        if (int st = d2h(okeys, ok.p, groups * 4, s)) return st;
+        if (osum) if (int st = d2h(osum, os.p, groups * 8, s)) return st;
+        if (omin) if (int st = d2h(omin, omn.p, groups * 8, s)) return st;
+        if (omax) if (int st = d2h(omax, omx.p, groups * 8, s)) return st;
+        if (ocount) if (int st = d2h(ocount, oc.p, groups * 8, s)) return st;
+        return radix_check(s);
+    }
+};
+
+struct DictF64 {
+    DevBuf dict, indices;
+    uint64_t card = 0, n = 0;
+};
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+// ---- HashAggregator<u32,f64> (reference bindings/voxel_c.cpp:168-182) ----------------
+void* voxel_agg_create(void) { return new HashAgg(); }
+void voxel_agg_destroy(void* a) { delete static_cast<HashAgg*>(a); }
+void voxel_agg_init(void* a, size_t expected) {
+    clear_error();
+    if (ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    static_cast<HashAgg*>(a)->init(expected, s);
+    sync(s);
+}
+void voxel_agg_accumulate(void* a, const uint32_t* keys, const double* values, size_t n) {
+    clear_error();
+    if (ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    DevBuf dk(n * 4 + 4), dv(n * 8 + 8);
+    if (!dk.p || !dv.p) return;
+    if (h2d(dk.p, keys, n * 4, s) || h2d(dv.p, values, n * 8, s)) return;
+    static_cast<HashAgg*>(a)->accumulate(dk.as<uint32_t>(), dv.as<double>(), n, s);
+}
+size_t voxel_agg_group_count(const void* a) { return static_cast<const HashAgg*>(a)->groups; }
+int voxel_agg_accumulate_dev(void* a, const uint32_t* d_keys, const double* d_values, size_t n, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    return static_cast<HashAgg*>(a)->accumulate(d_keys, d_values, n, static_cast<cudaStream_t>(stream));
+}
+size_t voxel_agg_results(void* a, uint32_t* keys, double* sum, double* mn, double* mx, uint64_t* count) {
+    clear_error();
+    if (ensure_device()) return static_cast<size_t>(-1);
+    HashAgg* h = static_cast<HashAgg*>(a);
+    if (h->results(0, keys, sum, mn, mx, count, thread_stream())) return static_cast<size_t>(-1);
+    return h->groups;
+}
+
+size_t voxel_groupby_u32_f64(const uint32_t* keys, const double* values, size_t n, size_t expected,
+                             uint32_t* okeys, double* osum, double* omin, double* omax, uint64_t* ocount) {
+    clear_error();
+    if (ensure_device()) return static_cast<size_t>(-1);
+    cudaStream_t s = thread_stream();
+    HashAgg h;
+    if (h.init(expected, s)) return static_cast<size_t>(-1);
+    DevBuf dk(n * 4 + 4), dv(n * 8 + 8);
+    if (!dk.p || !dv.p) return static_cast<size_t>(-1);
+    if (h2d(dk.p, keys, n * 4, s) || h2d(dv.p, values, n * 8, s)) return static_cast<size_t>(-1);
+    if (h.accumulate(dk.as<uint32_t>(), dv.as<double>(), n, s)) return static_cast<size_t>(-1);
+    if (h.results(0, okeys, osum, omin, omax, ocount, s)) return static_cast<size_t>(-1);
+    return h.groups;
+}
+
+size_t voxel_groupby_i32_f64(const int32_t* keys, const double* values, size_t n, size_t expected, int32_t* okeys,
+                             double* osum, double* omin, double* omax, uint64_t* ocount) {
+    clear_error();
+    if (ensure_device()) return static_cast<size_t>(-1);
+    cudaStream_t s = thread_stream();
+    HashAgg h;
+    if (h.init(expected, s)) return static_cast<size_t>(-1);
+    DevBuf dk(n * 4 + 4), dv(n * 8 + 8);
+    if (!dk.p || !dv.p) return static_cast<size_t>(-1);
+    if (h2d(dk.p, keys, n * 4, s) || h2d(dv.p, values, n * 8, s)) return static_cast<size_t>(-1);
+    if (h.accumulate(dk.as<uint32_t>(), dv.as<double>(), n, s)) return static_cast<size_t>(-1);
+    if (h.results(1, okeys, osum, omin, omax, ocount, s)) return static_cast<size_t>(-1);
+    return h.groups;
+}
+
+size_t voxel_grouped_sorted_i32_f64(const int32_t* sorted_keys, const double* values, size_t n, int32_t* okeys,
+                                    double* osum, double* omin, double* omax, uint64_t* ocount) {
+    clear_error();
+    if (n == 0) return 0;
+    if (ensure_device()) return static_cast<size_t>(-1);
+    cudaStream_t s = thread_stream();
+    DevBuf dk(n * 4), dv(n * 8);
+    if (!dk.p || !dv.p) return static_cast<size_t>(-1);
+    if (h2d(dk.p, sorted_keys, n * 4, s) || h2d(dv.p, values, n * 8, s)) return static_cast<size_t>(-1);
+    DevBuf run;
+    uint64_t g = 0;
+    if (run_ids(dk.as<int32_t>(), n, run, s, &g)) return static_cast<size_t>(-1);
+    DevBuf st(g * 48), ok(g * 4), os(g * 8), omn(g * 8), omx(g * 8), oc(g * 8);
+    if (!st.p || !ok.p || !os.p || !omn.p || !omx.p || !oc.p) return static_cast<size_t>(-1);
+    unsigned long long* sum = st.as<unsigned long long>();
+    unsigned long long *cnt = sum + 3 * g, *mn = cnt + g, *mx = mn + g;
+    init_runs_kernel<<<ogrid(g), kOThreads, 0, s>>>(sum, cnt, mn, mx, g);
+    grouped_sorted_kernel<<<ogrid(n), kOThreads, 0, s>>>(dk.as<int32_t>(), dv.as<double>(), n, run.as<uint32_t>(),
+                                                         sum, cnt, mn, mx, oerr(s));
+    emit_runs_kernel<<<ogrid(n), kOThreads, 0, s>>>(dk.as<int32_t>(), run.as<uint32_t>(), n, sum, cnt, mn, mx,
+                                                    ok.as<int32_t>(), os.as<double>(), omn.as<double>(),
+                                                    omx.as<double>(), oc.as<uint64_t>());
+    if (cudaGetLastError() != cudaSuccess) return static_cast<size_t>(-1);
+    if (d2h(okeys, ok.p, g * 4, s) || d2h(osum, os.p, g * 8, s) || d2h(omin, omn.p, g * 8, s) ||
+        d2h(omax, omx.p, g * 8, s) || d2h(ocount, oc.p, g * 8, s))
+        return static_cast<size_t>(-1);
+    if (ocheck(s, "sorted group-by")) return static_cast<size_t>(-1);
+    return g;
+}
+
+// ---- SortOperator / TopK (reference bindings/voxel_c.cpp:187-203) ---------------------
+static int sort_f64_index(const double* data, size_t n, int desc, DevBuf& dx, DevBuf& keys, DevBuf& idx,
+                          cudaStream_t s) {
+    dx = DevBuf(n * 8);
+    keys = DevBuf(n * 8);
+    idx = DevBuf(n * 4);
+    if (!dx.p || !keys.p || !idx.p) return kErrOutOfMemory;
+    if (int st = h2d(dx.p, data, n * 8, s)) return st;
+    f64_sort_keys_kernel<<<ogrid(n), kOThreads, 0, s>>>(dx.as<double>(), n, desc, keys.as<uint64_t>(),
+                                                        idx.as<uint32_t>());
+    VX_CUDA(cudaGetLastError());
+    size_t tb = radix_tmp_bytes(U64, n);
+    DevBuf tmp(tb);
+    if (!tmp.p) return kErrOutOfMemory;
+    return launch_radix_sort(U64, keys.p, idx.as<uint32_t>(), n, tmp.p, tb, radix_err(s), s, nullptr);
+}
+
+static void sort_impl(const double* data, size_t n, uint32_t* out, int desc) {
+    clear_error();
+    if (n == 0) return;
+    if (n == 1) { out[0] = 0; return; }
+    if (ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    DevBuf dx, keys, idx;
+    if (sort_f64_index(data, n, desc, dx, keys, idx, s)) return;
+    if (d2h(out, idx.p, n * 4, s)) return;
+    radix_check(s);
+}
+
+void voxel_sort_ascending(const double* data, size_t n, uint32_t* out) { sort_impl(data, n, out, 0); }
+void voxel_sort_descending(const double* data, size_t n, uint32_t* out) { sort_impl(data, n, out, 1); }
+
+void voxel_topk(const double* data, size_t n, size_t k, double* out, int largest) {
+    clear_error();
+    if (k >= n) {  // sort.hpp:491: k >= count copies the input unchanged
+        if (n) std::memcpy(out, data, n * 8);
+        return;
+    }
+    if (ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    DevBuf dx, keys, idx;
+    if (sort_f64_index(data, n, largest ? 1 : 0, dx, keys, idx, s)) return;
+    DevBuf o(k * 8 + 8);
+    if (!o.p) return;
+    gather_f64_kernel<<<ogrid(k), kOThreads, 0, s>>>(dx.as<double>(), idx.as<uint32_t>(), k, o.as<double>());
+    if (d2h(out, o.p, k * 8, s)) return;
+    radix_check(s);
+}
+
+// ---- DictionaryEncoding<f64> (reference bindings/voxel_c.cpp:208-214) -----------------
+void* voxel_dict_create(void) { return new DictF64(); }
+void voxel_dict_destroy(void* d) { delete static_cast<DictF64*>(d); }
+void voxel_dict_build(void* h, const double* data, size_t n) {
+    clear_error();
+    DictF64* d = static_cast<DictF64*>(h);
+    d->card = 0;
+    d->n = n;
+    d->dict.reset();
+    d->indices.reset();
+    if (n == 0) return;
+    if (ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    DevBuf dx, keys, idx;
+    if (sort_f64_index(data, n, 0, dx, keys, idx, s)) return;
+    DevBuf flag(n * 4), run(n * 4);
+    uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    DevBuf scratch((ntiles + 1) * 8 + 64);
+    if (!flag.p || !run.p || !scratch.p) return;
+    dict_heads_kernel<<<ogrid(n), kOThreads, 0, s>>>(keys.as<uint64_t>(), n, flag.as<uint32_t>());
+    cudaMemsetAsync(scratch.p, 0, scratch.n, s);
+    unsigned long long* status = scratch.as<unsigned long long>();
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = ntiles < static_cast<uint64_t>(sms) * 4 ? ntiles : static_cast<uint64_t>(sms) * 4;
+    run_ids_kernel<<<static_cast<unsigned>(b), kOThreads, 0, s>>>(flag.as<uint32_t>(), n, run.as<uint32_t>(), status,
+                                                                 reinterpret_cast<unsigned int*>(status + ntiles),
+                                                                 oerr(s));
+    uint32_t last = 0;
+    if (d2h(&last, run.as<uint32_t>() + (n - 1), 4, s) || ocheck(s, "dictionary build")) return;
+    d->card = static_cast<uint64_t>(last) + 1;
+    d->dict = DevBuf(d->card * 8);
+    d->indices = DevBuf(n * 4);
+    if (!d->dict.p || !d->indices.p) return;
+    dict_emit_kernel<<<ogrid(n), kOThreads, 0, s>>>(dx.as<double>(), idx.as<uint32_t>(), run.as<uint32_t>(), n,
+                                                    d->dict.as<double>(), d->indices.as<uint32_t>());
+    sync(s);
+}
+size_t voxel_dict_cardinality(const void* h) { return static_cast<const DictF64*>(h)->card; }
+void voxel_dict_decode_batch(void* h, double* out, size_t offset, size_t count) {
+    clear_error();
+    DictF64* d = static_cast<DictF64*>(h);
+    if (offset >= d->n) return;
+    if (count > d->n - offset) count = d->n - offset;  // encoding.hpp:163
+    if (!count || ensure_device()) return;
+    cudaStream_t s = thread_stream();
+    DevBuf o(count * 8);
+    if (!o.p) return;
+    f64_dict_gather_kernel<<<ogrid(count), kOThreads, 0, s>>>(d->dict.as<double>(), d->indices.as<uint32_t>() + offset,
+                                                              count, o.as<double>());
+    if (d2h(out, o.p, count * 8, s)) return;
+    sync(s);
+}
+size_t voxel_dict_values(const void* h, double* out) {
+    const DictF64* d = static_cast<const DictF64*>(h);
+    if (d->card && out) {
+        cudaStream_t s = thread_stream();
+        if (d2h(out, d->dict.p, d->card * 8, s) || sync(s)) return static_cast<size_t>(-1);
+    }
+    return d->card;
+}
+
+}  // extern "C"
