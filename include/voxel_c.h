@@ -244,8 +244,11 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              const int32_t* qty, size_t n, double price_gt, int32_t qty_lo,
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
-/* rows each thread of the fused scan handles per tile (4, 8 or 16; tuning knob) */
-int       voxel_scan_groupby_tune(int rows_per_thread);
+/* kernel variant of the calling thread's fused scan: 0 = TMA-fed private warp
+ * tables (dictionaries up to 1024 entries), 4 (default) / 8 / 16 = shared-table
+ * atomics with that many rows per thread; and the variant the last call used */
+int       voxel_scan_groupby_tune(int variant);
+int       voxel_scan_groupby_last_variant(void);
 int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,
                                  const int32_t* d_dict, size_t card, const double* d_price,
                                  const int32_t* d_qty, size_t n, double price_gt, int32_t qty_lo,
@@ -300,6 +303,68 @@ int       voxel_hashjoin_i64_dev(const int64_t* d_build, const uint64_t* d_paylo
                                  const int64_t* d_probe, size_t np, uint32_t* d_left,
                                  uint32_t* d_right, size_t max_matches, int all,
                                  uint64_t* d_count_sum, void* stream);
+
+/* ================================================================
+ * Additive: batched persistent executor.  Many single-column filter /
+ * aggregate programs over device-resident columns run in ONE persistent
+ * launch (a device work queue of (program, tile) items), optionally replayed
+ * from a captured CUDA graph.  Each program can also emit its selection
+ * vector (ascending row ids satisfying all of its predicates) into a caller
+ * buffer of a given capacity; a program whose selection does not fit is
+ * flagged (its exact count is still reported) and can be re-run.
+ * ================================================================ */
+void*     voxel_batch_create(void);
+void      voxel_batch_destroy(void* batch);
+size_t    voxel_batch_size(const void* batch);
+/* regs64: the 64 registers before the run; returns a status */
+int       voxel_batch_add(void* batch, int dtype, const uint32_t* code, size_t len, const uint64_t* regs64,
+                          const void* d_col, size_t count, int want_selection, size_t sel_capacity,
+                          uint32_t* d_sel);
+int       voxel_batch_set_capacity(void* batch, size_t prog, size_t capacity, uint32_t* d_sel);
+int       voxel_batch_launch(void* batch, int use_graph, void* stream);
+int       voxel_batch_fetch(void* batch, void* stream);
+/* after fetch: the program's 64 registers, exact selected-row count, overflow flag */
+int       voxel_batch_result(const void* batch, size_t prog, uint64_t* regs64, uint64_t* sel_count,
+                             int* overflow);
+
+/* ================================================================
+ * Additive: learned cardinality / selectivity estimator.
+ * Column sketches are computed on the device (min / max, 64-bucket
+ * equi-width histogram, HyperLogLog p = 12); the FP32 MLP
+ * (48 -> 64 -> 64 -> 64 -> 2, 11,586 parameters) is trained and evaluated by
+ * the backend's own kernels.  Estimates only size buffers and pick plans.
+ * ================================================================ */
+typedef struct {
+    uint64_t n;
+    double min, max;
+    uint64_t hist[64];
+    uint8_t hll[4096];
+} voxel_column_sketch;
+
+/* up to 4 conjunctive "value op threshold" atoms (threshold as T bits) */
+typedef struct {
+    int32_t natoms;
+    int32_t op[4];
+    int32_t pad;
+    uint64_t thr[4];
+} voxel_pred_set;
+
+int       voxel_sketch_column_dev(int dtype, const void* d_col, size_t n, voxel_column_sketch* out);
+/* exact selected-row and distinct-selected-value counts for each predicate set */
+int       voxel_exact_labels_dev(int dtype, const void* d_col, size_t n, const voxel_pred_set* sets,
+                                 uint32_t nsets, uint64_t* rows, uint64_t* distinct);
+size_t    voxel_mlp_param_count(void);
+void*     voxel_mlp_create(uint64_t seed);
+void      voxel_mlp_destroy(void* mlp);
+int       voxel_mlp_set_params(void* mlp, const float* params);
+int       voxel_mlp_get_params(const void* mlp, float* params);
+/* gradient (summed over the samples) of the squared error and the loss, on the host */
+int       voxel_mlp_grad(void* mlp, const float* d_x, const float* d_y, const uint32_t* d_idx, uint32_t count,
+                         float* grad, float* loss);
+/* one Adam step on the minibatch d_idx[0..count) of (d_x [N x 48], d_y [N x 2]) */
+int       voxel_mlp_train_step(void* mlp, const float* d_x, const float* d_y, const uint32_t* d_idx,
+                               uint32_t count, float lr);
+int       voxel_mlp_infer(void* mlp, const float* d_x, size_t n, float* d_y, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,142 @@
+"""Batched persistent executor: many programs of mixed element types in one
+launch (and replayed from a CUDA graph) must reproduce each program run alone
+through the engine, the reference interpreter's registers (oracle), and the
+exact selection vector; undersized selection buffers are flagged with the
+exact count still reported."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from voxel_b200 import capi
+from voxel_b200 import templates as T
+from voxel_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+F64_RTOL = 1e-12
+
+
+def f64(b):
+    return np.array([b], np.uint64).view(np.float64)[0]
+
+
+def float_acc_regs(code):
+    out = set()
+    for c in code:
+        if c & 0xFF == 0x2A and ((c >> 8) & 0xF) in (((c >> 12) & 0xF), ((c >> 16) & 0xF)):
+            out.add((c >> 8) & 0xF)
+    return out
+
+
+def make_batch(progs, cols, caps, want=1):
+    L = capi.lib()
+    b = L.voxel_batch_create()
+    dev = torch.device("cuda", 0)
+    keep = []
+    for prog, col, cap in zip(progs, cols, caps):
+        dcol = torch.from_numpy(col).to(dev)
+        sel = torch.zeros(max(cap, 1), dtype=torch.int32, device=dev)
+        keep += [dcol, sel]
+        regs = np.array(prog.registers(col.size), np.uint64)
+        code = np.asarray(prog.code, np.uint32)
+        st = L.voxel_batch_add(b, prog.dtype, code.ctypes.data, code.size, regs.ctypes.data, dcol.data_ptr(), col.size,
+                               want, cap, sel.data_ptr())
+        assert st == 0, capi.last_error()
+    return b, keep
+
+
+def results(b, i):
+    L = capi.lib()
+    regs = np.zeros(64, np.uint64)
+    cnt = np.zeros(1, np.uint64)
+    ovf = np.zeros(1, np.int32)
+    assert L.voxel_batch_result(b, i, regs.ctypes.data, cnt.ctypes.data, ovf.ctypes.data) == 0
+    return [int(x) for x in regs], int(cnt[0]), int(ovf[0])
+
+
+def check_regs(dt, code, got, want, rtol=F64_RTOL):
+    facc = float_acc_regs(code) if dt in (0, 1) else set()
+    for r in range(16):
+        if got[r] != want[r]:
+            assert r in facc, (dt, r, got[r], want[r])
+            g, w = f64(got[r]), f64(want[r])
+            assert abs(g - w) <= rtol * max(abs(w), 1e-300)
+
+
+def test_batch_matches_engine_oracle_and_selection():
+    L = capi.lib()
+    rng = np.random.default_rng(41)
+    progs, cols, masks = [], [], []
+    for i in range(96):
+        dt = i % 6
+        n = int(T.K_LANES[dt] * rng.integers(1, 3000))
+        col = T.make_column(dt, n, rng)
+        prog = T.random_program(dt, rng)
+        progs.append(prog)
+        cols.append(col)
+        m = np.ones(n, bool)
+        for p in prog.preds:
+            v = np.float32(p.value) if dt == T.F32 else T.NP[dt](p.value)
+            m &= [np.equal, np.not_equal, np.less, np.less_equal, np.greater, np.greater_equal][p.op](col, v)
+        masks.append(m)
+    caps = [int(m.sum()) for m in masks]
+    b, keep = make_batch(progs, cols, caps)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    for use_graph in (0, 1, 1):
+        assert L.voxel_batch_launch(b, use_graph, stream.cuda_stream) == 0, capi.last_error()
+        assert L.voxel_batch_fetch(b, stream.cuda_stream) == 0, capi.last_error()
+        for i, (prog, col, m) in enumerate(zip(progs, cols, masks)):
+            regs, cnt, ovf = results(b, i)
+            assert cnt == int(m.sum()) and ovf == 0
+            sel = keep[2 * i + 1][:cnt].cpu().numpy().astype(np.int64)
+            assert (sel == np.flatnonzero(m)).all()
+            e = Engine(prog.dtype)
+            e.add_segment(col)
+            for r, v in enumerate(prog.registers(col.size)):
+                e.set_scalar(r, v)
+            e.load_program(prog.code)
+            e.run()
+            check_regs(prog.dtype, prog.code, regs, e.registers(16))
+            if prog.dtype != T.F32 and col.size <= 4000:
+                want = oracle.engine_run_ref(prog.dtype, prog.code, [col], prog.registers(col.size))
+                check_regs(prog.dtype, prog.code, regs, want)
+    L.voxel_batch_destroy(b)
+
+
+def test_batch_overflow_is_flagged_with_exact_count():
+    L = capi.lib()
+    rng = np.random.default_rng(42)
+    col = T.make_column(T.I32, 80_000, rng)
+    prog = T.build(T.I32, [T.Pred(2, 500)], "COUNT")  # ~50% of rows
+    want = int((col < 500).sum())
+    b, keep = make_batch([prog], [col], [want // 3])
+    assert L.voxel_batch_launch(b, 1, None) == 0 and L.voxel_batch_fetch(b, None) == 0
+    regs, cnt, ovf = results(b, 0)
+    assert ovf == 1 and cnt == want and regs[0] == want
+    sel = keep[1][: want // 3].cpu().numpy().astype(np.int64)
+    assert (sel == np.flatnonzero(col < 500)[: want // 3]).all()
+    L.voxel_batch_destroy(b)
+
+
+def test_batch_large_columns_properties():
+    """Two 2^26-row columns plus small ones in one launch: results equal the
+    single-program kernels (integers bit-exact, f64 within 1e-12)."""
+    L = capi.lib()
+    rng = np.random.default_rng(43)
+    progs, cols = [], []
+    for dt, n in ((T.F64, 1 << 26), (T.U32, 1 << 26), (T.I64, 1000), (T.F32, 8 * 12345)):
+        cols.append(T.make_column(dt, n, rng))
+        progs.append(T.random_program(dt, rng, selectivity=0.3))
+    b, keep = make_batch(progs, cols, [0] * len(cols), want=0)
+    assert L.voxel_batch_launch(b, 1, None) == 0 and L.voxel_batch_fetch(b, None) == 0
+    for i, (prog, col) in enumerate(zip(progs, cols)):
+        regs, cnt, ovf = results(b, i)
+        e = Engine(prog.dtype)
+        e.add_segment(col)
+        for r, v in enumerate(prog.registers(col.size)):
+            e.set_scalar(r, v)
+        e.load_program(prog.code)
+        e.run()
+        check_regs(prog.dtype, prog.code, regs, e.registers(16))
+    L.voxel_batch_destroy(b)

@@ -138,6 +138,19 @@ _SIGS = {
     "voxel_radix_sort": (C.c_int, [C.c_int, vp, vp, sz]),
     "voxel_radix_sort_dev": (C.c_int, [C.c_int, vp, vp, sz, vp, sz, vp]),
     "voxel_radix_sort_tmp_bytes": (sz, [C.c_int, sz]),
+    "voxel_scan_groupby_tune": (C.c_int, [C.c_int]),
+    "voxel_scan_groupby_last_variant": (C.c_int, []),
+    "voxel_agg_accumulate_dev": (C.c_int, [vp, vp, vp, sz, vp]),
+    "voxel_agg_results": (sz, [vp, vp, vp, vp, vp, vp]),
+    "voxel_dict_values": (sz, [vp, vp]),
+    "voxel_batch_create": (vp, []),
+    "voxel_batch_destroy": (None, [vp]),
+    "voxel_batch_size": (sz, [vp]),
+    "voxel_batch_add": (C.c_int, [vp, C.c_int, vp, sz, vp, vp, sz, C.c_int, sz, vp]),
+    "voxel_batch_set_capacity": (C.c_int, [vp, sz, sz, vp]),
+    "voxel_batch_launch": (C.c_int, [vp, C.c_int, vp]),
+    "voxel_batch_fetch": (C.c_int, [vp, vp]),
+    "voxel_batch_result": (C.c_int, [vp, sz, vp, vp, vp]),
     "voxel_hashjoin_i64": (sz, [vp, sz, vp, sz, vp, vp, sz, C.c_int]),
     "voxel_hashjoin_i64_dev": (C.c_int, [vp, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
 }

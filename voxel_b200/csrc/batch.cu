@@ -1,0 +1,474 @@
+// Batched persistent executor: many lowered programs in one launch.
+//
+// Replaces a loop of per-program Engine<T>::Run calls (include/voxel/exec/
+// engine.hpp:70-81) for single-column filter/aggregate programs.  The host
+// lowers every program (lower.cpp) to a ScanParams and splits its data groups
+// into work items of kItemGroups groups; items of a program are contiguous in
+// a global item list.  One persistent kernel takes items from a device work
+// queue (an atomic counter), so big and small columns interleave across the
+// SMs; per item a block:
+//   - evaluates the program's groups exactly as the single-program kernel does
+//     (scan_core.cuh) and writes a per-item partial of every reduction,
+//   - counts the rows that satisfy all of the program's predicate atoms, gets
+//     the item's output offset from a decoupled look-back over the program's
+//     earlier items, and writes those row ids (ascending) into the program's
+//     selection buffer while they fit its capacity (else flags overflow),
+//   - and, if it is the program's last item to finish, folds the partials in
+//     item order and writes the program's final registers and exact count.
+// Every wait is bounded.  The launch (with its memsets) is captured into a
+// CUDA graph once per batch and replayed.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "batch.h"
+#include "engine.h"
+#include "scan_core.cuh"
+#include "voxel_c.h"
+#include "vx_runtime.h"
+#include "vx_scan.cuh"
+
+namespace vx {
+
+namespace {
+
+constexpr int kBThreads = 256;
+constexpr int kBU = 2;          // groups per thread per pass
+constexpr int kBW = 8;          // passes per item
+constexpr int kBNR = 4;         // reductions per batched program
+constexpr uint64_t kItemGroups = static_cast<uint64_t>(kBThreads) * kBU * kBW;
+
+// shared memory of one block's current item (one copy for every element type)
+struct ItemShared {
+    uint32_t mask[kBW][kBThreads];  // selected lanes per pass (bit u*KL+l)
+    uint32_t scan[kBThreads / 32 + 1];
+    Acc blk[kBNR];
+    uint64_t item_base;
+};
+
+struct ItemPartial {
+    uint64_t u[kBNR];
+    double s[kBNR];
+    double c[kBNR];
+};
+
+// block-wide exclusive scan of one value per thread; returns the block total
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* excl, uint32_t* sh) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += y;
+    }
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = lane < kBThreads / 32 ? sh[lane] : 0, t = x;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, t, d);
+            if (lane >= d) t += y;
+        }
+        if (lane < kBThreads / 32) sh[lane] = t - x;
+        if (lane == kBThreads / 32 - 1) sh[kBThreads / 32] = t;
+    }
+    __syncthreads();
+    *excl = sh[warp] + inc - v;
+    uint32_t total = sh[kBThreads / 32];
+    __syncthreads();
+    return total;
+}
+
+template <typename T>
+__device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
+                                          unsigned long long* status_prog, int* err, ItemShared& sh) {
+    constexpr int KL = 32 / sizeof(T);
+    const ScanParams& p = bp.p;
+    uint32_t* s_scan = sh.scan;
+    uint32_t (*s_mask)[kBThreads] = sh.mask;
+    Acc acc[kBNR];
+#pragma unroll
+    for (int r = 0; r < kBNR; ++r) {
+        acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
+        acc[r].k = {0.0, 0.0};
+    }
+    const uint64_t g0 = t * kItemGroups;
+    const uint64_t lastj = p.ngroups - 1;
+    const bool vec = bp.vec != 0;
+    uint32_t total = 0;  // this thread's selected rows over all passes
+    // phase 1: evaluate every pass, fold the reductions, keep the selection masks
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        uint32_t mask = 0;
+        // this thread's kBU contiguous groups of pass w
+        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
+        T v[kBU][1][KL];
+#pragma unroll
+        for (int u = 0; u < kBU; ++u)
+            if (jb + u < p.ndata) load_group<T, 1>(p, jb + u, vec, v[u]);
+#pragma unroll
+        for (int u = 0; u < kBU; ++u) {
+            uint64_t j = jb + u;
+            if (j >= p.ndata) continue;
+            uint32_t ab[KL];
+            eval_atoms<T, 1>(p, v[u], ab);
+            uint64_t res[kBNR];
+            eval_reds<T, 1, kBNR>(p, v[u], ab, res);
+#pragma unroll
+            for (int r = 0; r < kBNR; ++r) {
+                if (r >= p.nred) break;
+                acc_fold<T>(acc[r], p.red[r].acc, res[r]);
+                if (j == lastj) out->res.last[r] = res[r];
+            }
+            if (bp.sel_mask) {
+                uint64_t row0 = p.off0 + j * KL;
+#pragma unroll
+                for (int l = 0; l < KL; ++l)
+                    if ((ab[l] & bp.sel_mask) == bp.sel_mask && row0 + l < p.count[0]) mask |= 1u << (u * KL + l);
+            }
+        }
+        s_mask[w][threadIdx.x] = mask;
+        total += __popc(mask);
+    }
+    // reductions -> this item's partial
+    Acc* blk = sh.blk;
+    block_reduce<T, kBNR, kBThreads>(p, acc, blk);
+    if (threadIdx.x < kBNR && threadIdx.x < p.nred) {
+        part_item->u[threadIdx.x] = blk[threadIdx.x].u;
+        part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
+        part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
+    }
+    // the item's selected-row count, then its offset from the look-back
+    uint32_t unused;
+    const uint32_t run = block_excl_scan(total, &unused, s_scan);
+    if (threadIdx.x == 0) {
+        uint64_t e = lookback_exclusive(status_prog, t, run, err);
+        sh.item_base = e;
+        if (t == bp.nitems - 1) out->sel_count = e + run;
+    }
+    __syncthreads();
+    if (!(bp.sel_mask && bp.want_sel)) return;
+    // phase 2: row ids in ascending order, pass by pass
+    uint64_t pass_base = sh.item_base;
+    bool ovf = false;
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        uint32_t m = s_mask[w][threadIdx.x];
+        uint32_t excl;
+        const uint32_t tot = block_excl_scan(__popc(m), &excl, s_scan);
+        uint64_t pos = pass_base + excl;
+        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
+        while (m) {
+            int b = __ffs(m) - 1;
+            m &= m - 1;
+            uint64_t row = p.off0 + (jb + b / KL) * KL + (b % KL);
+            if (pos < bp.sel_cap) bp.sel_out[pos] = static_cast<uint32_t>(row);
+            else ovf = true;
+            ++pos;
+        }
+        pass_base += tot;
+    }
+    if (ovf) out->overflow = 1;
+}
+
+template <typename T>
+__device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPartial* parts, BatchOut* out,
+                                              ItemShared& sh) {
+    const ScanParams& p = bp.p;
+    Acc acc[kBNR];
+#pragma unroll
+    for (int r = 0; r < kBNR; ++r) {
+        acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
+        acc[r].k = {0.0, 0.0};
+    }
+    for (uint32_t i = threadIdx.x; i < bp.nitems; i += blockDim.x) {
+#pragma unroll
+        for (int r = 0; r < kBNR; ++r) {
+            if (r >= p.nred) break;
+            Acc o;
+            o.u = __ldcg(&parts[i].u[r]);
+            o.k.s = __ldcg(&parts[i].s[r]);
+            o.k.c = __ldcg(&parts[i].c[r]);
+            acc_merge<T>(acc[r], p.red[r].acc, o);
+        }
+    }
+    Acc (&blk)[kBNR] = sh.blk;
+    block_reduce<T, kBNR, kBThreads>(p, acc, blk);
+    if (threadIdx.x == 0) finalize_scan<T, 1, kBNR>(p, blk, &out->res);
+}
+
+__global__ void __launch_bounds__(kBThreads) batch_kernel(const BatchProg* __restrict__ progs, uint32_t nprog,
+                                                          const uint64_t* __restrict__ item_start, uint64_t nitems,
+                                                          ItemPartial* parts, unsigned long long* status,
+                                                          unsigned int* pdone, unsigned int* item_ctr, BatchOut* outs,
+                                                          int* err) {
+    __shared__ uint64_t s_item;
+    __shared__ uint32_t s_prog;
+    __shared__ __align__(16) BatchProg s_bp;
+    __shared__ bool s_last;
+    __shared__ ItemShared sh;
+    uint32_t cached = 0xFFFFFFFFu;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint64_t it = atomicAdd(item_ctr, 1u);
+            s_item = it;
+            if (it < nitems) {
+                // program owning item `it`: last start <= it
+                uint32_t lo = 0, hi = nprog;
+                while (hi - lo > 1) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (item_start[mid] <= it) lo = mid; else hi = mid;
+                }
+                s_prog = lo;
+            }
+        }
+        __syncthreads();
+        const uint64_t it = s_item;
+        if (it >= nitems) break;
+        const uint32_t pid = s_prog;
+        if (pid != cached) {
+            const int4* src = reinterpret_cast<const int4*>(progs + pid);
+            int4* dst = reinterpret_cast<int4*>(&s_bp);
+            for (uint32_t i = threadIdx.x; i < sizeof(BatchProg) / 16; i += blockDim.x) dst[i] = src[i];
+            cached = pid;
+        }
+        __syncthreads();
+        const uint64_t t = it - item_start[pid];
+        switch (s_bp.p.dtype) {
+        case F64: process_item<double>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        case F32: process_item<float>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        case I64: process_item<int64_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        case I32: process_item<int32_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        case U64: process_item<uint64_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        default: process_item<uint32_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const ItemPartial* pp = parts + s_bp.item0;
+            switch (s_bp.p.dtype) {
+            case F64: finalize_program<double>(s_bp, pp, outs + pid, sh); break;
+            case F32: finalize_program<float>(s_bp, pp, outs + pid, sh); break;
+            case I64: finalize_program<int64_t>(s_bp, pp, outs + pid, sh); break;
+            case I32: finalize_program<int32_t>(s_bp, pp, outs + pid, sh); break;
+            case U64: finalize_program<uint64_t>(s_bp, pp, outs + pid, sh); break;
+            default: finalize_program<uint32_t>(s_bp, pp, outs + pid, sh); break;
+            }
+            if (threadIdx.x == 0) pdone[pid] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void clear_outs_kernel(BatchOut* outs, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        outs[i].overflow = 0;
+        outs[i].sel_count = 0;
+    }
+}
+
+}  // namespace
+
+Batch::~Batch() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (capture_) cudaStreamDestroy(capture_);
+}
+
+int Batch::add(int dtype, const uint32_t* code, size_t len, const uint64_t* regs, const void* d_col, uint64_t count,
+               bool want_sel, uint64_t sel_cap, uint32_t* d_sel) {
+    Engine e(dtype);
+    e.add_segment_device(d_col, count);
+    for (int r = 0; r < 64; ++r) e.reg(r) = regs[r];
+    e.load_program(code, len);
+    std::vector<LoweredRegion> regions;
+    int st = e.lower_regions(regions);
+    if (st) return st;
+    if (regions.size() != 1 || regions[0].params.ncols > 1 || regions[0].params.nred > kBNR) {
+        set_error(kErrUnsupportedProgram, "batched programs need exactly one single-column loop with <= %d reductions",
+                  kBNR);
+        return kErrUnsupportedProgram;
+    }
+    BatchProg bp{};
+    bp.p = regions[0].params;
+    bp.p.col[0] = d_col;
+    bp.sel_mask = bp.p.natoms ? ((1u << bp.p.natoms) - 1) : 0;
+    bp.want_sel = want_sel ? 1 : 0;
+    bp.sel_cap = sel_cap;
+    bp.sel_out = d_sel;
+    uintptr_t a = reinterpret_cast<uintptr_t>(d_col) + bp.p.off0 * dtype_size(dtype);
+    bp.vec = (a % 16) == 0;
+    host_.push_back(bp);
+    writes_.push_back(regions[0].writes);
+    regs_.emplace_back(regs, regs + 64);
+    dirty_ = true;
+    return kOk;
+}
+
+void Batch::set_capacity(size_t i, uint64_t cap, uint32_t* d_sel) {
+    host_[i].sel_cap = cap;
+    host_[i].sel_out = d_sel;
+    dirty_ = true;
+}
+
+int Batch::upload(cudaStream_t s) {
+    const uint32_t np = static_cast<uint32_t>(host_.size());
+    std::vector<uint64_t> start(np + 1);
+    uint64_t items = 0;
+    for (uint32_t i = 0; i < np; ++i) {
+        uint64_t ni = (host_[i].p.ndata + kItemGroups - 1) / kItemGroups;
+        if (ni == 0) ni = 1;  // every program finalises, even with no data groups
+        host_[i].item0 = items;
+        host_[i].nitems = static_cast<uint32_t>(ni);
+        start[i] = items;
+        items += ni;
+    }
+    start[np] = items;
+    nitems_ = items;
+    if (d_progs_.n < np * sizeof(BatchProg)) d_progs_ = DevBuf(np * sizeof(BatchProg) + 16);
+    if (d_start_.n < (np + 1) * 8) d_start_ = DevBuf((np + 1) * 8 + 8);
+    if (d_outs_.n < np * sizeof(BatchOut)) d_outs_ = DevBuf(np * sizeof(BatchOut) + 16);
+    if (d_parts_.n < items * sizeof(ItemPartial)) d_parts_ = DevBuf(items * sizeof(ItemPartial) + 16);
+    if (d_status_.n < items * 8 + 64) d_status_ = DevBuf(items * 8 + 64);
+    if (d_pdone_.n < np * 4 + 16) {
+        d_pdone_ = DevBuf(np * 4 + 16);
+        if (d_pdone_.p) VX_CUDA(cudaMemsetAsync(d_pdone_.p, 0, d_pdone_.n, s));
+    }
+    if (!d_err_.p) {
+        d_err_ = DevBuf(16);
+        if (d_err_.p) VX_CUDA(cudaMemsetAsync(d_err_.p, 0, 16, s));
+    }
+    if (!d_progs_.p || !d_start_.p || !d_outs_.p || !d_parts_.p || !d_status_.p || !d_pdone_.p || !d_err_.p)
+        return kErrOutOfMemory;
+    if (int st = h2d(d_progs_.p, host_.data(), np * sizeof(BatchProg), s)) return st;
+    if (int st = h2d(d_start_.p, start.data(), (np + 1) * 8, s)) return st;
+    if (int st = sync(s)) return st;
+    int per_sm = 0;
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBThreads, 0));
+    if (per_sm < 1) per_sm = 1;
+    grid_ = (sm_count() > 0 ? sm_count() : 148) * per_sm;
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    if (graph_) {
+        cudaGraphDestroy(graph_);
+        graph_ = nullptr;
+    }
+    dirty_ = false;
+    return kOk;
+}
+
+int Batch::enqueue(cudaStream_t s) {
+    const uint32_t np = static_cast<uint32_t>(host_.size());
+    VX_CUDA(cudaMemsetAsync(d_status_.p, 0, nitems_ * 8 + 64, s));
+    clear_outs_kernel<<<(np + 255) / 256, 256, 0, s>>>(d_outs_.as<BatchOut>(), np);
+    uint64_t grid = static_cast<uint64_t>(grid_);
+    if (grid > nitems_) grid = nitems_;
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(d_status_.as<unsigned long long>() + nitems_);
+    batch_kernel<<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(
+        d_progs_.as<BatchProg>(), np, d_start_.as<uint64_t>(), nitems_, d_parts_.as<ItemPartial>(),
+        d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr, d_outs_.as<BatchOut>(),
+        d_err_.as<int>());
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int Batch::launch(cudaStream_t s, bool use_graph) {
+    if (host_.empty()) return kOk;
+    if (dirty_) {
+        if (int st = upload(s)) return st;
+    }
+    if (!use_graph) return enqueue(s);
+    if (!graph_exec_) {
+        // Recorded on a private stream: the caller's stream may be the legacy
+        // default stream, which cannot be captured.  Recording runs nothing.
+        if (!capture_) VX_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
+        VX_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
+        int st = enqueue(capture_);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(capture_, &g);
+        if (st) return st;
+        VX_CUDA(e);
+        graph_ = g;
+        VX_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+    }
+    VX_CUDA(cudaGraphLaunch(graph_exec_, s));
+    return kOk;
+}
+
+int Batch::fetch(cudaStream_t s) {
+    const size_t np = host_.size();
+    outs_.resize(np);
+    if (!np) return kOk;
+    if (int st = d2h(outs_.data(), d_outs_.p, np * sizeof(BatchOut), s)) return st;
+    int h = 0;
+    if (int st = d2h(&h, d_err_.p, 4, s)) return st;
+    if (int st = sync(s)) return st;
+    if (h) {
+        cudaMemsetAsync(d_err_.p, 0, 4, s);
+        set_error(kErrDeviceTimeout, "batched executor: a look-back wait ran out of budget");
+        return kErrDeviceTimeout;
+    }
+    return kOk;
+}
+
+void Batch::registers(size_t i, uint64_t* regs) const {
+    std::memcpy(regs, regs_[i].data(), 64 * 8);
+    const BatchOut& o = outs_[i];
+    for (const RegWrite& w : writes_[i]) {
+        switch (w.kind) {
+        case RegWrite::kAcc: regs[w.reg] = o.res.acc[w.red]; break;
+        case RegWrite::kLast: if (host_[i].p.ngroups) regs[w.reg] = o.res.last[w.red]; break;
+        case RegWrite::kValue: regs[w.reg] = w.value; break;
+        }
+    }
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+void* voxel_batch_create(void) { return new Batch(); }
+void voxel_batch_destroy(void* b) { delete static_cast<Batch*>(b); }
+size_t voxel_batch_size(const void* b) { return static_cast<const Batch*>(b)->size(); }
+
+int voxel_batch_add(void* b, int dtype, const uint32_t* code, size_t len, const uint64_t* regs64, const void* d_col,
+                    size_t count, int want_selection, size_t sel_capacity, uint32_t* d_sel) {
+    clear_error();
+    return static_cast<Batch*>(b)->add(dtype, code, len, regs64, d_col, count, want_selection != 0, sel_capacity,
+                                       d_sel);
+}
+
+int voxel_batch_set_capacity(void* b, size_t prog, size_t capacity, uint32_t* d_sel) {
+    Batch* B = static_cast<Batch*>(b);
+    if (prog >= B->size()) return kErrInvalidArg;
+    B->set_capacity(prog, capacity, d_sel);
+    return kOk;
+}
+
+int voxel_batch_launch(void* b, int use_graph, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    return static_cast<Batch*>(b)->launch(static_cast<cudaStream_t>(stream), use_graph != 0);
+}
+
+int voxel_batch_fetch(void* b, void* stream) {
+    clear_error();
+    return static_cast<Batch*>(b)->fetch(static_cast<cudaStream_t>(stream));
+}
+
+int voxel_batch_result(const void* b, size_t prog, uint64_t* regs64, uint64_t* sel_count, int* overflow) {
+    const Batch* B = static_cast<const Batch*>(b);
+    if (prog >= B->size() || prog >= B->fetched()) return kErrInvalidArg;
+    if (regs64) B->registers(prog, regs64);
+    if (sel_count) *sel_count = B->out(prog).sel_count;
+    if (overflow) *overflow = B->out(prog).overflow;
+    return kOk;
+}
+
+}  // extern "C"

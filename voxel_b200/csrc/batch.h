@@ -1,0 +1,66 @@
+// Batched persistent executor: host object.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "lower.h"
+#include "vx_runtime.h"
+#include "vx_types.h"
+
+namespace vx {
+
+struct __align__(16) BatchProg {
+    ScanParams p;
+    uint32_t sel_mask;    // atoms whose conjunction selects rows (0: no selection)
+    uint32_t want_sel;    // write row ids (else only count)
+    uint32_t* sel_out;
+    uint64_t sel_cap;     // capacity of sel_out in row ids
+    uint64_t item0;       // first work item of this program
+    uint32_t nitems;
+    uint32_t vec;         // 16-byte aligned column: vector loads
+};
+
+struct BatchOut {
+    ScanResult res;
+    unsigned long long sel_count;  // exact count of selected rows
+    int overflow;                  // the selection did not fit sel_cap
+    int pad;
+};
+
+class Batch {
+public:
+    ~Batch();
+    int add(int dtype, const uint32_t* code, size_t len, const uint64_t* regs, const void* d_col, uint64_t count,
+            bool want_sel, uint64_t sel_cap, uint32_t* d_sel);
+    void set_capacity(size_t i, uint64_t cap, uint32_t* d_sel);
+    // one persistent launch for the whole batch (replayed from a CUDA graph when use_graph)
+    int launch(cudaStream_t s, bool use_graph);
+    int fetch(cudaStream_t s);  // copies the per-program outputs back (synchronises)
+    size_t size() const { return host_.size(); }
+    size_t fetched() const { return outs_.size(); }
+    const BatchOut& out(size_t i) const { return outs_[i]; }
+    const BatchProg& prog(size_t i) const { return host_[i]; }
+    void registers(size_t i, uint64_t* regs) const;
+    uint64_t items() const { return nitems_; }
+
+private:
+    int upload(cudaStream_t s);
+    int enqueue(cudaStream_t s);
+
+    std::vector<BatchProg> host_;
+    std::vector<std::vector<RegWrite>> writes_;
+    std::vector<std::vector<uint64_t>> regs_;
+    std::vector<BatchOut> outs_;
+    DevBuf d_progs_, d_start_, d_outs_, d_parts_, d_status_, d_pdone_, d_err_;
+    uint64_t nitems_ = 0;
+    int grid_ = 148;
+    bool dirty_ = true;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaStream_t capture_ = nullptr;  // private stream the graph is recorded on
+};
+
+}  // namespace vx

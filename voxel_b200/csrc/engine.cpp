@@ -168,6 +168,7 @@ int Engine::ensure_device_data(int seg, const void** dptr) {
 int Engine::run_region(LoweredRegion& lr) {
     ScanParams& p = lr.params;
     if (dry_) {
+        if (capture_) capture_->push_back(lr);
         for (const RegWrite& w : lr.writes) R_[w.reg] = w.kind == RegWrite::kValue ? w.value : 0;
         if (lr.set_flags) arith_flags(flags_, lr.flag_value);
         explain_ += describe(lr);
@@ -349,6 +350,14 @@ int Engine::plan() {
     pc_ = pc;
     running_ = running;
     flags_ = fl;
+    return st;
+}
+
+int Engine::lower_regions(std::vector<LoweredRegion>& out) {
+    out.clear();
+    capture_ = &out;
+    int st = plan();
+    capture_ = nullptr;
     return st;
 }
 

@@ -42,6 +42,10 @@ public:
     // Lowers every data region without touching the device; explain() then
     // holds the schedules (register results of regions read as zero).
     int plan();
+    // Lowers the loaded program to its data regions without running it; the
+    // host-side scalar glue before each region is stepped with the current
+    // registers.  Used by the batched executor.
+    int lower_regions(std::vector<LoweredRegion>& out);
     int run_parallel(size_t seg_id, uint32_t threads, uint8_t result_reg);
     void reset();
     uint64_t& reg(size_t i) { return R_[i & 63]; }
@@ -78,6 +82,7 @@ private:
     std::string explain_;
     double last_ms_ = 0.0;
     bool dry_ = false;
+    std::vector<LoweredRegion>* capture_ = nullptr;
 };
 
 }  // namespace vx

@@ -24,6 +24,7 @@
 
 #include "fixedpoint.cuh"
 #include "groupby.h"
+#include "tma.cuh"
 #include "voxel_c.h"
 #include "vx_common.cuh"
 #include "vx_runtime.h"
@@ -162,19 +163,50 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     const unsigned lanemask_lt = (1u << lane) - 1;
     WarpQueue& Q = s_queue[threadIdx.x >> 5];
     int qn = 0;  // warp-uniform fill of Q
-    // lanes < cnt fold queue entry `lane` into the block table, converged
+    // lanes < cnt fold queue entry `lane` into the block table, converged.
+    // Entries of the same group are first combined by the lowest such lane
+    // (match + shuffles), so a hot group costs one set of atomics per round
+    // instead of one per row, and no two lanes of an atomic hit one address.
     auto consume = [&](int cnt) {
-        if (lane < cnt) {
-            uint32_t gi = Q.gid[lane];
-            if (gi >= card) {
-                bad_key = true;
-            } else {
-                double p = Q.price[lane];
-                fix_atomic_add(&s_acc[3 * gi], pack_row(fix_from_double_s<kFixScale>(Q.val[lane], &bad_value)));
-                uint64_t ok = f64_order_key(p);
-                if (ok < s_mn[gi]) atomicMin(&s_mn[gi], static_cast<unsigned long long>(ok));
-                if (ok > s_mx[gi]) atomicMax(&s_mx[gi], static_cast<unsigned long long>(ok));
+        bool valid = lane < cnt;
+        uint32_t gi = valid ? Q.gid[lane] : 0;
+        if (valid && gi >= card) {
+            bad_key = true;
+            valid = false;
+        }
+        Fix3 f{0, 0, 0};
+        double p = 0.0;
+        if (valid) {
+            p = Q.price[lane];
+            f = pack_row(fix_from_double_s<kFixScale>(Q.val[lane], &bad_value));
+        }
+        uint32_t key = valid ? gi : (0x80000000u | static_cast<uint32_t>(lane));
+        unsigned peers = __match_any_sync(0xffffffffu, key);
+        bool leader = valid && (__ffs(peers) - 1 == lane);
+        double pmin = p, pmax = p;
+        Fix3 acc = f;
+        if (__any_sync(0xffffffffu, valid && __popc(peers) > 1)) {
+            unsigned rest = leader ? (peers & ~(1u << lane)) : 0u;
+            while (__any_sync(0xffffffffu, rest != 0)) {
+                int src = rest ? __ffs(rest) - 1 : lane;
+                Fix3 o;
+                o.w0 = __shfl_sync(0xffffffffu, f.w0, src);
+                o.w1 = __shfl_sync(0xffffffffu, f.w1, src);
+                o.w2 = __shfl_sync(0xffffffffu, f.w2, src);
+                double op = __shfl_sync(0xffffffffu, p, src);
+                if (rest) {
+                    fix_add(acc, o);
+                    pmin = op < pmin ? op : pmin;
+                    pmax = op > pmax ? op : pmax;
+                    rest &= rest - 1;
+                }
             }
+        }
+        if (leader) {
+            fix_atomic_add(&s_acc[3 * gi], acc);
+            uint64_t kmin = f64_order_key(pmin), kmax = f64_order_key(pmax);
+            if (kmin < s_mn[gi]) atomicMin(&s_mn[gi], static_cast<unsigned long long>(kmin));
+            if (kmax > s_mx[gi]) atomicMax(&s_mx[gi], static_cast<unsigned long long>(kmax));
         }
     };
 
@@ -295,6 +327,290 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed variant for dictionaries up to kTmaMaxCard entries.
+//
+// A producer warp streams 2048-row tiles of price / qty / packed keys into a
+// 3-stage shared-memory ring with bulk async copies (cp.async.bulk, counted on
+// mbarriers).  Each of 8 consumer warps owns a private per-group table
+// (compensated FP64 sum with an f32 error term, u32 count) and updates it
+// without atomics: passing rows are compacted into a per-warp queue with a
+// ballot, rows of the same group inside a 32-row round are folded by the
+// leader lane (__match_any_sync + shuffles), and leaders have distinct groups,
+// so plain read-modify-writes suffice.  MIN/MAX live in one block table and
+// change rarely (conditional atomics).  At the end the warp tables are merged
+// in warp order and added exactly (192-bit fixed point) to the global table.
+// ---------------------------------------------------------------------------
+constexpr int kTmaConsumers = 8;
+constexpr int kTmaThreads = (kTmaConsumers + 1) * 32;
+constexpr int kTmaRows = 2048;
+constexpr int kTmaStages = 3;
+constexpr uint32_t kTmaMaxCard = 1024;
+constexpr long long kTmaWaitBudget = 1ll << 32;  // clock cycles
+
+__device__ __forceinline__ size_t tma_stage_bytes(uint32_t width) { return 24576u + 256u * width; }
+
+// Folds one row per lane (valid lanes) into the warp's private table.
+__device__ __forceinline__ void warp_table_update(uint32_t gid, double v, double p, bool valid, uint32_t card,
+                                                  double* ts, float* tc, uint32_t* tn, unsigned long long* s_mn,
+                                                  unsigned long long* s_mx, bool* bad_key) {
+    const int lane = threadIdx.x & 31;
+    if (valid && gid >= card) {
+        *bad_key = true;
+        valid = false;
+    }
+    uint32_t key = valid ? gid : (0x80000000u | static_cast<uint32_t>(lane));
+    unsigned peers = __match_any_sync(0xffffffffu, key);
+    bool leader = valid && (__ffs(peers) - 1 == lane);
+    double vs = v, pmin = p, pmax = p;
+    uint32_t cn = 1;
+    if (__any_sync(0xffffffffu, valid && __popc(peers) > 1)) {
+        unsigned rest = leader ? (peers & ~(1u << lane)) : 0u;
+        while (__any_sync(0xffffffffu, rest != 0)) {
+            int src = rest ? __ffs(rest) - 1 : lane;
+            double ov = __shfl_sync(0xffffffffu, v, src);
+            double op = __shfl_sync(0xffffffffu, p, src);
+            if (rest) {
+                vs = __dadd_rn(vs, ov);
+                ++cn;
+                pmin = op < pmin ? op : pmin;
+                pmax = op > pmax ? op : pmax;
+                rest &= rest - 1;
+            }
+        }
+    }
+    if (leader) {
+        double s0 = ts[gid];
+        double t = __dadd_rn(s0, vs);
+        double e = fabs(s0) >= fabs(vs) ? __dadd_rn(__dsub_rn(s0, t), vs) : __dadd_rn(__dsub_rn(vs, t), s0);
+        ts[gid] = t;
+        tc[gid] = __fadd_rn(tc[gid], static_cast<float>(e));
+        tn[gid] += cn;
+        uint64_t kmin = f64_order_key(pmin), kmax = f64_order_key(pmax);
+        if (kmin < s_mn[gid]) atomicMin(&s_mn[gid], static_cast<unsigned long long>(kmin));
+        if (kmax > s_mx[gid]) atomicMax(&s_mx[gid], static_cast<unsigned long long>(kmax));
+    }
+}
+
+// Last block: compact the global table's non-empty groups in key order and
+// reset it.  All threads of the block call.
+template <int THREADS>
+__device__ void finalize_groups(const GlobalGroups& g, const int32_t* dict, uint32_t card, unsigned int* done,
+                                int32_t* out_keys, double* out_sum, double* out_min, double* out_max,
+                                uint64_t* out_count, uint64_t* out_ngroups) {
+    __shared__ unsigned int s_scan[THREADS];
+    uint32_t per = (card + THREADS - 1) / THREADS;
+    uint32_t lo = threadIdx.x * per < card ? threadIdx.x * per : card;
+    uint32_t hi = lo + per < card ? lo + per : card;
+    unsigned int mine = 0;
+    for (uint32_t i = lo; i < hi; ++i) mine += __ldcg(&g.cnt[i]) ? 1 : 0;
+    s_scan[threadIdx.x] = mine;
+    __syncthreads();
+    for (int d = 1; d < THREADS; d <<= 1) {
+        unsigned int v = threadIdx.x >= static_cast<unsigned>(d) ? s_scan[threadIdx.x - d] : 0;
+        __syncthreads();
+        s_scan[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned int pos = s_scan[threadIdx.x] - mine;
+    for (uint32_t i = lo; i < hi; ++i) {
+        unsigned long long c = __ldcg(&g.cnt[i]);
+        if (c) {
+            Fix3 f{__ldcg(&g.sum[3 * i]), __ldcg(&g.sum[3 * i + 1]), __ldcg(&g.sum[3 * i + 2])};
+            out_keys[pos] = dict[i];
+            out_sum[pos] = fix_to_double_s<kFixScale>(f);
+            out_min[pos] = f64_from_order_key(__ldcg(&g.mn[i]));
+            out_max[pos] = f64_from_order_key(__ldcg(&g.mx[i]));
+            out_count[pos] = c;
+            ++pos;
+        }
+        g.sum[3 * i] = 0;
+        g.sum[3 * i + 1] = 0;
+        g.sum[3 * i + 2] = 0;
+        g.cnt[i] = 0;
+        g.mn[i] = ~0ull;
+        g.mx[i] = 0;
+    }
+    if (threadIdx.x == THREADS - 1) {
+        *out_ngroups = s_scan[threadIdx.x];
+        *done = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 1) scan_groupby_tma_kernel(
+    const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
+    const double* __restrict__ price, const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo,
+    int32_t qhi, GlobalGroups g, unsigned int* done, int32_t* out_keys, double* out_sum, double* out_min,
+    double* out_max, uint64_t* out_count, uint64_t* out_ngroups, int* status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const uint32_t stage_bytes = static_cast<uint32_t>(tma_stage_bytes(width));
+    unsigned char* stages = smem;
+    double* t_s = reinterpret_cast<double*>(smem + kTmaStages * stage_bytes);
+    float* t_c = reinterpret_cast<float*>(t_s + kTmaConsumers * card);
+    uint32_t* t_n = reinterpret_cast<uint32_t*>(t_c + kTmaConsumers * card);
+    unsigned long long* s_mn = reinterpret_cast<unsigned long long*>(
+        (reinterpret_cast<uintptr_t>(t_n + kTmaConsumers * card) + 7) & ~static_cast<uintptr_t>(7));
+    unsigned long long* s_mx = s_mn + card;
+    uint16_t* queues = reinterpret_cast<uint16_t*>(s_mx + card);
+    uint64_t* full = reinterpret_cast<uint64_t*>(
+        (reinterpret_cast<uintptr_t>(queues + kTmaConsumers * 64) + 7) & ~static_cast<uintptr_t>(7));
+    uint64_t* empty = full + kTmaStages;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint32_t i = threadIdx.x; i < kTmaConsumers * card; i += blockDim.x) {
+        t_s[i] = 0.0;
+        t_c[i] = 0.0f;
+        t_n[i] = 0;
+    }
+    for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+        s_mn[i] = ~0ull;
+        s_mx[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kTmaStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTmaConsumers);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    const uint64_t nfull = n / kTmaRows;
+    const uint64_t mytiles = nfull > blockIdx.x ? (nfull - blockIdx.x - 1) / gridDim.x + 1 : 0;
+    const uint64_t mask = (1ull << width) - 1;
+    bool bad_value = false, bad_key = false, timeout = false;
+
+    if (warp == kTmaConsumers) {
+        // producer: one lane issues the bulk copies, a stage ahead of the consumers
+        if (lane == 0) {
+            uint64_t issued = 0;
+            for (uint64_t k = 0; k < mytiles; ++k) {
+                const int s = static_cast<int>(k % kTmaStages);
+                const uint64_t r = k / kTmaStages;
+                if (r > 0 && !mbar_wait(&empty[s], static_cast<uint32_t>((r - 1) & 1), kTmaWaitBudget)) {
+                    timeout = true;
+                    break;
+                }
+                const uint64_t base = (blockIdx.x + k * gridDim.x) * kTmaRows;
+                unsigned char* st = stages + static_cast<size_t>(s) * stage_bytes;
+                mbar_arrive_expect_tx(&full[s], stage_bytes);
+                bulk_g2s(st, price + base, kTmaRows * 8, &full[s]);
+                bulk_g2s(st + kTmaRows * 8, qty + base, kTmaRows * 4, &full[s]);
+                bulk_g2s(st + kTmaRows * 12, packed + base * width / 64, 256u * width, &full[s]);
+                ++issued;
+            }
+            // never leave the block with copies still landing in its shared memory
+            uint64_t from = issued > kTmaStages ? issued - kTmaStages : 0;
+            for (uint64_t k = from; k < issued; ++k)
+                if (!mbar_wait(&full[k % kTmaStages], static_cast<uint32_t>((k / kTmaStages) & 1), kTmaWaitBudget))
+                    timeout = true;
+        }
+    } else {
+        double* ts = t_s + warp * card;
+        float* tc = t_c + warp * card;
+        uint32_t* tn = t_n + warp * card;
+        uint16_t* q = queues + warp * 64;
+        const unsigned lanemask_lt = (1u << lane) - 1;
+        for (uint64_t k = 0; k < mytiles; ++k) {
+            const int s = static_cast<int>(k % kTmaStages);
+            // every lane observes the phase (visibility of the copied bytes); the
+            // warp then agrees, so the warp-wide intrinsics below stay converged
+            bool ok = mbar_wait(&full[s], static_cast<uint32_t>((k / kTmaStages) & 1), kTmaWaitBudget);
+            if (!__all_sync(0xffffffffu, ok)) {
+                timeout = true;
+                break;
+            }
+            const unsigned char* st = stages + static_cast<size_t>(s) * stage_bytes;
+            const double* sp = reinterpret_cast<const double*>(st);
+            const int32_t* sq = reinterpret_cast<const int32_t*>(st + kTmaRows * 8);
+            const uint64_t* sk = reinterpret_cast<const uint64_t*>(st + kTmaRows * 12);
+            int qn = 0;
+            auto round = [&](int cnt) {
+                bool valid = lane < cnt;
+                uint32_t gid = 0;
+                double v = 0.0, p = 0.0;
+                if (valid) {
+                    uint32_t j = q[lane];
+                    p = sp[j];
+                    v = __dmul_rn(p, static_cast<double>(sq[j]));  // one rounded multiply
+                    uint32_t bit = j * width, wi = bit >> 6, sh = bit & 63;
+                    uint64_t x = sk[wi] >> sh;
+                    if (sh + width > 64) x |= sk[wi + 1] << (64 - sh);
+                    gid = static_cast<uint32_t>(x & mask);
+                }
+                warp_table_update(gid, v, p, valid, card, ts, tc, tn, s_mn, s_mx, &bad_key);
+            };
+            const uint32_t r0 = static_cast<uint32_t>(warp) * (kTmaRows / kTmaConsumers);
+#pragma unroll 2
+            for (uint32_t sl = 0; sl < kTmaRows / kTmaConsumers; sl += 32) {
+                uint32_t j = r0 + sl + lane;
+                double p = sp[j];
+                int32_t qq = sq[j];
+                bool pass = p > pthr && qq >= qlo && qq <= qhi;
+                unsigned m = __ballot_sync(0xffffffffu, pass);
+                if (pass) q[qn + __popc(m & lanemask_lt)] = static_cast<uint16_t>(j);
+                qn += __popc(m);
+                if (qn >= 32) {
+                    __syncwarp();
+                    round(32);
+                    __syncwarp();
+                    if (lane < qn - 32) q[lane] = q[32 + lane];
+                    __syncwarp();
+                    qn -= 32;
+                }
+            }
+            __syncwarp();
+            round(qn);  // the queue refers to this stage: drain before releasing it
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+        // the partial tail tile: block 0's consumer warps, plain loads
+        if (blockIdx.x == 0 && !timeout) {
+            const uint64_t tb = nfull * kTmaRows;
+            for (uint64_t r = tb + static_cast<uint64_t>(warp) * 32 + lane; r - lane < n;
+                 r += kTmaConsumers * 32) {
+                bool in = r < n;
+                double p = in ? price[r] : 0.0;
+                int32_t qq = in ? qty[r] : 0;
+                bool pass = in && p > pthr && qq >= qlo && qq <= qhi;
+                uint32_t gid = pass ? key_bits(packed, r, width, mask) : 0;
+                warp_table_update(gid, __dmul_rn(p, static_cast<double>(qq)), p, pass, card, ts, tc, tn, s_mn, s_mx,
+                                  &bad_key);
+            }
+        }
+    }
+    if (timeout) atomicOr(status, 4);
+    if (bad_key) atomicOr(status, 2);
+    __syncthreads();
+    // merge the warp tables (warp order) and add them exactly to the global table
+    for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+        KSum k{0.0, 0.0};
+        unsigned long long c = 0;
+        double ec = 0.0;
+        for (int w = 0; w < kTmaConsumers; ++w) {
+            ksum_add(k, t_s[w * card + i]);
+            ec += static_cast<double>(t_c[w * card + i]);
+            c += t_n[w * card + i];
+        }
+        if (!c) continue;
+        Fix3 f = fix_from_double_s<kFixScale>(k.s, &bad_value);
+        fix_add(f, fix_from_double_s<kFixScale>(__dadd_rn(k.c, ec), &bad_value));
+        fix_atomic_add(&g.sum[3 * i], f);
+        atomicAdd(&g.cnt[i], c);
+        atomicMin(&g.mn[i], s_mn[i]);
+        atomicMax(&g.mx[i], s_mx[i]);
+    }
+    if (bad_value) atomicOr(status, 1);
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    finalize_groups<kTmaThreads>(g, dict, card, done, out_keys, out_sum, out_min, out_max, out_count, out_ngroups);
+}
+
 __global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* done) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < card; i += gridDim.x * blockDim.x) {
         g.sum[3 * i] = 0;
@@ -308,6 +624,47 @@ __global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* 
 }
 
 size_t table_bytes(uint32_t card) { return static_cast<size_t>(card) * 6 * 8 + 256; }
+
+size_t tma_smem_bytes(uint32_t card, uint32_t width) {
+    return kTmaStages * (24576u + 256u * width) + static_cast<size_t>(kTmaConsumers) * card * 16 +
+           static_cast<size_t>(card) * 16 + kTmaConsumers * 64 * 2 + 2 * kTmaStages * 8 + 64;
+}
+
+// 227 KB per block on sm_100, less the TMA kernel's static shared memory
+constexpr size_t kSmemOptIn = 232448 - 2048;
+
+int launch_tma(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+               const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+               int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
+    size_t smem = tma_smem_bytes(card, width);
+    static thread_local int max_dyn = 0;
+    if (!max_dyn) {
+        int dev = 0, optin = 0;
+        VX_CUDA(cudaGetDevice(&dev));
+        VX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        VX_CUDA(cudaFuncGetAttributes(&fa, scan_groupby_tma_kernel));
+        max_dyn = optin - static_cast<int>(fa.sharedSizeBytes);
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    }
+    if (smem > static_cast<size_t>(max_dyn)) {
+        set_error(kErrInvalidArg, "TMA group-by needs %zu bytes of shared memory, %d available", smem, max_dyn);
+        return kErrInvalidArg;
+    }
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t nfull = n / kTmaRows;
+    uint64_t grid = static_cast<uint64_t>(sms);
+    if (grid > nfull) grid = nfull;
+    if (grid < 1) grid = 1;
+    GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
+    scan_groupby_tma_kernel<<<static_cast<unsigned>(grid), kTmaThreads, smem, s>>>(
+        packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, S.g_done, ok, os, omn, omx, oc, ong,
+        static_cast<int*>(S.status.p));
+    VX_CUDA(cudaGetLastError());
+    S.last_grid = static_cast<int>(grid);
+    S.last_kernel = 1;
+    return kOk;
+}
 
 template <int RPT>
 int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
@@ -380,6 +737,11 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
     }
     int st = prepare(card, s);
     if (st) return st;
+    if (use_tma && card <= kTmaMaxCard && tma_smem_bytes(card, width) <= kSmemOptIn && n >= kTmaRows &&
+        ((reinterpret_cast<uintptr_t>(packed) & 15) == 0))
+        return launch_tma(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
+                          out_min, out_max, out_count, out_ngroups, s);
+    last_kernel = 0;
     switch (rows_per_thread) {
     case 8:
         return launch_rpt<8>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
@@ -438,11 +800,18 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
                                        qlo, qhi, d_keys, d_sum, d_min, d_max, d_count, d_ngroups, s);
 }
 
-int voxel_scan_groupby_tune(int rows_per_thread) {
-    if (rows_per_thread != 4 && rows_per_thread != 8 && rows_per_thread != 16) return kErrInvalidArg;
-    scan_groupby_state().rows_per_thread = rows_per_thread;
+int voxel_scan_groupby_tune(int variant) {
+    if (variant == 0) {
+        scan_groupby_state().use_tma = true;
+        return kOk;
+    }
+    if (variant != 4 && variant != 8 && variant != 16) return kErrInvalidArg;
+    scan_groupby_state().use_tma = false;
+    scan_groupby_state().rows_per_thread = variant;
     return kOk;
 }
+
+int voxel_scan_groupby_last_variant(void) { return scan_groupby_state().last_kernel; }
 
 size_t voxel_scan_groupby(const uint64_t* packed, size_t nwords, uint32_t width, const int32_t* dict, size_t card,
                           const double* price, const int32_t* qty, size_t n, double pthr, int32_t qlo, int32_t qhi,

@@ -19,8 +19,10 @@ struct ScanGroupBy {
     uint32_t card_ = 0;
     unsigned long long *g_sum = nullptr, *g_cnt = nullptr, *g_mn = nullptr, *g_mx = nullptr;
     unsigned int* g_done = nullptr;
-    int rows_per_thread = 8;  // autotuned per shape: 4, 8 or 16
+    int rows_per_thread = 4;  // tuning knob of the atomic variant: 4, 8 or 16
+    bool use_tma = false;     // TMA-fed private-table variant when the dictionary fits
     int last_grid = 0;
+    int last_kernel = 0;      // 0: shared-atomic variant, 1: TMA-fed variant
 
     int prepare(uint32_t card, cudaStream_t s);
     int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
