@@ -256,6 +256,38 @@ int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, ui
                                  double* d_max, uint64_t* d_count, uint64_t* d_ngroups,
                                  void* stream);
 
+/*
+ * Allocation-free variant of voxel_scan_groupby_dev (no counterpart in the
+ * reference; added for callers that must not allocate device memory, e.g. a
+ * host that has handed all device memory to its own pool and forbids the
+ * library from calling cudaMalloc/cudaFree, or a caller on a latency-critical
+ * path where an allocation could block).  Same inputs, outputs and results as
+ * voxel_scan_groupby_dev (bit-identical), always with the shared-atomic kernel.
+ *
+ * - Allocates nothing: the group table (the only scratch) is a fixed
+ *   196,864-byte device array inside libvoxel_c.so, sized for the largest
+ *   dictionary, card <= 4096 groups.  A larger card returns VOXEL_EINVAL with
+ *   a message; nothing is launched.
+ * - The first call on each device does a one-time setup (finds the array's
+ *   address, sets its min keys, waits for that on `stream`); make the first
+ *   call before any stream capture.  Later calls only enqueue the kernel.
+ * - *d_status is caller-owned device memory that must be 0 before the call;
+ *   the kernel ORs in 1 (a price*qty product not finite or beyond 2^63) or 2
+ *   (a packed key index outside the dictionary).  Output buffers need no
+ *   clearing.
+ * - The table is shared by every call on a device: calls that overlap in time
+ *   (different streams or threads, same device) race and give wrong results;
+ *   calls queued on one stream are fine.  Each launch leaves the table ready
+ *   for the next.
+ */
+int       voxel_scan_groupby_noalloc_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,
+                                         const int32_t* d_dict, size_t card, const double* d_price,
+                                         const int32_t* d_qty, size_t n, double price_gt,
+                                         int32_t qty_lo, int32_t qty_hi, int32_t* d_keys,
+                                         double* d_sum, double* d_min, double* d_max,
+                                         uint64_t* d_count, uint64_t* d_ngroups, int* d_status,
+                                         void* stream);
+
 /* ================================================================
  * Additive: GROUP BY over explicit keys (HashAggregator semantics,
  * aggregate.hpp:159-301): per key SUM (compensated f64), MIN, MAX, COUNT,

@@ -132,6 +132,8 @@ _SIGS = {
     "voxel_scan_groupby": (sz, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32, vp, vp, vp, vp, vp]),
     "voxel_scan_groupby_dev": (C.c_int, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32,
                                           vp, vp, vp, vp, vp, vp, vp]),
+    "voxel_scan_groupby_noalloc_dev": (C.c_int, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32,
+                                                  vp, vp, vp, vp, vp, vp, vp, vp]),
     "voxel_groupby_i32_f64": (sz, [vp, vp, sz, sz, vp, vp, vp, vp, vp]),
     "voxel_groupby_u32_f64": (sz, [vp, vp, sz, sz, vp, vp, vp, vp, vp]),
     "voxel_grouped_sorted_i32_f64": (sz, [vp, vp, sz, vp, vp, vp, vp, vp]),

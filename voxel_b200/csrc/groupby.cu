@@ -21,6 +21,7 @@
 // the embedded count, and the last block to finish converts the global table
 // to sorted output rows and resets it for the next launch.
 #include <cstdio>
+#include <mutex>
 
 #include "fixedpoint.cuh"
 #include "groupby.h"
@@ -778,6 +779,58 @@ ScanGroupBy& scan_groupby_state() {
     return s;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant (voxel_scan_groupby_noalloc_dev).
+//
+// The group table lives in a fixed file-scope device array laid out for the
+// largest dictionary (kMaxGroups groups at a fixed stride, so a call with any
+// smaller dictionary uses a prefix of each field).  Its resting state is: sum
+// words 0, counts 0, min keys all ones, max keys 0, completion counter 0.  The
+// loader zeroes the array; the first call on a device sets the min keys and
+// waits for that; every launch's last block puts the groups it used and the
+// counter back to the resting state.
+namespace {
+
+constexpr size_t kNoAllocWords = static_cast<size_t>(kMaxGroups) * 6 + 32;  // 196,864 bytes
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_addr[kNoAllocMaxDevices] = {};
+int g_noalloc_per_sm[kNoAllocMaxDevices] = {};
+
+// One-time per-device setup: symbol address, resting state of the min keys,
+// kernel attribute, occupancy.  Synchronises `s`.
+int noalloc_setup(cudaStream_t s, unsigned long long** base, int* per_sm) {
+    int dev = 0;
+    VX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error(kErrInvalidArg, "device ordinal %d outside 0..%d", dev, kNoAllocMaxDevices - 1);
+        return kErrInvalidArg;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        VX_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        unsigned long long* b = static_cast<unsigned long long*>(p);
+        VX_CUDA(cudaMemsetAsync(b + 4 * static_cast<size_t>(kMaxGroups), 0xFF, kMaxGroups * sizeof(unsigned long long),
+                                s));
+        VX_CUDA(cudaStreamSynchronize(s));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
+        int occ = 0;
+        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_groupby_kernel<4>, kGbThreads,
+                                                              scan_groupby_smem_bytes(kMaxGroups)));
+        g_noalloc_per_sm[dev] = occ < 1 ? 1 : occ;
+        g_noalloc_addr[dev] = b;
+    }
+    *base = g_noalloc_addr[dev];
+    *per_sm = g_noalloc_per_sm[dev];
+    return kOk;
+}
+
+}  // namespace
+
 }  // namespace vx
 
 using namespace vx;
@@ -812,6 +865,58 @@ int voxel_scan_groupby_tune(int variant) {
 }
 
 int voxel_scan_groupby_last_variant(void) { return scan_groupby_state().last_kernel; }
+
+int voxel_scan_groupby_noalloc_dev(const uint64_t* d_packed, size_t nwords, uint32_t width, const int32_t* d_dict,
+                                   size_t card, const double* d_price, const int32_t* d_qty, size_t n, double pthr,
+                                   int32_t qlo, int32_t qhi, int32_t* d_keys, double* d_sum, double* d_min,
+                                   double* d_max, uint64_t* d_count, uint64_t* d_ngroups, int* d_status,
+                                   void* stream) {
+    clear_error();
+    int st = ensure_device();
+    if (st) return st;
+    if (card == 0 || card > kMaxGroups) {
+        set_error(kErrInvalidArg,
+                  "voxel_scan_groupby_noalloc_dev: dictionary of %zu entries; its fixed scratch holds 1..%u groups",
+                  card, kMaxGroups);
+        return kErrInvalidArg;
+    }
+    if (width == 0 || width > kMaxWidth) {
+        set_error(kErrInvalidArg, "bit width %u outside 1..%d", width, kMaxWidth);
+        return kErrInvalidArg;
+    }
+    if (nwords * 64 < n * static_cast<uint64_t>(width)) {
+        set_error(kErrInvalidArg, "packed key column has %zu words, %zu rows of %u bits need more", nwords, n, width);
+        return kErrInvalidArg;
+    }
+    if ((reinterpret_cast<uintptr_t>(d_price) | reinterpret_cast<uintptr_t>(d_qty)) & 15) {
+        set_error(kErrInvalidArg, "price / qty columns must be 16-byte aligned");
+        return kErrInvalidArg;
+    }
+    if (!d_status) {
+        set_error(kErrInvalidArg, "voxel_scan_groupby_noalloc_dev needs a device status word");
+        return kErrInvalidArg;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    unsigned long long* base = nullptr;
+    int per_sm = 1;
+    st = noalloc_setup(s, &base, &per_sm);
+    if (st) return st;
+    const size_t G = kMaxGroups;
+    GlobalGroups g{base, base + 3 * G, base + 4 * G, base + 5 * G};
+    unsigned int* done = reinterpret_cast<unsigned int*>(base + 6 * G);
+    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * 4;
+    const uint32_t c32 = static_cast<uint32_t>(card);
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t ntiles = (n + kTile - 1) / kTile;
+    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (grid < 1) grid = 1;
+    scan_groupby_kernel<4><<<static_cast<unsigned>(grid), kGbThreads, scan_groupby_smem_bytes(c32), s>>>(
+        d_packed, width, d_dict, c32, d_price, d_qty, n, pthr, qlo, qhi, g, done, d_keys, d_sum, d_min, d_max,
+        d_count, d_ngroups, d_status);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
 
 size_t voxel_scan_groupby(const uint64_t* packed, size_t nwords, uint32_t width, const int32_t* dict, size_t card,
                           const double* price, const int32_t* qty, size_t n, double pthr, int32_t qlo, int32_t qhi,
