@@ -244,9 +244,16 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              const int32_t* qty, size_t n, double price_gt, int32_t qty_lo,
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
-/* kernel variant of the calling thread's fused scan: 0 = TMA-fed private warp
- * tables (dictionaries up to 1024 entries), 4 (default) / 8 / 16 = shared-table
- * atomics with that many rows per thread; and the variant the last call used */
+/* kernel variant of the calling thread's fused scan:
+ *   -1 = default (1);
+ *    1 / 2 = 32-bit-word group table fed by a per-warp row queue, 4 / 8 rows
+ *        per thread (1 is the default);
+ *    3 / 5 = 32-bit-word group table, rows added where read, 4 / 8 rows per thread;
+ *    4 / 8 / 16 = warp-merged rows, 192-bit shared atomics, that many rows per thread;
+ *    0 = TMA-fed private warp tables (dictionaries up to 1024 entries).
+ * All but 0 give bit-identical results.  voxel_scan_groupby_last_variant
+ * reports the kernel the last call ran: 0 warp-merged, 1 TMA-fed, 2 word table
+ * with queue, 3 word table direct. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
 int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,

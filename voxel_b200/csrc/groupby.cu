@@ -37,6 +37,8 @@ namespace {
 constexpr int kGbThreads = 512;
 constexpr int kCountBits = 20;
 constexpr int kFixScale = 76;  // LSB weight 2^-76 of the group sums
+constexpr int kWordScale = 76; // LSB weight of the 32-bit word accumulators (the same)
+constexpr int kWords = 5;      // 160-bit word accumulator per group
 constexpr int kMaxWidth = 32;
 
 struct GlobalGroups {
@@ -107,42 +109,136 @@ __device__ __forceinline__ uint32_t key_bits(const uint64_t* __restrict__ packed
     return static_cast<uint32_t>(v & mask);
 }
 
+// Word form of a row value for the 32-bit table (MODE 1, 2): the magnitude
+// trunc(|x| * 2^76) -- the integer fix_from_double_s<76> produces -- as three
+// 32-bit words c0..c2 placed at word k0 of a 160-bit group accumulator.
+// Returns false for NaN, inf or |x| >= 2^63; zero and subnormals give c = 0.
+struct RowWords {
+    uint32_t c0, c1, c2;
+    int k0;
+};
+
+__device__ __forceinline__ bool row_words(double x, RowWords* w) {
+    const uint64_t b = static_cast<uint64_t>(__double_as_longlong(x));
+    const int ex = static_cast<int>((b >> 52) & 0x7FF);
+    w->c0 = w->c1 = w->c2 = 0;
+    w->k0 = 0;
+    if (ex >= 1023 + 63) return false;  // inf, NaN, |x| >= 2^63
+    if (ex == 0) return true;
+    uint64_t m = (b & ((1ull << 52) - 1)) | (1ull << 52);
+    int s = ex - 1075 + kWordScale;  // |x| * 2^76 = m * 2^s, s <= 86
+    if (s < 0) {
+        m = s > -64 ? (m >> -s) : 0;
+        s = 0;
+    }
+    const uint32_t ml = static_cast<uint32_t>(m), mh = static_cast<uint32_t>(m >> 32);
+    const uint32_t r = static_cast<uint32_t>(s) & 31;
+    w->k0 = s >> 5;  // <= 2, so words k0..k0+2 lie inside the 5-word accumulator
+    w->c0 = ml << r;
+    w->c1 = __funnelshift_l(ml, mh, r);
+    w->c2 = __funnelshift_l(mh, 0u, r);
+    return true;
+}
+
+// Propagates a carry (+1) or borrow (-1) into word j and upwards of a 5-word
+// two's-complement accumulator (exact modulo 2^160; no true sum needs more).
+__device__ __noinline__ void word_ripple(uint32_t* acc, int j, bool borrow) {
+    for (; j < kWords; ++j) {
+        const uint32_t old = atomicAdd(&acc[j], borrow ? 0xFFFFFFFFu : 1u);
+        if (borrow ? (old != 0u) : (old != 0xFFFFFFFFu)) break;
+    }
+}
+
+// Adds (neg: subtracts) a row's words to a group accumulator: the three
+// atomics are issued back to back, then each one's own wrap (read from its
+// returned old value) ripples into the next word.  Every wrap is accounted
+// exactly once, so concurrent updates compose to the exact sum.
+__device__ __forceinline__ void words_add(uint32_t* acc, const RowWords& w, bool neg) {
+    const uint32_t d0 = neg ? 0u - w.c0 : w.c0, d1 = neg ? 0u - w.c1 : w.c1, d2 = neg ? 0u - w.c2 : w.c2;
+    uint32_t o0 = 0, o1 = 0, o2 = 0;
+    if (w.c0) o0 = atomicAdd(&acc[w.k0], d0);
+    if (w.c1) o1 = atomicAdd(&acc[w.k0 + 1], d1);
+    if (w.c2) o2 = atomicAdd(&acc[w.k0 + 2], d2);
+    // add: carry when old + c wraps; subtract: borrow when old < c
+    const bool r0 = w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0);
+    const bool r1 = w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1);
+    const bool r2 = w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2);
+    if (r0) word_ripple(acc, w.k0 + 1, neg);
+    if (r1) word_ripple(acc, w.k0 + 2, neg);
+    if (r2) word_ripple(acc, w.k0 + 3, neg);
+}
+
+// 160-bit two's complement (5 words) -> 192-bit.
+__device__ __forceinline__ Fix3 fix_from_words(const uint32_t* w) {
+    const uint64_t lo = w[0] | (static_cast<uint64_t>(w[1]) << 32);
+    const uint64_t mid = w[2] | (static_cast<uint64_t>(w[3]) << 32);
+    const int64_t top = static_cast<int32_t>(w[4]);
+    return Fix3{lo, mid, static_cast<uint64_t>(top)};
+}
+
 // Per-warp queue of passing rows (ballot compaction): the atomic path then runs
 // with all 32 lanes converged instead of once per 32-row slice with ~6 lanes.
 constexpr int kQueue = 64;
+// Entries carry the row, its price and qty; the key decode and the price*qty
+// product happen when the queue is consumed, with all 32 lanes busy.
 struct WarpQueue {
-    uint32_t gid[kQueue];
-    double val[kQueue];
+    uint64_t row[kQueue];
     double price[kQueue];
+    int32_t qty[kQueue];
 };
 
-template <int RPT>
+// MODE 0: rows merged per group within the warp (match + shuffles), packed
+//         192-bit sum+count words updated with carrying 64-bit atomics;
+// MODE 1: every row added by its own lane to a 160-bit accumulator of five
+//         32-bit words (native 32-bit shared atomics, carries propagated),
+//         a 32-bit count, and min/max keys; rows reach the lanes through the
+//         warp queue (all 32 lanes busy);
+// MODE 2: as MODE 1, rows added where they are read (no queue).
+template <int RPT, int MODE>
 __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
     const double* __restrict__ price, const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo,
     int32_t qhi, GlobalGroups g, unsigned int* done, int32_t* out_keys, double* out_sum, double* out_min,
     double* out_max, uint64_t* out_count, uint64_t* out_ngroups, int* status) {
     constexpr int kTile = kGbThreads * RPT;
-    extern __shared__ __align__(16) unsigned char smem[];
-    unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem);  // 3 words per group
-    unsigned long long* s_mn = s_acc + 3 * card;
+    constexpr bool WORDS = MODE != 0;
+    extern __shared__ __align__(128) unsigned char smem[];
+    // MODE 0: 3 words per group (packed 192-bit sum + count), min, max.
+    // MODE 1, 2: min, max, then 5 32-bit words and a 32-bit count per group.
+    unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem);
+    unsigned long long* s_mn = WORDS ? s_acc : s_acc + 3 * card;
     unsigned long long* s_mx = s_mn + card;
+    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + card);  // MODE 1, 2
+    uint32_t* s_cnt = s_w + kWords * card;                      // MODE 1, 2
 
     auto reset_table = [&]() {
         for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
-            s_acc[3 * i] = 0;
-            s_acc[3 * i + 1] = 0;
-            s_acc[3 * i + 2] = 0;
+            if (WORDS) {
+#pragma unroll
+                for (int k = 0; k < kWords; ++k) s_w[kWords * i + k] = 0;
+                s_cnt[i] = 0;
+            } else {
+                s_acc[3 * i] = 0;
+                s_acc[3 * i + 1] = 0;
+                s_acc[3 * i + 2] = 0;
+            }
             s_mn[i] = ~0ull;
             s_mx[i] = 0;
         }
     };
     auto flush_table = [&]() {
         for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
-            Fix3 x{s_acc[3 * i], s_acc[3 * i + 1], s_acc[3 * i + 2]};
             unsigned int c;
-            Fix3 f = unpack_sum(x, &c);
-            if (!c) continue;
+            Fix3 f;
+            if (WORDS) {
+                c = s_cnt[i];
+                if (!c) continue;
+                f = fix_from_words(s_w + kWords * i);
+            } else {
+                Fix3 x{s_acc[3 * i], s_acc[3 * i + 1], s_acc[3 * i + 2]};
+                f = unpack_sum(x, &c);
+                if (!c) continue;
+            }
             fix_atomic_add(&g.sum[3 * i], f);
             atomicAdd(&g.cnt[i], static_cast<unsigned long long>(c));
             atomicMin(&g.mn[i], s_mn[i]);
@@ -154,8 +250,9 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     __syncthreads();
     const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
     const uint64_t ntiles = (n + kTile - 1) / kTile;
-    // embedded counts stay below 2^20 per group between flushes
-    const uint64_t tiles_per_flush = ((1ull << kCountBits) - 1) / kTile;
+    // rows between flushes: MODE 0 embeds counts in 20 bits; MODES 1, 2 sum
+    // rows below 2^139 in 160 bits (and count in 32)
+    const uint64_t tiles_per_flush = WORDS ? (1ull << 19) / kTile : ((1ull << kCountBits) - 1) / kTile;
     bool bad_value = false, bad_key = false;
     uint64_t since_flush = 0;
 
@@ -168,19 +265,41 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     // Entries of the same group are first combined by the lowest such lane
     // (match + shuffles), so a hot group costs one set of atomics per round
     // instead of one per row, and no two lanes of an atomic hit one address.
+    // MODE 1, 2: a row is added by its own lane; same-address lanes are handled
+    // by the shared-memory atomic unit (32-bit atomics stay fast under conflicts)
+    auto add_row = [&](uint32_t gi, double v, double p) {
+        if (gi >= card) {
+            bad_key = true;
+            return;
+        }
+        RowWords w;
+        if (row_words(v, &w)) words_add(s_w + kWords * gi, w, v < 0.0);
+        else bad_value = true;
+        atomicAdd(&s_cnt[gi], 1u);
+        const uint64_t k = f64_order_key(p);
+        if (k < s_mn[gi]) atomicMin(&s_mn[gi], static_cast<unsigned long long>(k));
+        if (k > s_mx[gi]) atomicMax(&s_mx[gi], static_cast<unsigned long long>(k));
+    };
     auto consume = [&](int cnt) {
         bool valid = lane < cnt;
-        uint32_t gi = valid ? Q.gid[lane] : 0;
+        uint32_t gi = 0;
+        double p = 0.0, v = 0.0;
+        if (valid) {
+            p = Q.price[lane];
+            gi = key_bits(packed, Q.row[lane], width, mask);
+            // one rounded multiply, as the reference materialises price*qty
+            v = __dmul_rn(p, static_cast<double>(Q.qty[lane]));
+        }
+        if (WORDS) {
+            if (valid) add_row(gi, v, p);
+            return;
+        }
         if (valid && gi >= card) {
             bad_key = true;
             valid = false;
         }
         Fix3 f{0, 0, 0};
-        double p = 0.0;
-        if (valid) {
-            p = Q.price[lane];
-            f = pack_row(fix_from_double_s<kFixScale>(Q.val[lane], &bad_value));
-        }
+        if (valid) f = pack_row(fix_from_double_s<kFixScale>(v, &bad_value));
         uint32_t key = valid ? gi : (0x80000000u | static_cast<uint32_t>(lane));
         unsigned peers = __match_any_sync(0xffffffffu, key);
         bool leader = valid && (__ffs(peers) - 1 == lane);
@@ -246,18 +365,20 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
         }
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
-            uint64_t r = r0 + k;
-            double p = pv[k];
-            int32_t q = qv[k];
-            bool pass = r < n && p > pthr && q >= qlo && q <= qhi;
+            const uint64_t r = r0 + k;
+            const double p = pv[k];
+            const int32_t q = qv[k];
+            const bool pass = r < n && p > pthr && q >= qlo && q <= qhi;
+            if (MODE == 2) {  // no queue: passing lanes add their rows directly
+                if (pass) add_row(key_bits(packed, r, width, mask), __dmul_rn(p, static_cast<double>(q)), p);
+                continue;
+            }
             unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
-                uint32_t gi = key_bits(packed, r, width, mask);
                 int pos = qn + __popc(m & lanemask_lt);
-                Q.gid[pos] = gi;
-                // one rounded multiply, as the reference materialises price*qty
-                Q.val[pos] = __dmul_rn(p, static_cast<double>(q));
+                Q.row[pos] = r;
                 Q.price[pos] = p;
+                Q.qty[pos] = q;
             }
             qn += __popc(m);
             if (qn >= 32) {
@@ -265,9 +386,9 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
                 consume(32);
                 __syncwarp();
                 if (lane < qn - 32) {
-                    Q.gid[lane] = Q.gid[32 + lane];
-                    Q.val[lane] = Q.val[32 + lane];
+                    Q.row[lane] = Q.row[32 + lane];
                     Q.price[lane] = Q.price[32 + lane];
+                    Q.qty[lane] = Q.qty[32 + lane];
                 }
                 __syncwarp();
                 qn -= 32;
@@ -667,7 +788,9 @@ int launch_tma(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
     return kOk;
 }
 
-template <int RPT>
+// dynamic shared memory of the MODE 1, 2 table: min, max (8 bytes each), five
+// accumulator words and a count (4 bytes each) per group -- the MODE 0 size
+template <int RPT, int MODE>
 int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
                const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
                int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
@@ -675,12 +798,12 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
     size_t smem = scan_groupby_smem_bytes(card);
     static thread_local uint32_t attr_set_for = 0;
     if (attr_set_for < card) {
-        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<RPT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
         attr_set_for = kMaxGroups;
     }
     int per_sm = 0;
-    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_groupby_kernel<RPT>, kGbThreads, smem));
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_groupby_kernel<RPT, MODE>, kGbThreads, smem));
     if (per_sm < 1) per_sm = 1;
     int sms = sm_count() > 0 ? sm_count() : 148;
     uint64_t ntiles = (n + kTile - 1) / kTile;
@@ -688,11 +811,12 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
     GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
-    scan_groupby_kernel<RPT><<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
+    scan_groupby_kernel<RPT, MODE><<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
         packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, S.g_done, ok, os, omn, omx, oc, ong,
         static_cast<int*>(S.status.p));
     VX_CUDA(cudaGetLastError());
     S.last_grid = static_cast<int>(grid);
+    S.last_kernel = MODE == 0 ? 0 : MODE + 1;
     return kOk;
 }
 
@@ -742,18 +866,17 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
         ((reinterpret_cast<uintptr_t>(packed) & 15) == 0))
         return launch_tma(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
                           out_min, out_max, out_count, out_ngroups, s);
-    last_kernel = 0;
+#define VX_LAUNCH_RPT(R, M)                                                                                    \
+    launch_rpt<R, M>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum, out_min, \
+                     out_max, out_count, out_ngroups, s)
+    if (mode == 1) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 1) : VX_LAUNCH_RPT(4, 1);
+    if (mode == 2) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 2) : VX_LAUNCH_RPT(4, 2);
     switch (rows_per_thread) {
-    case 8:
-        return launch_rpt<8>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
-                             out_min, out_max, out_count, out_ngroups, s);
-    case 16:
-        return launch_rpt<16>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
-                              out_min, out_max, out_count, out_ngroups, s);
-    default:
-        return launch_rpt<4>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
-                             out_min, out_max, out_count, out_ngroups, s);
+    case 8: return VX_LAUNCH_RPT(8, 0);
+    case 16: return VX_LAUNCH_RPT(16, 0);
+    default: return VX_LAUNCH_RPT(4, 0);
     }
+#undef VX_LAUNCH_RPT
 }
 
 int ScanGroupBy::check_status(cudaStream_t s) {
@@ -816,10 +939,10 @@ int noalloc_setup(cudaStream_t s, unsigned long long** base, int* per_sm) {
         VX_CUDA(cudaMemsetAsync(b + 4 * static_cast<size_t>(kMaxGroups), 0xFF, kMaxGroups * sizeof(unsigned long long),
                                 s));
         VX_CUDA(cudaStreamSynchronize(s));
-        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
         int occ = 0;
-        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_groupby_kernel<4>, kGbThreads,
+        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scan_groupby_kernel<4, 0>, kGbThreads,
                                                               scan_groupby_smem_bytes(kMaxGroups)));
         g_noalloc_per_sm[dev] = occ < 1 ? 1 : occ;
         g_noalloc_addr[dev] = b;
@@ -854,13 +977,28 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
 }
 
 int voxel_scan_groupby_tune(int variant) {
+    ScanGroupBy& S = scan_groupby_state();
+    if (variant == -1) variant = 1;
     if (variant == 0) {
-        scan_groupby_state().use_tma = true;
+        S.use_tma = true;
+        return kOk;
+    }
+    if (variant == 1 || variant == 2) {  // 32-bit word table, warp queue; 4 / 8 rows per thread
+        S.use_tma = false;
+        S.mode = 1;
+        S.rows_per_thread = 4 << (variant - 1);
+        return kOk;
+    }
+    if (variant == 3 || variant == 5) {  // 32-bit word table, direct; 4 / 8 rows per thread
+        S.use_tma = false;
+        S.mode = 2;
+        S.rows_per_thread = variant == 3 ? 4 : 8;
         return kOk;
     }
     if (variant != 4 && variant != 8 && variant != 16) return kErrInvalidArg;
-    scan_groupby_state().use_tma = false;
-    scan_groupby_state().rows_per_thread = variant;
+    S.use_tma = false;
+    S.mode = 0;
+    S.rows_per_thread = variant;
     return kOk;
 }
 
@@ -911,7 +1049,7 @@ int voxel_scan_groupby_noalloc_dev(const uint64_t* d_packed, size_t nwords, uint
     uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
-    scan_groupby_kernel<4><<<static_cast<unsigned>(grid), kGbThreads, scan_groupby_smem_bytes(c32), s>>>(
+    scan_groupby_kernel<4, 0><<<static_cast<unsigned>(grid), kGbThreads, scan_groupby_smem_bytes(c32), s>>>(
         d_packed, width, d_dict, c32, d_price, d_qty, n, pthr, qlo, qhi, g, done, d_keys, d_sum, d_min, d_max,
         d_count, d_ngroups, d_status);
     VX_CUDA(cudaGetLastError());

@@ -19,10 +19,11 @@ struct ScanGroupBy {
     uint32_t card_ = 0;
     unsigned long long *g_sum = nullptr, *g_cnt = nullptr, *g_mn = nullptr, *g_mx = nullptr;
     unsigned int* g_done = nullptr;
-    int rows_per_thread = 4;  // tuning knob of the atomic variant: 4, 8 or 16
+    int rows_per_thread = 4;  // rows per thread of the shared-table variants: 4, 8 (16: merged only)
     bool use_tma = false;     // TMA-fed private-table variant when the dictionary fits
+    int mode = 1;             // 0: merged 192-bit atomics, 1: 32-bit word table + warp queue, 2: word table direct
     int last_grid = 0;
-    int last_kernel = 0;      // 0: shared-atomic variant, 1: TMA-fed variant
+    int last_kernel = 0;      // 0: merged 192-bit atomics, 1: TMA-fed, 2: word table + queue, 3: word table direct
 
     int prepare(uint32_t card, cudaStream_t s);
     int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
