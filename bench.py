@@ -117,6 +117,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_config(d: dict, world: int) -> dict:
+    """The `config` object both arms print."""
+    return {"workload": "scan+groupby 2^25 rows/GPU: key i32 zipf(1.1) over 1000, dict+bitpack 10-bit; "
+                        "price f64 lognormal(3,1); qty i32 U[1,100]; price>20 AND qty BETWEEN 10 AND 50; "
+                        "GROUP BY key SUM(price*qty) COUNT MIN MAX",
+            "rows_per_gpu": d["n"], "algorithmic_bytes_per_step": algorithmic_bytes(d),
+            "l2": "inputs (444.6 MB) larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}"}
+
+
 def make_data(rank: int, rows: int) -> dict:
     import inputs
 
@@ -162,8 +171,8 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": algorithmic_bytes(d) / v / 1e6,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)",
-            "config": {"workload": "scan+groupby 2^25 rows, key zipf1.1/1000 dict+bitpack10, price>20 AND qty 10..50"},
+            "data": "synthetic (seeded numpy PCG64, configs' distributions)",
+            "config": workload_config(d, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -304,11 +313,7 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64, configs' distributions)",
-        "config": {"workload": "scan+groupby 2^25 rows/GPU: key i32 zipf(1.1) over 1000, dict+bitpack 10-bit; "
-                               "price f64 lognormal(3,1); qty i32 U[1,100]; price>20 AND qty BETWEEN 10 AND 50; "
-                               "GROUP BY key SUM(price*qty) COUNT MIN MAX",
-                   "rows_per_gpu": d["n"], "algorithmic_bytes_per_step": nbytes, "groups": int(ng),
-                   "l2": "inputs (444.6 MB) larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}"},
+        "config": workload_config(d, world),
         "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": peak, "unit": "GB/s",
                      "frac": kernel_gbs / peak, "traffic": traffic, "peak_source": peak_kind,
                      "kernel": "scan_groupby_kernel", "launch_ms_mean": statistics.mean(launch_ms),
