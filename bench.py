@@ -29,11 +29,15 @@ import sys
 import threading
 import time
 
+import ctypes as C
+
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+from voxel_b200 import capi  # noqa: E402  (loads the library lazily)
 
 METRIC = "filter+agg GB/s vs HBM peak"
 UNIT = "GB/s"
@@ -178,6 +182,321 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# Secondary workloads (one JSON line each, same keys as the headline line).
+# --------------------------------------------------------------------------
+
+def _common_line(metric, unit, value, world, args, ms_per_step, config, roofline, cpu, e2e, clk, launches, dtype,
+                 higher=True):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": higher, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": config,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches}
+
+
+def _roofline(kernel, algo_bytes, launch_ms):
+    peak, kind = measured_peak()
+    gbs = algo_bytes / (launch_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "traffic": ncu_traffic(kernel), "peak_source": kind, "kernel": kernel, "launch_ms_mean": launch_ms,
+            "frac_of_nominal_8000": gbs / 8000.0}
+
+
+def _max_over_ranks(dist, dev, x):
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def workload_scan(args, L, rank, world, local, dist, dev):
+    """Fast-path filter+sum over 2^28 f64 U[0,1000) (mt19937_64 seed 42, the
+    reference's validation distribution), threshold 500: the streaming case of
+    the config-1 program, run through the engine with a device segment."""
+    import torch
+
+    from voxel_b200 import bytecode as bc
+
+    n = args.rows if args.rows != ROWS else 1 << 28
+    host = np.empty(n, np.float64)
+    capi.datagen().vgen_uniform_f64_mt(42 + rank, n, 0.0, 1000.0, host.ctypes.data)
+    dcol = torch.from_numpy(host).to(dev)
+    code = np.asarray(bc.filter_sum_program(), np.uint32)
+    nbytes = n * 8
+
+    def run_engine(e):
+        L.voxel_engine_set_scalar(e, 0, 0)
+        L.voxel_engine_set_scalar(e, 1, 0)
+        L.voxel_engine_set_scalar(e, 2, n)
+        L.voxel_engine_set_scalar_f64(e, 3, 500.0)
+        L.voxel_engine_set_scalar(e, 4, 4)
+        L.voxel_engine_load_program(e, code.ctypes.data, code.size)
+        if L.voxel_engine_run_status(e):
+            raise RuntimeError(capi.last_error())
+
+    e = L.voxel_engine_create_f64()
+    L.voxel_engine_add_segment_device(e, dcol.data_ptr(), n)
+    for _ in range(args.warmup):
+        run_engine(e)
+    dev_ms, wall = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            run_engine(e)
+            wall.append((time.perf_counter() - t0) * 1e3)
+            dev_ms.append(L.voxel_engine_last_device_ms(e))
+    result = L.voxel_engine_get_scalar_f64(e, 0)
+    L.voxel_engine_destroy(e)
+    launch_ms = _max_over_ranks(dist, dev, statistics.mean(dev_ms))
+    step_ms = _max_over_ranks(dist, dev, statistics.mean(wall))
+    # end to end: the borrowed host buffer (pinned) is uploaded by every run
+    pinned = torch.from_numpy(host).pin_memory()
+    e = L.voxel_engine_create_f64()
+    L.voxel_engine_add_segment(e, pinned.data_ptr(), n)
+    run_engine(e)
+    w0 = time.perf_counter()
+    e_steps = max(3, min(args.steps, 10))
+    for _ in range(e_steps):
+        run_engine(e)
+    e_ms = _max_over_ranks(dist, dev, (time.perf_counter() - w0) * 1e3 / e_steps)
+    L.voxel_engine_destroy(e)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.have_ref():
+            m = 1 << 26
+            out = C.c_double(0)
+            threads = os.cpu_count() or 1
+            us = oracle.ref().vref_time_filter_sum_f64(2, code.ctypes.data, code.size, host.ctypes.data, m, 500.0, 2,
+                                                       5, threads, C.byref(out))
+            cpu = {"value": m * 8 / (us * 1e-6) / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"Engine<f64>::RunParallel, first {m} rows, median of 5 after 2 warm-ups"}
+    line = _common_line(
+        "fast-path filter+sum GB/s vs HBM peak", UNIT, world * nbytes / (launch_ms * 1e-3) / 1e9, world, args,
+        step_ms,
+        {"workload": f"engine fast path VLOAD,VFILTER_GT,VSUM,ADDF,ADD,CMP,JNZ over {n} f64 U[0,1000) "
+                     "(mt19937_64 seed 42), threshold 500; device-resident segment",
+         "rows_per_gpu": n, "algorithmic_bytes_per_step": nbytes, "result_R0": result,
+         "l2": "input (2.1 GB) larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}",
+         "ms_per_step_note": "wall time of Engine::Run incl. launch, sync and register read-back"},
+        _roofline("fsum_kernel", nbytes, launch_ms), cpu,
+        {"value": world * nbytes / (e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+         "d2h_bytes_per_step": 8 * 64, "ms_per_step": e_ms},
+        clk.summary(), args.steps, "f64")
+    return line
+
+
+def workload_sort(args, L, rank, world, local, dist, dev):
+    """Stable LSD radix sort of 2^28 u64 keys (SplitMix64, seed 3001) with u32
+    row ids: keys ascending and the stable permutation."""
+    import torch
+
+    n = args.rows if args.rows != ROWS else 1 << 28
+    keys = np.empty(n, np.uint64)
+    capi.datagen().vgen_splitmix64(3001 + rank, n, keys.ctypes.data)
+    src = torch.from_numpy(keys.view(np.int64)).to(dev)
+    work = torch.empty_like(src)
+    idx = torch.empty(n, dtype=torch.int32, device=dev)
+    tmp_bytes = L.voxel_radix_sort_tmp_bytes(capi.U64, n)
+    tmp = torch.empty(tmp_bytes, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(dev)
+    passes = 8
+    nbytes = n * (8 + 2 * 12 * passes)
+
+    iota = torch.arange(n, dtype=torch.int32, device=dev)  # the payload: row ids, sorted along with the keys
+
+    def step(ev=None):
+        with torch.cuda.stream(stream):
+            work.copy_(src)
+            idx.copy_(iota)
+        if ev:
+            ev[0].record(stream)
+        st = L.voxel_radix_sort_dev(capi.U64, work.data_ptr(), idx.data_ptr(), n, tmp.data_ptr(), tmp_bytes,
+                                    stream.cuda_stream)
+        if ev:
+            ev[1].record(stream)
+        if st:
+            raise RuntimeError(capi.last_error())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            step(evs[i])
+        torch.cuda.synchronize()
+    launch_ms = _max_over_ranks(dist, dev, statistics.mean(a.elapsed_time(b) for a, b in evs))
+    # check the last result: ascending as u64, and work == src[idx]
+    flip = work ^ torch.tensor(-(1 << 63), dtype=torch.int64, device=dev)
+    checked = bool(torch.all(flip[1:] >= flip[:-1]).item()) and bool(torch.equal(src[idx.long()], work))
+    del flip
+    # end to end: host keys in, sorted keys + ids out
+    hk = torch.from_numpy(keys.view(np.int64)).pin_memory()
+    hout = torch.empty(n, dtype=torch.int64).pin_memory()
+    hidx = torch.empty(n, dtype=torch.int32).pin_memory()
+    e_steps = max(3, min(args.steps, 5))
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e_steps):
+        with torch.cuda.stream(stream):
+            work.copy_(hk, non_blocking=True)
+            idx.copy_(iota)
+        st = L.voxel_radix_sort_dev(capi.U64, work.data_ptr(), idx.data_ptr(), n, tmp.data_ptr(), tmp_bytes,
+                                    stream.cuda_stream)
+        if st:
+            raise RuntimeError(capi.last_error())
+        with torch.cuda.stream(stream):
+            hout.copy_(work, non_blocking=True)
+            hidx.copy_(idx, non_blocking=True)
+        stream.synchronize()
+    e_ms = _max_over_ranks(dist, dev, (time.perf_counter() - w0) * 1e3 / e_steps)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.have_ref():
+            m = 1 << 23
+            k = keys[:m].copy()
+            ids = np.arange(m, dtype=np.uint32)
+            t0 = time.perf_counter()
+            oracle.ref().vref_radix_sort_u64(k.ctypes.data, ids.ctypes.data, m)
+            secs = time.perf_counter() - t0
+            cpu = {"value": m / secs / 1e6, "unit": "M keys/s", "cores": 1, "kind": "reference",
+                   "sample": f"RadixSort<u64>::Sort on the first {m} keys (single-threaded, as in the reference)"}
+    line = _common_line(
+        "radix sort M keys/s", "M keys/s", world * n / (launch_ms * 1e-3) / 1e6, world, args, launch_ms,
+        {"workload": f"stable LSD radix sort, {n} u64 keys SplitMix64 seed 3001 + u32 row ids",
+         "rows_per_gpu": n, "result_checked": checked, "passes": passes, "algorithmic_bytes_per_step": nbytes,
+         "l2": "keys (2.1 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
+        _roofline("radix_onesweep", nbytes, launch_ms), cpu,
+        {"value": world * n / (e_ms * 1e-3) / 1e6, "unit": "M keys/s", "h2d_bytes_per_step": n * 8,
+         "d2h_bytes_per_step": n * 12, "ms_per_step": e_ms},
+        clk.summary(), args.steps, "u64")
+    return line
+
+
+def workload_join(args, L, rank, world, local, dist, dev):
+    """Hash join: build 2^24 unique i64 keys + u64 payload, probe 2^29 keys
+    (90% Zipf(0.8) over the build keys, 10% guaranteed misses); all matching
+    (probe, build) pairs in probe order plus COUNT and SUM(payload)."""
+    import torch
+
+    nb = 1 << 24
+    npr = args.rows if args.rows != ROWS else 1 << 29
+    bkeys = np.empty(nb, np.uint64)
+    capi.datagen().vgen_splitmix64(3002 + rank, nb, bkeys.ctypes.data)
+    bkeys &= np.uint64(0xFFFFFFFFFFFFFFFE)  # build keys even, miss keys odd
+    build = torch.from_numpy(bkeys.view(np.int64)).to(dev)
+    payload = torch.arange(nb, dtype=torch.int64, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(3003 + rank)
+    w = torch.arange(1, nb + 1, dtype=torch.float64, device=dev).pow_(-0.8)
+    cdf = torch.cumsum(w, 0)
+    cdf /= cdf[-1].clone()
+    del w
+    perm = torch.randperm(nb, device=dev, generator=g)
+    probe = torch.empty(npr, dtype=torch.int64, device=dev)
+    chunk = 1 << 26
+    for s0 in range(0, npr, chunk):
+        m = min(chunk, npr - s0)
+        u = torch.rand(m, dtype=torch.float64, device=dev, generator=g)
+        r = torch.searchsorted(cdf, u).clamp_(max=nb - 1)
+        k = build[perm[r]]
+        miss = torch.rand(m, device=dev, generator=g) < 0.1
+        odd = torch.randint(0, 1 << 62, (m,), device=dev, generator=g) * 2 + 1
+        probe[s0:s0 + m] = torch.where(miss, odd, k)
+        del u, r, k, miss, odd
+    del cdf, perm
+    left = torch.empty(npr, dtype=torch.int32, device=dev)
+    right = torch.empty(npr, dtype=torch.int32, device=dev)
+    cs = torch.zeros(2, dtype=torch.int64, device=dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.synchronize()
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        st = L.voxel_hashjoin_i64_dev(build.data_ptr(), payload.data_ptr(), nb, probe.data_ptr(), npr,
+                                      left.data_ptr(), right.data_ptr(), npr, 1, cs.data_ptr(), stream.cuda_stream)
+        if ev:
+            ev[1].record(stream)
+        if st:
+            raise RuntimeError(capi.last_error())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    matches = int(cs[0].item())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            step(evs[i])
+        torch.cuda.synchronize()
+    launch_ms = _max_over_ranks(dist, dev, statistics.mean(a.elapsed_time(b) for a, b in evs))
+    nbytes = nb * 16 + npr * 8 + matches * 8
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.have_ref():
+            m = 1 << 23
+            hb = bkeys.view(np.int64).copy()
+            hp = probe[:m].cpu().numpy()
+            hl = np.empty(m, np.uint32)
+            hr = np.empty(m, np.uint32)
+            t0 = time.perf_counter()
+            got = oracle.ref().vref_hashjoin_i64(hb.ctypes.data, nb, hp.ctypes.data, m, hl.ctypes.data,
+                                                 hr.ctypes.data, m, 1)
+            secs = time.perf_counter() - t0
+            sb = nb * 16 + m * 8 + got * 8
+            cpu = {"value": sb / secs / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"HashJoin<i64> Build({nb}) + ProbeAllMatches of the first {m} probe keys, one run "
+                             f"({m / secs / 1e6:.1f} M probes/s incl. build)"}
+    line = _common_line(
+        "hash join GB/s (algorithmic bytes)", UNIT, world * nbytes / (launch_ms * 1e-3) / 1e9, world, args,
+        launch_ms,
+        {"workload": f"build {nb} unique i64 + u64 payload; probe {npr} i64, 90% Zipf(0.8) over build keys, 10% "
+                     "misses; all pairs in probe order + COUNT + SUM(payload)",
+         "build_rows": nb, "probe_rows_per_gpu": npr, "matches": matches, "algorithmic_bytes_per_step": nbytes,
+         "m_probes_per_s": npr / (launch_ms * 1e-3) / 1e6, "parallelism": f"replicas x{world}",
+         "l2": "probe (4.3 GB) larger than L2; no flush"},
+        _roofline("hashjoin", nbytes, launch_ms), cpu,
+        {"value": None, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+         "note": "device-resident inputs only for this workload"},
+        clk.summary(), args.steps, "i64")
+    return line
+
+
+WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join}
+
+
+def run_workload(args, rank, world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    L = capi.lib()
+    line = WORKLOADS[args.workload](args, L, rank, world, local, dist, dev)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -186,6 +505,9 @@ def main() -> None:
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join"],
+                    help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
+                         "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -194,6 +516,9 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.workload != "groupby":
+        run_workload(args, rank, world, local)
         return
 
     import torch
@@ -206,8 +531,6 @@ def main() -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    from voxel_b200 import capi
 
     L = capi.lib()
     d = make_data(rank, args.rows)

@@ -188,6 +188,8 @@ def datagen() -> C.CDLL:
         _datagen = C.CDLL(DATAGEN_PATH)
         _datagen.vgen_uniform_f64_mt.restype = None
         _datagen.vgen_uniform_f64_mt.argtypes = [u64, sz, dbl, dbl, vp]
+        _datagen.vgen_splitmix64.restype = None
+        _datagen.vgen_splitmix64.argtypes = [u64, sz, vp]
     return _datagen
 
 

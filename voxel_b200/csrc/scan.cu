@@ -96,6 +96,124 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
     }
 }
 
+// Specialised kernel for the dominant shape, the reference's fast path and the
+// Tier-0 loops of the same form: one column, one comparison atom, SUM of the
+// lanes that pass (failing lanes are zero, as VFILTER writes them), folded into
+// one accumulator.  The compare is a template parameter, so a group costs a
+// few instructions instead of the generic per-lane interpretation; the fold,
+// block partials and finalisation are the generic ones, so results are the
+// same bits.
+template <int OP, typename T>
+__device__ __forceinline__ bool cmp_op(T v, T t) {
+    if constexpr (OP == 0) return v == t;
+    else if constexpr (OP == 1) return v != t;
+    else if constexpr (OP == 2) return v < t;
+    else if constexpr (OP == 3) return v <= t;
+    else if constexpr (OP == 4) return v > t;
+    else return v >= t;
+}
+
+constexpr int kFsUnroll = 2;  // 2 groups in flight per thread, 6 blocks per SM (measured best)
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(kThreads, 6) fsum_kernel(const __grid_constant__ ScanParams p, int vec,
+                                                          ScanPartial* part, unsigned int* done,
+                                                          ScanResult* out) {
+    constexpr int KL = 32 / sizeof(T);
+    const T thr = from_bits<T>(p.atom[0].thr);
+    const uint8_t op = p.red[0].acc;
+    Acc acc[1];
+    acc[0].u = 0;
+    acc[0].k = {0.0, 0.0};
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t lastj = p.ngroups - 1;
+    for (uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j0 < p.ndata;
+         j0 += stride * kFsUnroll) {
+        T v[kFsUnroll][1][KL];
+#pragma unroll
+        for (int u = 0; u < kFsUnroll; ++u) {
+            uint64_t j = j0 + u * stride;
+            if (j < p.ndata) load_group<T, 1>(p, j, vec != 0, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kFsUnroll; ++u) {
+            uint64_t j = j0 + u * stride;
+            if (j < p.ndata) {
+                T sum = T(0);  // left to right in T, like VSUM
+#pragma unroll
+                for (int l = 0; l < KL; ++l) sum = t_add<T>(sum, cmp_op<OP>(v[u][0][l], thr) ? v[u][0][l] : T(0));
+                const uint64_t r = set_scalar<T>(sum);
+                acc_fold<T>(acc[0], op, r);
+                if (j == lastj) out->last[0] = r;
+            }
+        }
+    }
+    __shared__ Acc blk[1];
+    block_reduce<T, 1, kThreads>(p, acc, blk);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x].u[0] = blk[0].u;
+        part[blockIdx.x].s[0] = blk[0].k.s;
+        part[blockIdx.x].c[0] = blk[0].k.c;
+    }
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    acc[0].u = 0;
+    acc[0].k = {0.0, 0.0};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        Acc o;
+        o.u = __ldcg(&part[b].u[0]);
+        o.k.s = __ldcg(&part[b].s[0]);
+        o.k.c = __ldcg(&part[b].c[0]);
+        acc_merge<T>(acc[0], op, o);
+    }
+    block_reduce<T, 1, kThreads>(p, acc, blk);
+    if (threadIdx.x == 0) {
+        *done = 0;
+        finalize_scan<T, 1, 1>(p, blk, out);
+    }
+}
+
+bool fsum_shape(const ScanParams& p) {
+    if (p.ncols != 1 || p.natoms != 1 || p.nred != 1) return false;
+    const Atom& a = p.atom[0];
+    const Red& r = p.red[0];
+    if (a.col != 0 || a.op > 5) return false;
+    if (r.kind != kRedSum || r.pmask != 1u || r.a.kind != kOpCol || r.a.col != 0) return false;
+    if (!(r.b.kind == kOpZero || (r.b.kind == kOpConst && r.b.bits == 0))) return false;
+    return r.acc == kAccAdd || r.acc == kAccSub || r.acc == kAccAddF || r.acc == kAccTAdd;
+}
+
+int fsum_grid(uint64_t ndata) {
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t need = (ndata + static_cast<uint64_t>(kThreads) * kFsUnroll - 1) / (static_cast<uint64_t>(kThreads) * kFsUnroll);
+    uint64_t cap = static_cast<uint64_t>(sms) * 6;  // one wave of resident blocks
+    uint64_t g = need < cap ? need : cap;
+    return g < 1 ? 1 : static_cast<int>(g);
+}
+
+template <typename T>
+int launch_fsum(const ScanParams& p, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    ScanPartial* part = static_cast<ScanPartial*>(scratch);
+    unsigned int* done = reinterpret_cast<unsigned int*>(static_cast<char*>(scratch) + kMaxBlocks * sizeof(ScanPartial));
+    const int vec = (reinterpret_cast<uintptr_t>(p.col[0]) + p.off0 * sizeof(T)) % 16 == 0 ? 1 : 0;
+    const int grid = fsum_grid(p.ndata);
+    switch (p.atom[0].op) {
+    case 0: fsum_kernel<T, 0><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    case 1: fsum_kernel<T, 1><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    case 2: fsum_kernel<T, 2><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    case 3: fsum_kernel<T, 3><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    case 4: fsum_kernel<T, 4><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    default: fsum_kernel<T, 5><<<grid, kThreads, 0, s>>>(p, vec, part, done, d_out); break;
+    }
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
 template <typename T, int NC, int NR, int UNROLL>
 int launch_t(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
     ScanPartial* part = static_cast<ScanPartial*>(scratch);
@@ -112,6 +230,7 @@ int launch_t(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cu
 
 template <typename T>
 int dispatch(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    if (fsum_shape(p)) return launch_fsum<T>(p, d_out, scratch, s);
     if (p.ncols <= 1 && p.nred <= 2) return launch_t<T, 1, 2, 4>(p, grid, d_out, scratch, s);
     if (p.ncols <= 1) return launch_t<T, 1, kMaxRed, 2>(p, grid, d_out, scratch, s);
     return launch_t<T, kMaxCols, kMaxRed, 1>(p, grid, d_out, scratch, s);
