@@ -472,7 +472,115 @@ def workload_join(args, L, rank, world, local, dist, dev):
     return line
 
 
-WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join}
+def _device_column(dtype, n, g, dev):
+    """Column ~ U[0,1000) cast per element type (floor for integers), on the device."""
+    import torch
+
+    x = torch.rand(n, dtype=torch.float64, device=dev, generator=g).mul_(1000.0)
+    if dtype == capi.F64:
+        return x
+    if dtype == capi.F32:
+        return x.float()
+    x = x.floor_()
+    return x.to(torch.int64) if dtype in (capi.I64, capi.U64) else x.to(torch.int32)
+
+
+def workload_batch(args, L, rank, world, local, dist, dev):
+    """4,096 filter/aggregate programs (1-4 predicates, SUM/COUNT/MIN/MAX, six
+    element types, log-uniform lengths 1K-16M, log-uniform selectivity) with
+    their selection vectors: one graph-launched batch sized by the learned
+    estimator against one-launch-per-program exact two-pass kernels."""
+    import torch
+
+    from voxel_b200 import batch as B
+    from voxel_b200 import templates as T
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(4001 + rank)
+    # estimator: trained on engine-measured runs over separate generated columns
+    t0 = time.perf_counter()
+    trng = np.random.default_rng(4100 + rank)
+    tcols = []
+    for i in range(args.train_columns):
+        dt = i % 6
+        n = int(2 ** trng.uniform(10, 18)) // 8 * 8
+        tcols.append((dt, _device_column(dt, n, g, dev)))
+    model, q_m, q_b, nruns = B.train_estimator(tcols, args.train_runs, seed=11 + rank, epochs=20)
+    del tcols
+    train_s = time.perf_counter() - t0
+    # the batch
+    rng = np.random.default_rng(4001 + rank)
+    progs, cols = [], []
+    for _ in range(args.programs):
+        dt = int(rng.integers(6))
+        kl = T.K_LANES[dt]
+        n = max(kl, int(2 ** rng.uniform(10, 24)) // kl * kl)
+        progs.append(T.random_program(dt, rng))
+        cols.append(_device_column(dt, n, g, dev))
+    torch.cuda.synchronize()
+    nbytes = int(sum(c.numel() * c.element_size() for c in cols))
+    stream = torch.cuda.Stream(dev)
+    lb = B.LearnedBatch(model)
+    for p_, c in zip(progs, cols):
+        lb.add(p_, c)
+    t1 = time.perf_counter()
+    lb.prepare(stream)
+    prep_s = time.perf_counter() - t1
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3
+
+    for _ in range(args.warmup):
+        res = lb.run()
+    ev_ms, wall_ms = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            res, em, wm = timed(lb.run)
+            ev_ms.append(em)
+            wall_ms.append(wm)
+    step_ms = _max_over_ranks(dist, dev, statistics.mean(wall_ms))
+    plain, p_ev, p_wall = timed(lambda: B.plain_two_pass(progs, cols, stream))
+    p_wall = _max_over_ranks(dist, dev, p_wall)
+    # the batch must reproduce the plain kernels exactly
+    mism = 0
+    for a, b in zip(res, plain):
+        if a.registers != b.registers or a.count != b.count or not torch.equal(a.selection, b.selection):
+            mism += 1
+    exact = np.array([r.count for r in res], np.float64)
+    q = np.maximum((lb.est + 1) / (exact + 1), (exact + 1) / (lb.est + 1))
+    over = int(sum(r.overflowed for r in res))
+    lb.close()
+    line = _common_line(
+        "batched+learned GB/s (4096 programs, selection vectors)", UNIT, world * nbytes / (step_ms * 1e-3) / 1e9,
+        world, args, step_ms,
+        {"workload": f"{args.programs} programs: 1-4 conjunctive predicates + SUM/COUNT/MIN/MAX, dtypes uniform over "
+                     "6, lengths log-uniform 2^10..2^24, selectivity log-uniform 1e-4..0.9; every program also "
+                     "writes its selection vector",
+         "column_bytes_per_step": nbytes, "programs": args.programs,
+         "plain_two_pass_ms": p_wall, "plain_two_pass_gbs": nbytes / (p_wall * 1e-3) / 1e9,
+         "speedup_vs_plain": p_wall / step_ms, "batched_device_ms": statistics.mean(ev_ms),
+         "mismatches_vs_plain": mism, "overflowed_programs": over,
+         "q_error_batch": {"median": float(np.median(q)), "p90": float(np.percentile(q, 90)),
+                           "p99": float(np.percentile(q, 99)), "max": float(q.max())},
+         "estimator": {"training_runs": int(nruns), "train_s": train_s, "prepare_s": prep_s,
+                       "heldout_q_median_mlp": float(np.median(q_m)), "heldout_q_p90_mlp": float(np.percentile(q_m, 90)),
+                       "heldout_q_median_hist": float(np.median(q_b)), "heldout_q_p90_hist": float(np.percentile(q_b, 90))},
+         "l2": "columns (tens of GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
+        None, None,
+        {"value": None, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": args.programs * 528,
+         "note": "device-resident columns; per step the program results (registers, counts) come back to the host"},
+        clk.summary(), args.steps * 1, "mixed")
+    return line
+
+
+WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join, "batch": workload_batch}
 
 
 def run_workload(args, rank, world, local):
@@ -505,9 +613,13 @@ def main() -> None:
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join"],
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch"],
                     help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
-                         "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29")
+                         "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29; batch: 4096 "
+                         "programs, batched + learned sizing against plain two-pass kernels")
+    ap.add_argument("--programs", type=int, default=4096)
+    ap.add_argument("--train-runs", type=int, default=200_000)
+    ap.add_argument("--train-columns", type=int, default=512)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

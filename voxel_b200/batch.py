@@ -1,0 +1,201 @@
+"""Batched execution of many bytecode programs with learned output sizing.
+
+Each program is one filter/aggregate loop over one device-resident column.  A
+`LearnedBatch` runs all of them in one persistent launch of the batched
+executor (`voxel_batch_*`, replayed from a CUDA graph) and also writes each
+program's selection vector (the ascending row ids that satisfy all of its
+predicates).  Selection buffers are sized from the learned estimator: every
+column is sketched once on the device, the MLP predicts each program's
+selected-row count, and the buffer gets that estimate times a margin.  The
+estimate never changes a result: the executor always reports the exact count,
+and a program whose buffer was too small is re-run with a buffer of exactly
+that size (count, then write).
+
+`plain_two_pass` is the baseline the batch replaces: one launch per program to
+count, then one more to write into an exactly sized buffer.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+from . import estimator as E
+
+
+@dataclass
+class ProgramResult:
+    registers: list
+    count: int
+    selection: object = None  # device int32 tensor view (row ids), or None
+    estimate: float = 0.0
+    overflowed: bool = False
+
+
+def _batch_add(L, b, prog, dcol, n, want, cap, sel_ptr):
+    regs = np.array(prog.registers(n), np.uint64)
+    code = np.asarray(prog.code, np.uint32)
+    st = L.voxel_batch_add(b, prog.dtype, code.ctypes.data, code.size, regs.ctypes.data, dcol.data_ptr(), n, want,
+                           cap, sel_ptr)
+    if st:
+        raise RuntimeError(capi.last_error())
+
+
+def _batch_out(L, b, i):
+    regs = np.zeros(64, np.uint64)
+    cnt = np.zeros(1, np.uint64)
+    ovf = np.zeros(1, np.int32)
+    if L.voxel_batch_result(b, i, regs.ctypes.data, cnt.ctypes.data, ovf.ctypes.data):
+        raise RuntimeError(capi.last_error())
+    return [int(x) for x in regs], int(cnt[0]), bool(ovf[0])
+
+
+@dataclass
+class LearnedBatch:
+    model: "E.Model | None"
+    margin: float = 2.0
+    slack: int = 256
+    programs: list = field(default_factory=list)
+    columns: list = field(default_factory=list)  # (dtype, device tensor) per program
+    sketches: dict = field(default_factory=dict)
+
+    def add(self, program, dcol) -> int:
+        self.programs.append(program)
+        self.columns.append(dcol)
+        return len(self.programs) - 1
+
+    # -- sizing ---------------------------------------------------------------
+    def estimates(self) -> np.ndarray:
+        """Predicted selected rows per program (sketches are cached per column)."""
+        feats = []
+        for prog, dcol in zip(self.programs, self.columns):
+            key = dcol.data_ptr()
+            if key not in self.sketches:
+                self.sketches[key] = E.sketch(prog.dtype, dcol.data_ptr(), dcol.numel())
+            feats.append(E.features(prog.dtype, self.sketches[key], prog.preds))
+        X = np.asarray(feats, np.float32)
+        if self.model is None:  # no model: histogram + independence estimate
+            return np.array([E.baseline_estimate(p.dtype, self.sketches[c.data_ptr()], p.preds)[0]
+                             for p, c in zip(self.programs, self.columns)])
+        Y = self.model.predict(X)
+        return np.array([E.decode(y, c.numel())[0] for y, c in zip(Y, self.columns)])
+
+    def prepare(self, stream=None):
+        """Sizes the buffers and records the batch (one CUDA graph)."""
+        import torch  # noqa: PLC0415
+
+        L = capi.lib()
+        est = self.estimates()
+        caps = [int(min(c.numel(), np.ceil(max(e, 0.0) * self.margin) + self.slack))
+                for e, c in zip(est, self.columns)]
+        self.est = est
+        self.caps = caps
+        offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+        dev = self.columns[0].device
+        self.pool = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=dev)
+        self.offs = offs
+        self.b = L.voxel_batch_create()
+        base = self.pool.data_ptr()
+        for i, (prog, dcol) in enumerate(zip(self.programs, self.columns)):
+            _batch_add(L, self.b, prog, dcol, dcol.numel(), 1, caps[i], base + 4 * int(offs[i]))
+        self.stream = stream
+        return self
+
+    # -- execution ------------------------------------------------------------
+    def run(self):
+        """One graph launch of every program; undersized buffers are re-run
+        exactly.  Returns a list of ProgramResult."""
+        import torch  # noqa: PLC0415
+
+        L = capi.lib()
+        sh = self.stream.cuda_stream if self.stream is not None else None
+        if L.voxel_batch_launch(self.b, 1, sh) or L.voxel_batch_fetch(self.b, sh):
+            raise RuntimeError(capi.last_error())
+        out, redo = [], []
+        for i in range(len(self.programs)):
+            regs, cnt, ovf = _batch_out(L, self.b, i)
+            sel = self.pool[int(self.offs[i]):int(self.offs[i]) + cnt] if not ovf else None
+            out.append(ProgramResult(regs, cnt, sel, float(self.est[i]), ovf))
+            if ovf:
+                redo.append(i)
+        if redo:  # exact write pass for the programs whose estimate was low
+            b2 = L.voxel_batch_create()
+            bufs = []
+            try:
+                for i in redo:
+                    buf = torch.empty(max(out[i].count, 1), dtype=torch.int32, device=self.pool.device)
+                    bufs.append(buf)
+                    _batch_add(L, b2, self.programs[i], self.columns[i], self.columns[i].numel(), 1, out[i].count,
+                               buf.data_ptr())
+                if L.voxel_batch_launch(b2, 0, sh) or L.voxel_batch_fetch(b2, sh):
+                    raise RuntimeError(capi.last_error())
+                for k, i in enumerate(redo):
+                    regs, cnt, ovf = _batch_out(L, b2, k)
+                    if ovf or cnt != out[i].count:
+                        raise RuntimeError("exact re-run disagrees with the batch")
+                    out[i].selection = bufs[k][:cnt]
+            finally:
+                L.voxel_batch_destroy(b2)
+        return out
+
+    def close(self):
+        if getattr(self, "b", None):
+            capi.lib().voxel_batch_destroy(self.b)
+            self.b = None
+
+
+def plain_two_pass(programs, columns, stream=None):
+    """One launch per program to count, then one to write the selection into an
+    exactly sized buffer.  Returns a list of ProgramResult."""
+    import torch  # noqa: PLC0415
+
+    L = capi.lib()
+    sh = stream.cuda_stream if stream is not None else None
+    out = []
+    for prog, dcol in zip(programs, columns):
+        n = dcol.numel()
+        b = L.voxel_batch_create()
+        try:
+            _batch_add(L, b, prog, dcol, n, 0, 0, None)
+            if L.voxel_batch_launch(b, 0, sh) or L.voxel_batch_fetch(b, sh):
+                raise RuntimeError(capi.last_error())
+            _, cnt, _ = _batch_out(L, b, 0)
+        finally:
+            L.voxel_batch_destroy(b)
+        buf = torch.empty(max(cnt, 1), dtype=torch.int32, device=dcol.device)
+        b = L.voxel_batch_create()
+        try:
+            _batch_add(L, b, prog, dcol, n, 1, cnt, buf.data_ptr())
+            if L.voxel_batch_launch(b, 0, sh) or L.voxel_batch_fetch(b, sh):
+                raise RuntimeError(capi.last_error())
+            regs, cnt2, ovf = _batch_out(L, b, 0)
+        finally:
+            L.voxel_batch_destroy(b)
+        if ovf or cnt2 != cnt:
+            raise RuntimeError("write pass disagrees with the count pass")
+        out.append(ProgramResult(regs, cnt, buf[:cnt]))
+    return out
+
+
+def train_estimator(columns, runs: int, seed: int = 0, epochs: int = 30, batch: int = 1024, lr: float = 2e-3):
+    """Trains the MLP on `runs` engine-measured (exact) selectivities over the
+    given (dtype, device column) list.  Returns (model, held-out q-errors of the
+    model and of the histogram + independence estimator)."""
+    rng = np.random.default_rng(seed)
+    per_col = max(1, runs // max(len(columns), 1))
+    X, Y, meta = E.build_training_set(columns, per_col, rng)
+    n = len(X)
+    perm = rng.permutation(n)
+    ntr = int(0.9 * n)
+    tr, te = perm[:ntr], perm[ntr:]
+    model = E.Model(seed=seed + 1)
+    model.train(X[tr], Y[tr], epochs=epochs, batch=batch, lr=lr, seed=seed)
+    pred = model.predict(X[te])
+    q_m, q_b = [], []
+    for y, k in zip(pred, te):
+        nrows, rows, _, base, _ = meta[k]
+        q_m.append(E.q_error(E.decode(y, nrows)[0], rows))
+        q_b.append(E.q_error(base[0], rows))
+    return model, np.array(q_m), np.array(q_b), n
+

@@ -196,7 +196,7 @@ __device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPar
     if (threadIdx.x == 0) finalize_scan<T, 1, kBNR>(p, blk, &out->res);
 }
 
-__global__ void __launch_bounds__(kBThreads) batch_kernel(const BatchProg* __restrict__ progs, uint32_t nprog,
+__global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __restrict__ progs, uint32_t nprog,
                                                           const uint64_t* __restrict__ item_start, uint64_t nitems,
                                                           ItemPartial* parts, unsigned long long* status,
                                                           unsigned int* pdone, unsigned int* item_ctr, BatchOut* outs,

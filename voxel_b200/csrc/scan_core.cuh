@@ -83,22 +83,64 @@ __device__ __forceinline__ T opnd_val(const Opnd& o, const T (&v)[NC][32 / sizeo
     return T(0);
 }
 
-// per-lane bitmask of the atoms that hold
+// All lanes of an operand (column lane values, a splatted constant, or zero):
+// the kind is decided once per group, not per lane.
+template <typename T, int NC>
+__device__ __forceinline__ void opnd_lanes(const Opnd& o, const T (&v)[NC][32 / sizeof(T)],
+                                           T (&out)[32 / sizeof(T)]) {
+    constexpr int KL = 32 / sizeof(T);
+    if (o.kind == kOpCol) {
+#pragma unroll
+        for (int l = 0; l < KL; ++l) out[l] = col_val<T, NC>(v, o.col, l);
+    } else {
+        const T c = o.kind == kOpConst ? from_bits<T>(o.bits) : T(0);
+#pragma unroll
+        for (int l = 0; l < KL; ++l) out[l] = c;
+    }
+}
+
+// per-lane bitmask of the atoms that hold (compare op decided once per atom)
 template <typename T, int NC>
 __device__ __forceinline__ void eval_atoms(const ScanParams& p, const T (&v)[NC][32 / sizeof(T)],
                                            uint32_t (&ab)[32 / sizeof(T)]) {
     constexpr int KL = 32 / sizeof(T);
 #pragma unroll
-    for (int l = 0; l < KL; ++l) {
-        uint32_t b = 0;
+    for (int l = 0; l < KL; ++l) ab[l] = 0;
 #pragma unroll
-        for (int a = 0; a < kMaxAtoms; ++a) {
-            if (a < p.natoms) {
-                const Atom& at = p.atom[a];
-                if (t_cmp<T>(col_val<T, NC>(v, at.col, l), from_bits<T>(at.thr), at.op)) b |= 1u << a;
-            }
+    for (int a = 0; a < kMaxAtoms; ++a) {
+        if (a >= p.natoms) break;
+        const Atom& at = p.atom[a];
+        const T t = from_bits<T>(at.thr);
+        const uint32_t bit = 1u << a;
+        T x[KL];
+#pragma unroll
+        for (int l = 0; l < KL; ++l) x[l] = col_val<T, NC>(v, at.col, l);
+        switch (at.op) {
+        case 0:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] == t ? bit : 0u;
+            break;
+        case 1:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] != t ? bit : 0u;
+            break;
+        case 2:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] < t ? bit : 0u;
+            break;
+        case 3:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] <= t ? bit : 0u;
+            break;
+        case 4:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] > t ? bit : 0u;
+            break;
+        default:
+#pragma unroll
+            for (int l = 0; l < KL; ++l) ab[l] |= x[l] >= t ? bit : 0u;
+            break;
         }
-        ab[l] = b;
     }
 }
 
@@ -111,12 +153,13 @@ __device__ __forceinline__ void eval_reds(const ScanParams& p, const T (&v)[NC][
     for (int r = 0; r < NR; ++r) {
         if (r >= p.nred) break;
         const Red& rd = p.red[r];
-        T x[KL];
+        T A[KL], B[KL], x[KL];
+        opnd_lanes<T, NC>(rd.a, v, A);
+        opnd_lanes<T, NC>(rd.b, v, B);
+        const uint32_t pm = rd.pmask;
+        const bool never = (pm & kMaskFalse) != 0;
 #pragma unroll
-        for (int l = 0; l < KL; ++l) {
-            bool pass = !(rd.pmask & kMaskFalse) && ((ab[l] & rd.pmask) == rd.pmask);
-            x[l] = pass ? opnd_val<T, NC>(rd.a, v, l) : opnd_val<T, NC>(rd.b, v, l);
-        }
+        for (int l = 0; l < KL; ++l) x[l] = (!never && (ab[l] & pm) == pm) ? A[l] : B[l];
         uint64_t out;
         switch (rd.kind) {
         case kRedSum: {
