@@ -580,7 +580,107 @@ def workload_batch(args, L, rank, world, local, dist, dev):
     return line
 
 
-WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join, "batch": workload_batch}
+def workload_serve(args, L, rank, world, local, dist, dev):
+    """Serving loop under Poisson arrivals: config-4 style programs over a
+    resident column pool, plus group-by (1K-1M groups, Zipf 1.0) and hash-join
+    (1K-4M build keys, probe 10x) requests; p50/p99 latency per arrival rate."""
+    import torch
+
+    from voxel_b200 import templates as T
+    from voxel_b200.serve import Server
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(5001 + rank)
+    rng = np.random.default_rng(5001 + rank)
+    pool, pool_bytes = [], 0
+    while pool_bytes < args.pool_gb * (1 << 30):
+        dt = int(rng.integers(6))
+        kl = T.K_LANES[dt]
+        n = max(kl, int(2 ** rng.uniform(10, 24)) // kl * kl)
+        c = _device_column(dt, n, g, dev)
+        pool.append((dt, c))
+        pool_bytes += c.numel() * c.element_size()
+    gbs_in = []
+    for _ in range(8):
+        ng = int(2 ** rng.uniform(10, 20))
+        n = 16 * ng
+        r = torch.arange(1, ng + 1, dtype=torch.float64, device=dev).pow_(-1.0)
+        cdf = torch.cumsum(r, 0)
+        cdf /= cdf[-1].clone()
+        keys = torch.searchsorted(cdf, torch.rand(n, dtype=torch.float64, device=dev, generator=g)).clamp_(max=ng - 1)
+        perm = torch.randperm(ng, device=dev, generator=g)
+        gbs_in.append((perm[keys].to(torch.int32), torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 100,
+                       ng))
+    joins = []
+    for _ in range(8):
+        nb = int(2 ** rng.uniform(10, 22))
+        bk = torch.randperm(nb * 4, device=dev, generator=g)[:nb].to(torch.int64)
+        idx = torch.randint(0, nb, (nb * 10,), device=dev, generator=g)
+        pk = bk[idx]
+        miss = torch.rand(nb * 10, device=dev, generator=g) < 0.1
+        pk = torch.where(miss, -pk - 1, pk)
+        out = (torch.empty(nb * 10, dtype=torch.int32, device=dev), torch.empty(nb * 10, dtype=torch.int32, device=dev))
+        joins.append((bk, torch.arange(nb, dtype=torch.int64, device=dev), pk, out))
+    torch.cuda.synchronize()
+    rates = [int(x) for x in args.rates.split(",")]
+    table = []
+    with Server(budget_bytes=args.budget_gb << 30, max_batch=4096) as srv:
+        def one_rate(rate, nreq, seed):
+            r2 = np.random.default_rng(seed)
+            kinds = r2.choice(3, size=nreq, p=[0.90, 0.06, 0.04])
+            gaps = r2.exponential(1.0 / rate, size=nreq)
+            progs = [(T.random_program(pool[j][0], r2), pool[j][1]) for j in r2.integers(0, len(pool), size=nreq)]
+            which = r2.integers(0, 8, size=nreq)
+            srv.reset_stats()
+            ids, served = [], 0
+            t0 = time.perf_counter()
+            t_next = t0
+            for k in range(nreq):
+                t_next += gaps[k]
+                while time.perf_counter() < t_next:
+                    pass
+                if kinds[k] == 0:
+                    prog, col = progs[k]
+                    ids.append(srv.submit_program(prog, col))
+                    served += col.numel() * col.element_size()
+                elif kinds[k] == 1:
+                    keys, vals, ng = gbs_in[which[k]]
+                    ids.append(srv.submit_groupby(keys, vals, ng, capacity=ng))
+                    served += keys.numel() * 12
+                else:
+                    b, pay, pk, (lo, ro) = joins[which[k]]
+                    ids.append(srv.submit_join(b, pay, pk, lo, ro, pk.numel()))
+                    served += b.numel() * 16 + pk.numel() * 8
+            t_sub = time.perf_counter() - t0
+            for rid in ids:
+                srv.result(rid)
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            return {"rate_offered": rate, "rate_submitted": nreq / t_sub, "requests": nreq,
+                    "completed_per_s": nreq / wall, "served_gbs": served / wall / 1e9, "p50_ms": st["p50_ms"],
+                    "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
+
+        one_rate(1000, 200, 1)  # warm-up
+        with ClockSampler(local) as clk:
+            for i, rate in enumerate(rates):
+                table.append(one_rate(rate, args.requests, 100 + i))
+    ref = next((t for t in table if t["rate_offered"] == 10000), table[len(table) // 2])
+    line = _common_line(
+        "serving p99 latency at 10K requests/s", "ms", ref["p99_ms"], world, args, ref["mean_ms"],
+        {"workload": "serving loop: 90% config-4 programs (1-4 predicates + SUM/COUNT/MIN/MAX, six dtypes) over a "
+                     f"{pool_bytes / 1e9:.1f} GB resident column pool ({len(pool)} columns, 1K-16M rows), 6% group-by "
+                     "(1K-1M groups, Zipf 1.0, 16 rows per group), 4% hash join (1K-4M build, probe 10x, 90% match); "
+                     "Poisson arrivals",
+         "budget_gb": args.budget_gb, "sweep": table, "parallelism": f"replicas x{world}"},
+        None, None,
+        {"value": ref["served_gbs"], "unit": "GB/s served", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+         "note": "device-resident pool; results read by the host per request"},
+        clk.summary(), sum(t["requests"] for t in table), "mixed", higher=False)
+    return line
+
+
+WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join, "batch": workload_batch,
+             "serve": workload_serve}
 
 
 def run_workload(args, rank, world, local):
@@ -613,13 +713,18 @@ def main() -> None:
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch"],
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve"],
                     help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
                          "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29; batch: 4096 "
-                         "programs, batched + learned sizing against plain two-pass kernels")
+                         "programs, batched + learned sizing against plain two-pass kernels; serve: serving loop, "
+                         "Poisson arrivals over a resident column pool")
     ap.add_argument("--programs", type=int, default=4096)
     ap.add_argument("--train-runs", type=int, default=200_000)
     ap.add_argument("--train-columns", type=int, default=512)
+    ap.add_argument("--pool-gb", type=float, default=64.0)
+    ap.add_argument("--budget-gb", type=int, default=16)
+    ap.add_argument("--rates", default="1000,3000,10000,30000,100000")
+    ap.add_argument("--requests", type=int, default=3000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -367,6 +367,43 @@ int       voxel_batch_result(const void* batch, size_t prog, uint64_t* regs64, u
                              int* overflow);
 
 /* ================================================================
+ * Additive: serving loop (no reference counterpart).  Requests arrive from
+ * any thread; programs are batched continuously (each batch is one launch of
+ * the batched executor, prepared while the previous one runs), group-by and
+ * join requests run concurrently on a second stream, and every request is
+ * admitted only when its estimated device working memory fits what is left
+ * of `budget_bytes`.  Columns, keys, values and output buffers are caller
+ * device memory that must stay valid until the request completes.
+ * submit_* return a request id (0 on error: voxel_last_error says why, e.g.
+ * VOXEL_ECAPACITY for a request larger than the whole budget).  result()
+ * copies a completed request's outputs and forgets it:
+ *   program:  regs64 = the 64 registers after the run, *count = selected
+ *             rows, *aux = 1 if the selection overflowed its capacity;
+ *   group-by: *count = groups written (sorted by key) to the host arrays;
+ *   join:     *count = pairs written, *aux = u64 SUM of payload over them.
+ * stats(): requests completed since the last reset, latency percentiles
+ * (submission to completion, ms) and the peak reserved working memory.
+ * ================================================================ */
+void*     voxel_server_create(size_t budget_bytes, uint32_t max_batch);
+void      voxel_server_destroy(void* server);
+uint64_t  voxel_server_submit_program(void* server, int dtype, const uint32_t* code, size_t len,
+                                      const uint64_t* regs64, const void* d_col, size_t count,
+                                      int want_selection, size_t sel_capacity, uint32_t* d_sel);
+uint64_t  voxel_server_submit_groupby(void* server, const uint32_t* d_keys, const double* d_values,
+                                      size_t n, size_t expected_groups, size_t out_capacity,
+                                      uint32_t* out_keys, double* out_sum, double* out_min,
+                                      double* out_max, uint64_t* out_count);
+uint64_t  voxel_server_submit_join(void* server, const int64_t* d_build, const uint64_t* d_payload,
+                                   size_t nb, const int64_t* d_probe, size_t np, uint32_t* d_left,
+                                   uint32_t* d_right, size_t capacity);
+int       voxel_server_wait(void* server, uint64_t id, double timeout_s);
+int       voxel_server_result(void* server, uint64_t id, uint64_t* regs64, uint64_t* count,
+                              uint64_t* aux, double* latency_ms);
+int       voxel_server_stats(void* server, uint64_t* completed, double* p50_ms, double* p99_ms,
+                             double* mean_ms, uint64_t* peak_bytes);
+void      voxel_server_reset_stats(void* server);
+
+/* ================================================================
  * Additive: learned cardinality / selectivity estimator.
  * Column sketches are computed on the device (min / max, 64-bucket
  * equi-width histogram, HyperLogLog p = 12); the FP32 MLP

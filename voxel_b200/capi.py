@@ -153,6 +153,15 @@ _SIGS = {
     "voxel_batch_launch": (C.c_int, [vp, C.c_int, vp]),
     "voxel_batch_fetch": (C.c_int, [vp, vp]),
     "voxel_batch_result": (C.c_int, [vp, sz, vp, vp, vp]),
+    "voxel_server_create": (vp, [sz, u32]),
+    "voxel_server_destroy": (None, [vp]),
+    "voxel_server_submit_program": (u64, [vp, C.c_int, vp, sz, vp, vp, sz, C.c_int, sz, vp]),
+    "voxel_server_submit_groupby": (u64, [vp, vp, vp, sz, sz, sz, vp, vp, vp, vp, vp]),
+    "voxel_server_submit_join": (u64, [vp, vp, vp, sz, vp, sz, vp, vp, sz]),
+    "voxel_server_wait": (C.c_int, [vp, u64, dbl]),
+    "voxel_server_result": (C.c_int, [vp, u64, vp, vp, vp, vp]),
+    "voxel_server_stats": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "voxel_server_reset_stats": (None, [vp]),
     "voxel_hashjoin_i64": (sz, [vp, sz, vp, sz, vp, vp, sz, C.c_int]),
     "voxel_hashjoin_i64_dev": (C.c_int, [vp, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
 }
