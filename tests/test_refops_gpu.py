@@ -120,6 +120,16 @@ def test_dictionary_f64(golden):
     out = np.zeros(5)
     L.voxel_dict_decode_batch(d, out.ctypes.data, 0, 5)
     assert (out == data).all()
+    # zeros (both signs), negative values, NaNs and integer-valued doubles
+    z = np.array([0.0, -0.0, 3.0, -2.0, 0.0, np.nan, 3.0, -2.0, np.nan, 1e-310, 1e-310, -np.inf, np.inf, 0.0])
+    z = np.concatenate([z, np.arange(50.0)[np.random.default_rng(35).integers(0, 50, 10_000)]])
+    L.voxel_dict_build(d, z.ctypes.data, z.size)
+    fin = z[~np.isnan(z)]
+    want = np.unique(np.where(fin == 0.0, 0.0, fin)).size + int(np.isnan(z).sum())  # each NaN its own entry
+    assert L.voxel_dict_cardinality(d) == want
+    out = np.zeros(z.size)
+    L.voxel_dict_decode_batch(d, out.ctypes.data, 0, z.size)
+    assert ((out == z) | (np.isnan(out) & np.isnan(z))).all()
     rng = np.random.default_rng(34)
     pool = rng.random(777) * 1e6
     x = pool[rng.integers(0, pool.size, 100_000)]

@@ -316,9 +316,11 @@ __global__ void f64_sort_keys_kernel(const double* __restrict__ x, uint64_t n, i
                                      uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        double v = x[i];
-        if (v == 0.0) v = 0.0;  // -0.0 and +0.0 compare equal in the reference's merge
-        uint64_t k = f64_order_key(v);
+        // -0.0 and +0.0 compare equal in the reference's merge: both become +0.0
+        // (bit test: exact for every input, NaN included)
+        uint64_t b = static_cast<uint64_t>(__double_as_longlong(x[i]));
+        if ((b << 1) == 0) b = 0;
+        uint64_t k = f64_order_key(__longlong_as_double(static_cast<long long>(b)));
         key[i] = descending ? ~k : k;
         idx[i] = static_cast<uint32_t>(i);
     }
@@ -335,10 +337,12 @@ __global__ void gather_f64_kernel(const double* __restrict__ x, const uint32_t* 
 __global__ void dict_heads_kernel(const uint64_t* __restrict__ skey, uint64_t n, uint32_t* __restrict__ flag) {
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        // NaN images never compare equal, like std::unordered_map<double> keys
+        // NaN images never compare equal, like std::unordered_map<double> keys.
+        // Order key: non-negative x -> bits | sign (magnitude in k), negative
+        // x -> ~bits (magnitude in ~k).
         uint64_t k = skey[i];
-        bool nan = (k >> 63) ? ((~k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull)
-                             : ((k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull);
+        bool nan = (k >> 63) ? ((k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull)
+                             : ((~k & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull);
         flag[i] = (i > 0 && (skey[i] != skey[i - 1] || nan)) ? 1u : 0u;
     }
 }
