@@ -2,6 +2,7 @@
 header declares, the instruction encoders match the reference's builders, and
 the host lowering produces the expected schedules (or rejects programs)."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -116,3 +117,21 @@ def test_plan_rejects_unsupported_shape():
     code = [bc.vload(0, 1, 0), bc.enc(0x80, 6, 6, 0), bc.add(1, 1, 4), bc.cmp(1, 2), bc.jnz(-4), bc.halt()]
     st, _ = plan(0, code, [np.zeros(8)], [0, 0, 8, 0, 4])
     assert st == 2  # VOXEL_EUNSUPPORTED
+
+
+def test_reference_c_example_builds_against_this_library(tmp_path):
+    """The reference's own C example (examples/c_test.cpp) compiles and links
+    against include/ + libvoxel_c.so with no source change (its
+    "bindings/voxel_c.h" include resolves to the forwarding header)."""
+    import shutil
+    import subprocess
+
+    src = os.path.join(os.environ.get("VOXEL_REFERENCE_ROOT", "/root/reference"), "examples", "c_test.cpp")
+    if not os.path.exists(src) or shutil.which("g++") is None:
+        pytest.skip("reference sources not present")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = os.path.join(root, "voxel_b200", "lib")
+    out = tmp_path / "c_test"
+    r = subprocess.run(["g++", "-std=c++17", src, "-I", os.path.join(root, "include"), "-L", lib, "-lvoxel_c",
+                        f"-Wl,-rpath,{lib}", "-o", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
