@@ -78,16 +78,16 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* excl, 
     return total;
 }
 
-template <typename T>
+template <typename T, int NR>
 __device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
                                           unsigned long long* status_prog, int* err, ItemShared& sh) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
     uint32_t* s_scan = sh.scan;
     uint32_t (*s_mask)[kBThreads] = sh.mask;
-    Acc acc[kBNR];
+    Acc acc[NR];
 #pragma unroll
-    for (int r = 0; r < kBNR; ++r) {
+    for (int r = 0; r < NR; ++r) {
         acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
         acc[r].k = {0.0, 0.0};
     }
@@ -111,10 +111,10 @@ __device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemP
             if (j >= p.ndata) continue;
             uint32_t ab[KL];
             eval_atoms<T, 1>(p, v[u], ab);
-            uint64_t res[kBNR];
-            eval_reds<T, 1, kBNR>(p, v[u], ab, res);
+            uint64_t res[NR];
+            eval_reds<T, 1, NR>(p, v[u], ab, res);
 #pragma unroll
-            for (int r = 0; r < kBNR; ++r) {
+            for (int r = 0; r < NR; ++r) {
                 if (r >= p.nred) break;
                 acc_fold<T>(acc[r], p.red[r].acc, res[r]);
                 if (j == lastj) out->res.last[r] = res[r];
@@ -131,8 +131,8 @@ __device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemP
     }
     // reductions -> this item's partial
     Acc* blk = sh.blk;
-    block_reduce<T, kBNR, kBThreads>(p, acc, blk);
-    if (threadIdx.x < kBNR && threadIdx.x < p.nred) {
+    block_reduce<T, NR, kBThreads>(p, acc, blk);
+    if (threadIdx.x < NR && threadIdx.x < p.nred) {
         part_item->u[threadIdx.x] = blk[threadIdx.x].u;
         part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
         part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
@@ -170,19 +170,19 @@ __device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemP
     if (ovf) out->overflow = 1;
 }
 
-template <typename T>
+template <typename T, int NR>
 __device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPartial* parts, BatchOut* out,
                                               ItemShared& sh) {
     const ScanParams& p = bp.p;
-    Acc acc[kBNR];
+    Acc acc[NR];
 #pragma unroll
-    for (int r = 0; r < kBNR; ++r) {
+    for (int r = 0; r < NR; ++r) {
         acc[r].u = r < p.nred ? acc_identity(p.red[r].acc) : 0;
         acc[r].k = {0.0, 0.0};
     }
     for (uint32_t i = threadIdx.x; i < bp.nitems; i += blockDim.x) {
 #pragma unroll
-        for (int r = 0; r < kBNR; ++r) {
+        for (int r = 0; r < NR; ++r) {
             if (r >= p.nred) break;
             Acc o;
             o.u = __ldcg(&parts[i].u[r]);
@@ -191,9 +191,9 @@ __device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPar
             acc_merge<T>(acc[r], p.red[r].acc, o);
         }
     }
-    Acc (&blk)[kBNR] = sh.blk;
-    block_reduce<T, kBNR, kBThreads>(p, acc, blk);
-    if (threadIdx.x == 0) finalize_scan<T, 1, kBNR>(p, blk, &out->res);
+    Acc (&blk)[NR] = *reinterpret_cast<Acc (*)[NR]>(sh.blk);
+    block_reduce<T, NR, kBThreads>(p, acc, blk);
+    if (threadIdx.x == 0) finalize_scan<T, 1, NR>(p, blk, &out->res);
 }
 
 __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __restrict__ progs, uint32_t nprog,
@@ -233,14 +233,21 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
         }
         __syncthreads();
         const uint64_t t = it - item_start[pid];
+        // programs with one reduction (every filter/aggregate template) take
+        // the lean instantiation: one accumulator instead of kBNR
+#define VX_ITEM(TT)                                                                                \
+    (one ? process_item<TT, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh)       \
+         : process_item<TT, kBNR>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh))
+        const bool one = s_bp.p.nred <= 1;
         switch (s_bp.p.dtype) {
-        case F64: process_item<double>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-        case F32: process_item<float>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-        case I64: process_item<int64_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-        case I32: process_item<int32_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-        case U64: process_item<uint64_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-        default: process_item<uint32_t>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+        case F64: VX_ITEM(double); break;
+        case F32: VX_ITEM(float); break;
+        case I64: VX_ITEM(int64_t); break;
+        case I32: VX_ITEM(int32_t); break;
+        case U64: VX_ITEM(uint64_t); break;
+        default: VX_ITEM(uint32_t); break;
         }
+#undef VX_ITEM
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;
@@ -248,14 +255,17 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
         if (s_last) {
             __threadfence();
             const ItemPartial* pp = parts + s_bp.item0;
+#define VX_FIN(TT) \
+    (one ? finalize_program<TT, 1>(s_bp, pp, outs + pid, sh) : finalize_program<TT, kBNR>(s_bp, pp, outs + pid, sh))
             switch (s_bp.p.dtype) {
-            case F64: finalize_program<double>(s_bp, pp, outs + pid, sh); break;
-            case F32: finalize_program<float>(s_bp, pp, outs + pid, sh); break;
-            case I64: finalize_program<int64_t>(s_bp, pp, outs + pid, sh); break;
-            case I32: finalize_program<int32_t>(s_bp, pp, outs + pid, sh); break;
-            case U64: finalize_program<uint64_t>(s_bp, pp, outs + pid, sh); break;
-            default: finalize_program<uint32_t>(s_bp, pp, outs + pid, sh); break;
+            case F64: VX_FIN(double); break;
+            case F32: VX_FIN(float); break;
+            case I64: VX_FIN(int64_t); break;
+            case I32: VX_FIN(int32_t); break;
+            case U64: VX_FIN(uint64_t); break;
+            default: VX_FIN(uint32_t); break;
             }
+#undef VX_FIN
             if (threadIdx.x == 0) pdone[pid] = 0;
         }
         __syncthreads();

@@ -118,8 +118,17 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
         for (int i = 0; i < kRItems; ++i) {
             uint64_t pos = wbase + i * 32 + lane;
             bool valid = pos < n;
-            uint32_t d = valid ? digit_of(key[i], shift) : (kRadix + lane);  // invalid lanes never match
-            unsigned peers = __match_any_sync(0xffffffffu, d);
+            uint32_t d = valid ? digit_of(key[i], shift) : 0u;
+            // lanes holding the same digit: one ballot per digit bit (and one
+            // for validity) -- far cheaper here than __match_any_sync
+            unsigned peers = __ballot_sync(0xffffffffu, valid);
+            if (!valid) peers = ~peers;
+#pragma unroll
+            for (int b = 0; b < kRBits; ++b) {
+                const bool bit = (d >> b) & 1u;
+                const unsigned v = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? v : ~v;
+            }
             unsigned int before = valid ? wc[d] : 0;
             __syncwarp();
             if (valid) {
@@ -143,20 +152,23 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
             s_tstart[d] = run;
         }
         __syncthreads();
-        // tile-local digit starts (exclusive scan of tcount over digits)
+        // tile-local digit starts: inclusive scan of tcount over the 256 digits
+        // (warp shuffles within each of the 8 digit warps, then the warp totals)
+        __shared__ unsigned int s_wsum[kRadix / 32];
+        unsigned int incl = 0;
         if (threadIdx.x < kRadix) {
-            // simple Hillis-Steele in place over s_tstart
+            incl = tcount;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_wsum[warp] = incl;
         }
-        for (int o = 1; o < kRadix; o <<= 1) {
-            unsigned int v = 0;
-            if (threadIdx.x < kRadix && threadIdx.x >= static_cast<unsigned>(o)) v = s_tstart[threadIdx.x - o];
-            __syncthreads();
-            if (threadIdx.x < kRadix) s_tstart[threadIdx.x] += v;
-            __syncthreads();
-        }
+        __syncthreads();
         if (threadIdx.x < kRadix) {
+            for (int w = 0; w < warp; ++w) incl += s_wsum[w];
             int d = threadIdx.x;
-            unsigned int incl = s_tstart[d];
             // decoupled look-back for this digit's global offset
             unsigned int* st = status + tile * kRadix + d;
             uint64_t excl = 0;
