@@ -551,7 +551,8 @@ def workload_batch(args, L, rank, world, local, dist, dev):
     # the batch must reproduce the plain kernels exactly
     mism = 0
     for a, b in zip(res, plain):
-        if a.registers != b.registers or a.count != b.count or not torch.equal(a.selection, b.selection):
+        if (not np.array_equal(np.asarray(a.registers, np.uint64), np.asarray(b.registers, np.uint64))
+                or a.count != b.count or not torch.equal(a.selection, b.selection)):
             mism += 1
     exact = np.array([r.count for r in res], np.float64)
     q = np.maximum((lb.est + 1) / (exact + 1), (exact + 1) / (lb.est + 1))
@@ -566,7 +567,7 @@ def workload_batch(args, L, rank, world, local, dist, dev):
          "column_bytes_per_step": nbytes, "programs": args.programs,
          "plain_two_pass_ms": p_wall, "plain_two_pass_gbs": nbytes / (p_wall * 1e-3) / 1e9,
          "speedup_vs_plain": p_wall / step_ms, "batched_device_ms": statistics.mean(ev_ms),
-         "mismatches_vs_plain": mism, "overflowed_programs": over,
+         "mismatches_vs_plain": mism, "overflowed_programs": over, "last_step_breakdown_ms": lb.last_timing,
          "q_error_batch": {"median": float(np.median(q)), "p90": float(np.percentile(q, 90)),
                            "p99": float(np.percentile(q, 99)), "max": float(q.max())},
          "estimator": {"training_runs": int(nruns), "train_s": train_s, "prepare_s": prep_s,

@@ -365,6 +365,8 @@ int       voxel_batch_fetch(void* batch, void* stream);
 /* after fetch: the program's 64 registers, exact selected-row count, overflow flag */
 int       voxel_batch_result(const void* batch, size_t prog, uint64_t* regs64, uint64_t* sel_count,
                              int* overflow);
+/* after fetch: every program at once (regs64: 64 per program; any pointer may be NULL) */
+int       voxel_batch_results_all(const void* batch, uint64_t* regs64, uint64_t* sel_counts, int* overflows);
 
 /* ================================================================
  * Additive: serving loop (no reference counterpart).  Requests arrive from

@@ -24,13 +24,32 @@ from . import capi
 from . import estimator as E
 
 
-@dataclass
 class ProgramResult:
-    registers: list
-    count: int
-    selection: object = None  # device int32 tensor view (row ids), or None
-    estimate: float = 0.0
-    overflowed: bool = False
+    """One program's outputs: its 64 registers after the run, the exact count of
+    selected rows and the selection vector (a device int32 view of row ids,
+    made on first access)."""
+
+    __slots__ = ("registers", "count", "estimate", "overflowed", "_sel", "_pool", "_off")
+
+    def __init__(self, registers, count, selection=None, estimate=0.0, overflowed=False, pool=None, off=0):
+        self.registers = registers
+        self.count = count
+        self.estimate = estimate
+        self.overflowed = overflowed
+        self._sel = selection
+        self._pool = pool
+        self._off = off
+
+    @property
+    def selection(self):
+        if self._sel is None and self._pool is not None:
+            self._sel = self._pool[self._off:self._off + self.count]
+        return self._sel
+
+    @selection.setter
+    def selection(self, v):
+        self._sel = v
+        self._pool = None
 
 
 def _batch_add(L, b, prog, dcol, n, want, cap, sel_ptr):
@@ -108,17 +127,25 @@ class LearnedBatch:
         exactly.  Returns a list of ProgramResult."""
         import torch  # noqa: PLC0415
 
+        import time  # noqa: PLC0415
+
         L = capi.lib()
         sh = self.stream.cuda_stream if self.stream is not None else None
+        t0 = time.perf_counter()
         if L.voxel_batch_launch(self.b, 1, sh) or L.voxel_batch_fetch(self.b, sh):
             raise RuntimeError(capi.last_error())
-        out, redo = [], []
-        for i in range(len(self.programs)):
-            regs, cnt, ovf = _batch_out(L, self.b, i)
-            sel = self.pool[int(self.offs[i]):int(self.offs[i]) + cnt] if not ovf else None
-            out.append(ProgramResult(regs, cnt, sel, float(self.est[i]), ovf))
-            if ovf:
-                redo.append(i)
+        t1 = time.perf_counter()
+        n = len(self.programs)
+        regs = np.zeros((n, 64), np.uint64)
+        cnts = np.zeros(n, np.uint64)
+        ovfs = np.zeros(n, np.int32)
+        if L.voxel_batch_results_all(self.b, regs.ctypes.data, cnts.ctypes.data, ovfs.ctypes.data):
+            raise RuntimeError(capi.last_error())
+        redo = np.flatnonzero(ovfs).tolist()
+        cl, ol, el = cnts.tolist(), self.offs.tolist(), self.est.tolist()
+        out = [ProgramResult(regs[i], cl[i], None, el[i], bool(ovfs[i]), None if ovfs[i] else self.pool, ol[i])
+               for i in range(n)]
+        t2 = time.perf_counter()
         if redo:  # exact write pass for the programs whose estimate was low
             b2 = L.voxel_batch_create()
             bufs = []
@@ -137,6 +164,8 @@ class LearnedBatch:
                     out[i].selection = bufs[k][:cnt]
             finally:
                 L.voxel_batch_destroy(b2)
+        self.last_timing = {"launch_fetch_ms": (t1 - t0) * 1e3, "results_ms": (t2 - t1) * 1e3,
+                            "rerun_ms": (time.perf_counter() - t2) * 1e3, "reruns": len(redo)}
         return out
 
     def close(self):

@@ -79,7 +79,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* excl, 
 }
 
 template <typename T, int NR>
-__device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
+__device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
                                           unsigned long long* status_prog, int* err, ItemShared& sh) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
@@ -171,7 +171,7 @@ __device__ __noinline__ void process_item(const BatchProg& bp, uint64_t t, ItemP
 }
 
 template <typename T, int NR>
-__device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPartial* parts, BatchOut* out,
+__device__ __forceinline__ void finalize_program(const BatchProg& bp, const ItemPartial* parts, BatchOut* out,
                                               ItemShared& sh) {
     const ScanParams& p = bp.p;
     Acc acc[NR];
@@ -196,35 +196,42 @@ __device__ __noinline__ void finalize_program(const BatchProg& bp, const ItemPar
     if (threadIdx.x == 0) finalize_scan<T, 1, NR>(p, blk, &out->res);
 }
 
-__global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __restrict__ progs, uint32_t nprog,
-                                                          const uint64_t* __restrict__ item_start, uint64_t nitems,
+// One persistent kernel per program class (element type x one / several
+// reductions): blocks take the class's items from its own device work queue
+// (an atomic counter), so each kernel is compiled for one element type.
+// pids: the class's programs; cstart[k]: first class-local item of pids[k].
+template <typename T, int NR>
+__global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __restrict__ progs,
+                                                          const uint32_t* __restrict__ pids, uint32_t npc,
+                                                          const uint64_t* __restrict__ cstart, uint64_t citems,
                                                           ItemPartial* parts, unsigned long long* status,
-                                                          unsigned int* pdone, unsigned int* item_ctr, BatchOut* outs,
-                                                          int* err) {
+                                                          unsigned int* pdone, unsigned int* item_ctr,
+                                                          BatchOut* outs, int* err) {
     __shared__ uint64_t s_item;
-    __shared__ uint32_t s_prog;
+    __shared__ uint32_t s_k;
     __shared__ __align__(16) BatchProg s_bp;
     __shared__ bool s_last;
     __shared__ ItemShared sh;
     uint32_t cached = 0xFFFFFFFFu;
     for (;;) {
         if (threadIdx.x == 0) {
-            uint64_t it = atomicAdd(item_ctr, 1u);
-            s_item = it;
-            if (it < nitems) {
-                // program owning item `it`: last start <= it
-                uint32_t lo = 0, hi = nprog;
+            uint64_t ci = atomicAdd(item_ctr, 1u);
+            s_item = ci;
+            if (ci < citems) {
+                // class program owning item ci: last start <= ci
+                uint32_t lo = 0, hi = npc;
                 while (hi - lo > 1) {
                     uint32_t mid = (lo + hi) >> 1;
-                    if (item_start[mid] <= it) lo = mid; else hi = mid;
+                    if (cstart[mid] <= ci) lo = mid; else hi = mid;
                 }
-                s_prog = lo;
+                s_k = lo;
             }
         }
         __syncthreads();
-        const uint64_t it = s_item;
-        if (it >= nitems) break;
-        const uint32_t pid = s_prog;
+        const uint64_t ci = s_item;
+        if (ci >= citems) break;
+        const uint32_t k = s_k;
+        const uint32_t pid = pids[k];
         if (pid != cached) {
             const int4* src = reinterpret_cast<const int4*>(progs + pid);
             int4* dst = reinterpret_cast<int4*>(&s_bp);
@@ -232,44 +239,56 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
             cached = pid;
         }
         __syncthreads();
-        const uint64_t t = it - item_start[pid];
-        // programs with one reduction (every filter/aggregate template) take
-        // the lean instantiation: one accumulator instead of kBNR
-#define VX_ITEM(TT)                                                                                \
-    (one ? process_item<TT, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh)       \
-         : process_item<TT, kBNR>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh))
-        const bool one = s_bp.p.nred <= 1;
-        switch (s_bp.p.dtype) {
-        case F64: VX_ITEM(double); break;
-        case F32: VX_ITEM(float); break;
-        case I64: VX_ITEM(int64_t); break;
-        case I32: VX_ITEM(int32_t); break;
-        case U64: VX_ITEM(uint64_t); break;
-        default: VX_ITEM(uint32_t); break;
-        }
-#undef VX_ITEM
+        const uint64_t t = ci - cstart[k];
+        const uint64_t it = s_bp.item0 + t;  // global item index
+        process_item<T, NR>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;
         __syncthreads();
         if (s_last) {
             __threadfence();
-            const ItemPartial* pp = parts + s_bp.item0;
-#define VX_FIN(TT) \
-    (one ? finalize_program<TT, 1>(s_bp, pp, outs + pid, sh) : finalize_program<TT, kBNR>(s_bp, pp, outs + pid, sh))
-            switch (s_bp.p.dtype) {
-            case F64: VX_FIN(double); break;
-            case F32: VX_FIN(float); break;
-            case I64: VX_FIN(int64_t); break;
-            case I32: VX_FIN(int32_t); break;
-            case U64: VX_FIN(uint64_t); break;
-            default: VX_FIN(uint32_t); break;
-            }
-#undef VX_FIN
+            finalize_program<T, NR>(s_bp, parts + s_bp.item0, outs + pid, sh);
             if (threadIdx.x == 0) pdone[pid] = 0;
         }
         __syncthreads();
     }
+}
+
+constexpr int kClasses = 12;  // element type x (one reduction, several)
+
+template <typename T, int NR>
+int launch_class_t(const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
+                   uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
+                   unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, NR>, kBThreads, 0));
+        if (per_sm < 1) per_sm = 1;
+    }
+    uint64_t grid = static_cast<uint64_t>(sm_count() > 0 ? sm_count() : 148) * per_sm;
+    if (grid > citems) grid = citems;
+    batch_kernel<T, NR><<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(progs, pids, npc, cstart, citems, parts,
+                                                                        status, pdone, ctr, outs, err);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int launch_class(int cls, const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
+                 uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
+                 unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
+#define VX_CLASS(TT, NRR) \
+    launch_class_t<TT, NRR>(progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
+    const bool one = (cls & 1) == 0;
+    switch (cls >> 1) {
+    case F64: return one ? VX_CLASS(double, 1) : VX_CLASS(double, kBNR);
+    case F32: return one ? VX_CLASS(float, 1) : VX_CLASS(float, kBNR);
+    case I64: return one ? VX_CLASS(int64_t, 1) : VX_CLASS(int64_t, kBNR);
+    case I32: return one ? VX_CLASS(int32_t, 1) : VX_CLASS(int32_t, kBNR);
+    case U64: return one ? VX_CLASS(uint64_t, 1) : VX_CLASS(uint64_t, kBNR);
+    default: return one ? VX_CLASS(uint32_t, 1) : VX_CLASS(uint32_t, kBNR);
+    }
+#undef VX_CLASS
 }
 
 __global__ void clear_outs_kernel(BatchOut* outs, uint32_t n) {
@@ -325,20 +344,40 @@ void Batch::set_capacity(size_t i, uint64_t cap, uint32_t* d_sel) {
 
 int Batch::upload(cudaStream_t s) {
     const uint32_t np = static_cast<uint32_t>(host_.size());
-    std::vector<uint64_t> start(np + 1);
     uint64_t items = 0;
     for (uint32_t i = 0; i < np; ++i) {
         uint64_t ni = (host_[i].p.ndata + kItemGroups - 1) / kItemGroups;
         if (ni == 0) ni = 1;  // every program finalises, even with no data groups
         host_[i].item0 = items;
         host_[i].nitems = static_cast<uint32_t>(ni);
-        start[i] = items;
         items += ni;
     }
-    start[np] = items;
     nitems_ = items;
+    // programs by class (element type x one / several reductions), each class
+    // with its own item queue: pids grouped by class, class-local item starts
+    std::vector<uint32_t> pids;
+    std::vector<uint64_t> cstart;
+    pids.reserve(np);
+    cstart.reserve(np + kClasses);
+    for (int c = 0; c < kClasses; ++c) {
+        cls_[c] = ClassQueue{};
+        cls_[c].pid_off = static_cast<uint32_t>(pids.size());
+        cls_[c].cs_off = static_cast<uint32_t>(cstart.size());
+        uint64_t ci = 0;
+        for (uint32_t i = 0; i < np; ++i) {
+            const int ic = host_[i].p.dtype * 2 + (host_[i].p.nred <= 1 ? 0 : 1);
+            if (ic != c) continue;
+            pids.push_back(i);
+            cstart.push_back(ci);
+            ci += host_[i].nitems;
+        }
+        cls_[c].np = static_cast<uint32_t>(pids.size()) - cls_[c].pid_off;
+        cls_[c].items = ci;
+        cstart.push_back(ci);
+    }
     if (d_progs_.n < np * sizeof(BatchProg)) d_progs_ = DevBuf(np * sizeof(BatchProg) + 16);
-    if (d_start_.n < (np + 1) * 8) d_start_ = DevBuf((np + 1) * 8 + 8);
+    if (d_start_.n < cstart.size() * 8) d_start_ = DevBuf(cstart.size() * 8 + 8);
+    if (d_pids_.n < np * 4 + 4) d_pids_ = DevBuf(np * 4 + 4);
     if (d_outs_.n < np * sizeof(BatchOut)) d_outs_ = DevBuf(np * sizeof(BatchOut) + 16);
     if (d_parts_.n < items * sizeof(ItemPartial)) d_parts_ = DevBuf(items * sizeof(ItemPartial) + 16);
     if (d_status_.n < items * 8 + 64) d_status_ = DevBuf(items * 8 + 64);
@@ -350,15 +389,13 @@ int Batch::upload(cudaStream_t s) {
         d_err_ = DevBuf(16);
         if (d_err_.p) VX_CUDA(cudaMemsetAsync(d_err_.p, 0, 16, s));
     }
-    if (!d_progs_.p || !d_start_.p || !d_outs_.p || !d_parts_.p || !d_status_.p || !d_pdone_.p || !d_err_.p)
+    if (!d_progs_.p || !d_start_.p || !d_pids_.p || !d_outs_.p || !d_parts_.p || !d_status_.p || !d_pdone_.p ||
+        !d_err_.p)
         return kErrOutOfMemory;
     if (int st = h2d(d_progs_.p, host_.data(), np * sizeof(BatchProg), s)) return st;
-    if (int st = h2d(d_start_.p, start.data(), (np + 1) * 8, s)) return st;
+    if (int st = h2d(d_start_.p, cstart.data(), cstart.size() * 8, s)) return st;
+    if (int st = h2d(d_pids_.p, pids.data(), np * 4, s)) return st;
     if (int st = sync(s)) return st;
-    int per_sm = 0;
-    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBThreads, 0));
-    if (per_sm < 1) per_sm = 1;
-    grid_ = (sm_count() > 0 ? sm_count() : 148) * per_sm;
     if (graph_exec_) {
         cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
@@ -375,14 +412,17 @@ int Batch::enqueue(cudaStream_t s) {
     const uint32_t np = static_cast<uint32_t>(host_.size());
     VX_CUDA(cudaMemsetAsync(d_status_.p, 0, nitems_ * 8 + 64, s));
     clear_outs_kernel<<<(np + 255) / 256, 256, 0, s>>>(d_outs_.as<BatchOut>(), np);
-    uint64_t grid = static_cast<uint64_t>(grid_);
-    if (grid > nitems_) grid = nitems_;
-    unsigned int* ctr = reinterpret_cast<unsigned int*>(d_status_.as<unsigned long long>() + nitems_);
-    batch_kernel<<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(
-        d_progs_.as<BatchProg>(), np, d_start_.as<uint64_t>(), nitems_, d_parts_.as<ItemPartial>(),
-        d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr, d_outs_.as<BatchOut>(),
-        d_err_.as<int>());
     VX_CUDA(cudaGetLastError());
+    // one item counter per class after the look-back status words
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(d_status_.as<unsigned long long>() + nitems_);
+    for (int c = 0; c < kClasses; ++c) {
+        if (!cls_[c].np) continue;
+        if (int st = launch_class(c, d_progs_.as<BatchProg>(), d_pids_.as<uint32_t>() + cls_[c].pid_off, cls_[c].np,
+                                  d_start_.as<uint64_t>() + cls_[c].cs_off, cls_[c].items, d_parts_.as<ItemPartial>(),
+                                  d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr + c,
+                                  d_outs_.as<BatchOut>(), d_err_.as<int>(), s))
+            return st;
+    }
     return kOk;
 }
 
@@ -470,6 +510,17 @@ int voxel_batch_launch(void* b, int use_graph, void* stream) {
 int voxel_batch_fetch(void* b, void* stream) {
     clear_error();
     return static_cast<Batch*>(b)->fetch(static_cast<cudaStream_t>(stream));
+}
+
+int voxel_batch_results_all(const void* b, uint64_t* regs64, uint64_t* sel_counts, int* overflows) {
+    const Batch* B = static_cast<const Batch*>(b);
+    if (B->fetched() != B->size()) return kErrInvalidArg;
+    for (size_t i = 0; i < B->size(); ++i) {
+        if (regs64) B->registers(i, regs64 + 64 * i);
+        if (sel_counts) sel_counts[i] = B->out(i).sel_count;
+        if (overflows) overflows[i] = B->out(i).overflow;
+    }
+    return kOk;
 }
 
 int voxel_batch_result(const void* b, size_t prog, uint64_t* regs64, uint64_t* sel_count, int* overflow) {

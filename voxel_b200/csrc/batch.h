@@ -54,9 +54,15 @@ private:
     std::vector<std::vector<RegWrite>> writes_;
     std::vector<std::vector<uint64_t>> regs_;
     std::vector<BatchOut> outs_;
-    DevBuf d_progs_, d_start_, d_outs_, d_parts_, d_status_, d_pdone_, d_err_;
+    DevBuf d_progs_, d_start_, d_pids_, d_outs_, d_parts_, d_status_, d_pdone_, d_err_;
     uint64_t nitems_ = 0;
-    int grid_ = 148;
+    // per class (element type x one / several reductions): its programs
+    // (d_pids_ + pid_off), item starts (d_start_ + cs_off) and item count
+    struct ClassQueue {
+        uint32_t pid_off = 0, cs_off = 0, np = 0;
+        uint64_t items = 0;
+    };
+    ClassQueue cls_[12];
     bool dirty_ = true;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
