@@ -73,8 +73,8 @@ def _batch_out(L, b, i):
 @dataclass
 class LearnedBatch:
     model: "E.Model | None"
-    margin: float = 2.0
-    slack: int = 256
+    margin: float = 4.0
+    slack: int = 1024
     programs: list = field(default_factory=list)
     columns: list = field(default_factory=list)  # (dtype, device tensor) per program
     sketches: dict = field(default_factory=dict)
@@ -148,20 +148,24 @@ class LearnedBatch:
         t2 = time.perf_counter()
         if redo:  # exact write pass for the programs whose estimate was low
             b2 = L.voxel_batch_create()
-            bufs = []
             try:
-                for i in redo:
-                    buf = torch.empty(max(out[i].count, 1), dtype=torch.int32, device=self.pool.device)
-                    bufs.append(buf)
-                    _batch_add(L, b2, self.programs[i], self.columns[i], self.columns[i].numel(), 1, out[i].count,
-                               buf.data_ptr())
+                sizes = [out[i].count for i in redo]
+                offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+                pool2 = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=self.pool.device)
+                base = pool2.data_ptr()
+                for k, i in enumerate(redo):
+                    _batch_add(L, b2, self.programs[i], self.columns[i], self.columns[i].numel(), 1, sizes[k],
+                               base + 4 * int(offs[k]))
                 if L.voxel_batch_launch(b2, 0, sh) or L.voxel_batch_fetch(b2, sh):
                     raise RuntimeError(capi.last_error())
+                cnt2 = np.zeros(len(redo), np.uint64)
+                ovf2 = np.zeros(len(redo), np.int32)
+                if L.voxel_batch_results_all(b2, None, cnt2.ctypes.data, ovf2.ctypes.data):
+                    raise RuntimeError(capi.last_error())
+                if ovf2.any() or (cnt2 != np.asarray(sizes, np.uint64)).any():
+                    raise RuntimeError("exact re-run disagrees with the batch")
                 for k, i in enumerate(redo):
-                    regs, cnt, ovf = _batch_out(L, b2, k)
-                    if ovf or cnt != out[i].count:
-                        raise RuntimeError("exact re-run disagrees with the batch")
-                    out[i].selection = bufs[k][:cnt]
+                    out[i].selection = pool2[int(offs[k]):int(offs[k]) + sizes[k]]
             finally:
                 L.voxel_batch_destroy(b2)
         self.last_timing = {"launch_fetch_ms": (t1 - t0) * 1e3, "results_ms": (t2 - t1) * 1e3,

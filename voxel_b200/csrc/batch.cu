@@ -41,7 +41,7 @@ constexpr uint64_t kItemGroups = static_cast<uint64_t>(kBThreads) * kBU * kBW;
 // shared memory of one block's current item (one copy for every element type)
 struct ItemShared {
     uint32_t mask[kBW][kBThreads];  // selected lanes per pass (bit u*KL+l)
-    uint32_t scan[kBThreads / 32 + 1];
+    uint32_t pw[kBW][kBThreads / 32];  // selected rows per (pass, warp), then their exclusive prefix
     Acc blk[kBNR];
     uint64_t item_base;
 };
@@ -52,38 +52,47 @@ struct ItemPartial {
     double c[kBNR];
 };
 
-// block-wide exclusive scan of one value per thread; returns the block total
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* excl, uint32_t* sh) {
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t inc = v;
-    for (int d = 1; d < 32; d <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc += y;
+// Atom comparison of all lanes against one threshold (op decided per group).
+template <typename T>
+__device__ __forceinline__ void atom_lanes(uint8_t op, T t, uint32_t bit, const T (&x)[32 / sizeof(T)],
+                                           uint32_t (&ab)[32 / sizeof(T)]) {
+    constexpr int KL = 32 / sizeof(T);
+    switch (op) {
+    case 0:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] == t ? bit : 0u;
+        break;
+    case 1:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] != t ? bit : 0u;
+        break;
+    case 2:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] < t ? bit : 0u;
+        break;
+    case 3:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] <= t ? bit : 0u;
+        break;
+    case 4:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] > t ? bit : 0u;
+        break;
+    default:
+#pragma unroll
+        for (int l = 0; l < KL; ++l) ab[l] |= x[l] >= t ? bit : 0u;
+        break;
     }
-    if (lane == 31) sh[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t x = lane < kBThreads / 32 ? sh[lane] : 0, t = x;
-        for (int d = 1; d < 32; d <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, t, d);
-            if (lane >= d) t += y;
-        }
-        if (lane < kBThreads / 32) sh[lane] = t - x;
-        if (lane == kBThreads / 32 - 1) sh[kBThreads / 32] = t;
-    }
-    __syncthreads();
-    *excl = sh[warp] + inc - v;
-    uint32_t total = sh[kBThreads / 32];
-    __syncthreads();
-    return total;
 }
 
-template <typename T, int NR>
+// NA = 0: the generic evaluator (scan_core.cuh) for any program shape;
+// NA = 1..4 (one column, one reduction, NA atoms): the same evaluation with the
+// program's fields held in registers for the whole item.
+template <typename T, int NR, int NA>
 __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
                                           unsigned long long* status_prog, int* err, ItemShared& sh) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
-    uint32_t* s_scan = sh.scan;
     uint32_t (*s_mask)[kBThreads] = sh.mask;
     Acc acc[NR];
 #pragma unroll
@@ -94,7 +103,34 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
     const uint64_t g0 = t * kItemGroups;
     const uint64_t lastj = p.ngroups - 1;
     const bool vec = bp.vec != 0;
-    uint32_t total = 0;  // this thread's selected rows over all passes
+    // fast path: the program in registers
+    T f_thr[NA > 0 ? NA : 1];
+    uint8_t f_op[NA > 0 ? NA : 1];
+    uint8_t f_kind = 0, f_acc = 0;
+    uint32_t f_pm = 0, f_sel = 0;
+    bool f_never = false, f_acol = false, f_bcol = false;
+    T f_ac = T(0), f_bc = T(0);
+    uint64_t f_cnt = 0, f_off = 0, f_ndata = 0;
+    if constexpr (NA > 0) {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            f_thr[a] = from_bits<T>(p.atom[a].thr);
+            f_op[a] = p.atom[a].op;
+        }
+        const Red& r0 = p.red[0];
+        f_kind = r0.kind;
+        f_acc = r0.acc;
+        f_pm = r0.pmask;
+        f_never = (r0.pmask & kMaskFalse) != 0;
+        f_acol = r0.a.kind == kOpCol;
+        f_bcol = r0.b.kind == kOpCol;
+        f_ac = r0.a.kind == kOpConst ? from_bits<T>(r0.a.bits) : T(0);
+        f_bc = r0.b.kind == kOpConst ? from_bits<T>(r0.b.bits) : T(0);
+        f_sel = bp.sel_mask;
+        f_cnt = p.count[0];
+        f_off = p.off0;
+        f_ndata = p.ndata;
+    }
     // phase 1: evaluate every pass, fold the reductions, keep the selection masks
 #pragma unroll 1
     for (int w = 0; w < kBW; ++w) {
@@ -104,7 +140,35 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
         T v[kBU][1][KL];
 #pragma unroll
         for (int u = 0; u < kBU; ++u)
-            if (jb + u < p.ndata) load_group<T, 1>(p, jb + u, vec, v[u]);
+            if (jb + u < (NA > 0 ? f_ndata : p.ndata)) load_group<T, 1>(p, jb + u, vec, v[u]);
+        if constexpr (NA > 0) {
+#pragma unroll
+            for (int u = 0; u < kBU; ++u) {
+                const uint64_t j = jb + u;
+                if (j >= f_ndata) continue;
+                uint32_t ab[KL];
+#pragma unroll
+                for (int l = 0; l < KL; ++l) ab[l] = 0;
+#pragma unroll
+                for (int a = 0; a < NA; ++a) atom_lanes<T>(f_op[a], f_thr[a], 1u << a, v[u][0], ab);
+                T x[KL];
+#pragma unroll
+                for (int l = 0; l < KL; ++l) {
+                    const bool pass = !f_never && (ab[l] & f_pm) == f_pm;
+                    x[l] = pass ? (f_acol ? v[u][0][l] : f_ac) : (f_bcol ? v[u][0][l] : f_bc);
+                }
+                const uint64_t res = reduce_group<T>(f_kind, x);
+                acc_fold<T>(acc[0], f_acc, res);
+                if (j == lastj) out->res.last[0] = res;
+                if (f_sel) {
+                    const uint64_t row0 = f_off + j * KL;
+                    const bool full = row0 + KL <= f_cnt;
+#pragma unroll
+                    for (int l = 0; l < KL; ++l)
+                        if ((ab[l] & f_sel) == f_sel && (full || row0 + l < f_cnt)) mask |= 1u << (u * KL + l);
+                }
+            }
+        } else {
 #pragma unroll
         for (int u = 0; u < kBU; ++u) {
             uint64_t j = jb + u;
@@ -126,8 +190,8 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
                     if ((ab[l] & bp.sel_mask) == bp.sel_mask && row0 + l < p.count[0]) mask |= 1u << (u * KL + l);
             }
         }
+        }
         s_mask[w][threadIdx.x] = mask;
-        total += __popc(mask);
     }
     // reductions -> this item's partial
     Acc* blk = sh.blk;
@@ -137,25 +201,61 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
         part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
         part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
     }
-    // the item's selected-row count, then its offset from the look-back
-    uint32_t unused;
-    const uint32_t run = block_excl_scan(total, &unused, s_scan);
-    if (threadIdx.x == 0) {
-        uint64_t e = lookback_exclusive(status_prog, t, run, err);
-        sh.item_base = e;
-        if (t == bp.nitems - 1) out->sel_count = e + run;
+    // Selected rows per (pass, warp), then one warp's exclusive prefix over
+    // them in pass-major order (= ascending row order), the item total, and
+    // the item's offset from the look-back: two block barriers per item.
+    constexpr int kWarps = kBThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        const unsigned c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popc(s_mask[w][threadIdx.x])));
+        if (lane == 0) sh.pw[w][warp] = c;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int kPer = kBW * kWarps / 32;  // entries per lane
+        uint32_t* flat = &sh.pw[0][0];
+        uint32_t loc[kPer], sum = 0;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            loc[e] = flat[lane * kPer + e];
+            sum += loc[e];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint32_t run = incl - sum;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            flat[lane * kPer + e] = run;
+            run += loc[e];
+        }
+        const uint32_t total_item = __shfl_sync(0xffffffffu, incl, 31);
+        const uint64_t e = lookback_exclusive_warp(status_prog, t, total_item, err);
+        if (lane == 0) {
+            sh.item_base = e;
+            if (t == bp.nitems - 1) out->sel_count = e + total_item;
+        }
     }
     __syncthreads();
     if (!(bp.sel_mask && bp.want_sel)) return;
-    // phase 2: row ids in ascending order, pass by pass
-    uint64_t pass_base = sh.item_base;
+    // row ids in ascending order: pass-major, then warp, then lane
+    const uint64_t ibase = sh.item_base;
     bool ovf = false;
 #pragma unroll 1
     for (int w = 0; w < kBW; ++w) {
         uint32_t m = s_mask[w][threadIdx.x];
-        uint32_t excl;
-        const uint32_t tot = block_excl_scan(__popc(m), &excl, s_scan);
-        uint64_t pos = pass_base + excl;
+        const uint32_t c = __popc(m);
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint64_t pos = ibase + sh.pw[w][warp] + (incl - c);
         const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
         while (m) {
             int b = __ffs(m) - 1;
@@ -165,7 +265,6 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
             else ovf = true;
             ++pos;
         }
-        pass_base += tot;
     }
     if (ovf) out->overflow = 1;
 }
@@ -207,17 +306,26 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
                                                           ItemPartial* parts, unsigned long long* status,
                                                           unsigned int* pdone, unsigned int* item_ctr,
                                                           BatchOut* outs, int* err) {
-    __shared__ uint64_t s_item;
+    __shared__ uint64_t s_item, s_kbeg, s_kend;
     __shared__ uint32_t s_k;
     __shared__ __align__(16) BatchProg s_bp;
     __shared__ bool s_last;
     __shared__ ItemShared sh;
     uint32_t cached = 0xFFFFFFFFu;
+    // thread 0 claims the next item only when the block is ready for it (an
+    // item must never wait behind an item a block holds but has not started:
+    // the look-back relies on claimed items making progress); the owning
+    // program is looked up only when an item falls outside the block's
+    // current program
+    if (threadIdx.x == 0) {
+        s_kbeg = 1;
+        s_kend = 0;
+    }
     for (;;) {
         if (threadIdx.x == 0) {
-            uint64_t ci = atomicAdd(item_ctr, 1u);
+            const uint64_t ci = atomicAdd(item_ctr, 1u);
             s_item = ci;
-            if (ci < citems) {
+            if (ci < citems && (ci < s_kbeg || ci >= s_kend)) {
                 // class program owning item ci: last start <= ci
                 uint32_t lo = 0, hi = npc;
                 while (hi - lo > 1) {
@@ -225,6 +333,8 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
                     if (cstart[mid] <= ci) lo = mid; else hi = mid;
                 }
                 s_k = lo;
+                s_kbeg = cstart[lo];
+                s_kend = cstart[lo + 1];
             }
         }
         __syncthreads();
@@ -239,9 +349,19 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
             cached = pid;
         }
         __syncthreads();
-        const uint64_t t = ci - cstart[k];
+        const uint64_t t = ci - s_kbeg;
         const uint64_t it = s_bp.item0 + t;  // global item index
-        process_item<T, NR>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh);
+        if constexpr (NR == 1) {
+            switch (s_bp.p.ncols == 1 ? s_bp.p.natoms : 0) {
+            case 1: process_item<T, 1, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            case 2: process_item<T, 1, 2>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            case 3: process_item<T, 1, 3>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            case 4: process_item<T, 1, 4>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            default: process_item<T, 1, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            }
+        } else {
+            process_item<T, NR, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh);
+        }
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;

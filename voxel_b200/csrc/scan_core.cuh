@@ -144,6 +144,41 @@ __device__ __forceinline__ void eval_atoms(const ScanParams& p, const T (&v)[NC]
     }
 }
 
+// One group's lane values reduced like VSUM / VCOUNT / VRED_MIN / VRED_MAX
+// (engine.hpp:2980-3110); returns the register image.
+template <typename T>
+__device__ __forceinline__ uint64_t reduce_group(uint8_t kind, const T (&x)[32 / sizeof(T)]) {
+    constexpr int KL = 32 / sizeof(T);
+    switch (kind) {
+    case kRedSum: {
+        T s = T(0);
+#pragma unroll
+        for (int l = 0; l < KL; ++l) s = t_add<T>(s, x[l]);
+        return set_scalar<T>(s);
+    }
+    case kRedCount: {
+        uint64_t c = 0;
+#pragma unroll
+        for (int l = 0; l < KL; ++l) c += (!t_isnan<T>(x[l]) && x[l] != T(0)) ? 1 : 0;
+        return c;
+    }
+    case kRedMin: {
+        T m = x[0];
+#pragma unroll
+        for (int l = 1; l < KL; ++l)
+            if (x[l] < m || t_isnan<T>(x[l])) m = x[l];
+        return set_scalar<T>(m);
+    }
+    default: {
+        T m = x[0];
+#pragma unroll
+        for (int l = 1; l < KL; ++l)
+            if (x[l] > m || t_isnan<T>(m)) m = x[l];
+        return set_scalar<T>(m);
+    }
+    }
+}
+
 // Evaluate every reduction of one group; res[r] is the register image.
 template <typename T, int NC, int NR>
 __device__ __forceinline__ void eval_reds(const ScanParams& p, const T (&v)[NC][32 / sizeof(T)],
@@ -160,40 +195,7 @@ __device__ __forceinline__ void eval_reds(const ScanParams& p, const T (&v)[NC][
         const bool never = (pm & kMaskFalse) != 0;
 #pragma unroll
         for (int l = 0; l < KL; ++l) x[l] = (!never && (ab[l] & pm) == pm) ? A[l] : B[l];
-        uint64_t out;
-        switch (rd.kind) {
-        case kRedSum: {
-            T s = T(0);
-#pragma unroll
-            for (int l = 0; l < KL; ++l) s = t_add<T>(s, x[l]);
-            out = set_scalar<T>(s);
-            break;
-        }
-        case kRedCount: {
-            uint64_t c = 0;
-#pragma unroll
-            for (int l = 0; l < KL; ++l) c += (!t_isnan<T>(x[l]) && x[l] != T(0)) ? 1 : 0;
-            out = c;
-            break;
-        }
-        case kRedMin: {
-            T m = x[0];
-#pragma unroll
-            for (int l = 1; l < KL; ++l)
-                if (x[l] < m || t_isnan<T>(x[l])) m = x[l];
-            out = set_scalar<T>(m);
-            break;
-        }
-        default: {
-            T m = x[0];
-#pragma unroll
-            for (int l = 1; l < KL; ++l)
-                if (x[l] > m || t_isnan<T>(m)) m = x[l];
-            out = set_scalar<T>(m);
-            break;
-        }
-        }
-        res[r] = out;
+        res[r] = reduce_group<T>(rd.kind, x);
     }
 }
 

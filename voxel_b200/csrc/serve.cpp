@@ -9,7 +9,8 @@
 //     launch of the batched executor; programs that arrive while a batch runs
 //     form the next batch, prepared on the host while the device works on the
 //     previous one (two batches in flight, alternating streams);
-//   - the operator worker runs group-by and join requests one at a time.
+//   - operator workers (kOpWorkers threads, one stream each) run group-by
+//     and join requests, several at once.
 // Both workers admit work by device-memory footprint: a request reserves its
 // estimated working memory from a shared budget before it starts and returns
 // it when it completes, so a burst never oversubscribes HBM.  The workers run
@@ -100,7 +101,7 @@ class Server {
 public:
     Server(size_t budget, uint32_t max_batch) : budget_(budget), max_batch_(max_batch ? max_batch : 4096) {
         prog_thread_ = std::thread([this] { program_loop(); });
-        op_thread_ = std::thread([this] { operator_loop(); });
+        for (int i = 0; i < kOpWorkers; ++i) op_threads_.emplace_back([this] { operator_loop(); });
     }
 
     ~Server() {
@@ -111,7 +112,7 @@ public:
         cv_work_.notify_all();
         cv_done_.notify_all();
         prog_thread_.join();
-        op_thread_.join();
+        for (auto& t : op_threads_) t.join();
     }
 
     uint64_t submit(std::unique_ptr<Request> r) {
@@ -406,7 +407,9 @@ private:
     uint64_t next_id_ = 0;
     size_t in_use_ = 0, peak_ = 0;
     bool stop_ = false;
-    std::thread prog_thread_, op_thread_;
+    static constexpr int kOpWorkers = 4;
+    std::thread prog_thread_;
+    std::vector<std::thread> op_threads_;
 };
 
 }  // namespace vx
