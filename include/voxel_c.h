@@ -367,6 +367,11 @@ int       voxel_batch_result(const void* batch, size_t prog, uint64_t* regs64, u
                              int* overflow);
 /* after fetch: every program at once (regs64: 64 per program; any pointer may be NULL) */
 int       voxel_batch_results_all(const void* batch, uint64_t* regs64, uint64_t* sel_counts, int* overflows);
+/* how the executor runs program `prog`: 0 = interpreted atoms, 1..8 = range
+ * form (predicate rewritten as lo <= x <= hi with up to two excluded values;
+ * 1 + 2 * reduction kind SUM/COUNT/MIN/MAX + excluded values present);
+ * -1 for an invalid index */
+int       voxel_batch_form(const void* batch, size_t prog);
 
 /* ================================================================
  * Additive: serving loop (no reference counterpart).  Requests arrive from

@@ -28,16 +28,17 @@ def float_acc_regs(code):
     return out
 
 
-def make_batch(progs, cols, caps, want=1):
+def make_batch(progs, cols, caps, want=1, bounds=None):
+    """bounds: the loop's row bound per program (default: the column length)."""
     L = capi.lib()
     b = L.voxel_batch_create()
     dev = torch.device("cuda", 0)
     keep = []
-    for prog, col, cap in zip(progs, cols, caps):
+    for i, (prog, col, cap) in enumerate(zip(progs, cols, caps)):
         dcol = torch.from_numpy(col).to(dev)
         sel = torch.zeros(max(cap, 1), dtype=torch.int32, device=dev)
         keep += [dcol, sel]
-        regs = np.array(prog.registers(col.size), np.uint64)
+        regs = np.array(prog.registers(bounds[i] if bounds else col.size), np.uint64)
         code = np.asarray(prog.code, np.uint32)
         st = L.voxel_batch_add(b, prog.dtype, code.ctypes.data, code.size, regs.ctypes.data, dcol.data_ptr(), col.size,
                                want, cap, sel.data_ptr())
@@ -139,4 +140,77 @@ def test_batch_large_columns_properties():
         e.load_program(prog.code)
         e.run()
         check_regs(prog.dtype, prog.code, regs, e.registers(16))
+    L.voxel_batch_destroy(b)
+
+
+def _specials(dt):
+    if dt in (T.F64, T.F32):
+        fi = np.finfo(T.NP[dt])
+        return [np.nan, np.inf, -np.inf, 0.0, -0.0, float(fi.smallest_subnormal), -float(fi.smallest_subnormal),
+                float(fi.tiny), float(fi.max), float(fi.min), 1.0, -1.0, 2.5, -7.25]
+    ii = np.iinfo(T.NP[dt])
+    return [int(ii.min), int(ii.min) + 1, int(ii.max) - 1, int(ii.max), 0, 1, 2, 7] + ([-1, -7] if ii.min < 0 else [])
+
+
+def test_batch_range_form_edge_cases():
+    """Programs the executor rewrites as lo <= x <= hi (plus excluded values):
+    NaN / +-0 / +-inf / subnormal data and thresholds, thresholds at the type's
+    extremes (x < lowest, x > highest), empty intervals and repeated or NaN
+    exclusions give the same count, selection vector and registers as the
+    single-program engine.  Ragged columns run their loop to the next whole
+    group, so the last group's lanes past the column are zero padding (counted
+    by the reductions, never selected)."""
+    L = capi.lib()
+    rng = np.random.default_rng(44)
+    progs, cols, masks, bounds = [], [], [], []
+    for dt in range(6):
+        sp = _specials(dt)
+        flt = dt in (T.F64, T.F32)
+        for k in range(24):
+            kl = T.K_LANES[dt]
+            n = int(kl * rng.integers(40, 400) + (k % kl))  # ragged tails too
+            extra = ([float(v) for v in rng.uniform(-10, 10, 8)] if flt else
+                     [int(v) for v in rng.integers(-10 if dt in (T.I64, T.I32) else 0, 10, 8)])
+            vals = np.array(sp + extra, dtype=object)
+            col = np.array(list(rng.choice(vals, n)), dtype=T.NP[dt])
+            npred = int(rng.integers(1, 5))
+            preds = [T.Pred(int(rng.integers(0, 6)), rng.choice(vals)) for _ in range(npred)]
+            if k % 6 == 0:  # an empty interval
+                t = rng.choice(vals)
+                preds = [T.Pred(5, t), T.Pred(2, t)]
+            if k % 6 == 1 and npred < 4:  # a repeated exclusion
+                preds += [T.Pred(1, preds[0].value)]
+            prog = T.build(dt, preds, T.AGGS[k % 4])
+            m = np.ones(n, bool)
+            with np.errstate(invalid="ignore", over="ignore"):
+                for p in preds:
+                    v = np.float32(p.value) if dt == T.F32 else T.NP[dt](p.value)
+                    m &= [np.equal, np.not_equal, np.less, np.less_equal, np.greater, np.greater_equal][p.op](col, v)
+            progs.append(prog)
+            cols.append(col)
+            masks.append(m)
+            bounds.append(-(-n // kl) * kl)
+    caps = [int(m.sum()) for m in masks]
+    b, keep = make_batch(progs, cols, caps, bounds=bounds)
+    forms = [L.voxel_batch_form(b, i) for i in range(len(progs))]
+    assert sum(f > 0 for f in forms) >= len(progs) * 3 // 4  # most take the range form
+    assert L.voxel_batch_launch(b, 1, None) == 0 and L.voxel_batch_fetch(b, None) == 0, capi.last_error()
+    for i, (prog, col, m) in enumerate(zip(progs, cols, masks)):
+        regs, cnt, ovf = results(b, i)
+        assert cnt == int(m.sum()) and ovf == 0, (i, forms[i], prog.preds)
+        sel = keep[2 * i + 1][:cnt].cpu().numpy().astype(np.int64)
+        assert (sel == np.flatnonzero(m)).all(), (i, forms[i], prog.preds)
+        e = Engine(prog.dtype)
+        e.add_segment(col)
+        for r, v in enumerate(prog.registers(bounds[i])):
+            e.set_scalar(r, v)
+        e.load_program(prog.code)
+        e.run()
+        want = e.registers(16)
+        facc = float_acc_regs(prog.code) if prog.dtype in (0, 1) else set()
+        for r in range(16):
+            if regs[r] != want[r]:
+                g, w = f64(regs[r]), f64(want[r])
+                assert r in facc and ((np.isnan(g) and np.isnan(w)) or abs(g - w) <= F64_RTOL * max(abs(w), 1e-300)), \
+                    (i, forms[i], prog.preds, prog.agg, r, regs[r], want[r])
     L.voxel_batch_destroy(b)

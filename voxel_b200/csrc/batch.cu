@@ -18,7 +18,10 @@
 // Every wait is bounded.  The launch (with its memsets) is captured into a
 // CUDA graph once per batch and replayed.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "batch.h"
@@ -37,6 +40,7 @@ constexpr int kBU = 2;          // groups per thread per pass
 constexpr int kBW = 8;          // passes per item
 constexpr int kBNR = 4;         // reductions per batched program
 constexpr uint64_t kItemGroups = static_cast<uint64_t>(kBThreads) * kBU * kBW;
+constexpr int kRangeBlocks = 4;  // resident blocks per SM of the range-form kernels
 
 // shared memory of one block's current item (one copy for every element type)
 struct ItemShared {
@@ -85,6 +89,175 @@ __device__ __forceinline__ void atom_lanes(uint8_t op, T t, uint32_t bit, const 
     }
 }
 
+// The evaluators read an item one pass at a time; ask L2 for the whole item
+// up front (one bulk prefetch per pass, 16-byte aligned, inside the column) so
+// HBM streams it while the passes compute.
+template <typename T>
+__device__ __forceinline__ void prefetch_item(const ScanParams& p, uint64_t g0) {
+    constexpr int KL = 32 / sizeof(T);
+    if (threadIdx.x < kBW && p.ncols >= 1) {
+        const uint64_t jb = g0 + static_cast<uint64_t>(threadIdx.x) * kBThreads * kBU;
+        const uint64_t je = min(jb + static_cast<uint64_t>(kBThreads) * kBU, p.ndata);
+        const uint64_t r0 = p.off0 + jb * KL;
+        const uint64_t r1 = min(p.off0 + je * KL, p.count[0]);
+        if (jb < je && r0 < r1) {
+            const uintptr_t base = reinterpret_cast<uintptr_t>(p.col[0]);
+            const uintptr_t a = (base + r0 * sizeof(T) + 15) & ~uintptr_t(15);
+            const uintptr_t b = (base + r1 * sizeof(T)) & ~uintptr_t(15);
+            if (b > a)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<uint32_t>(b - a))
+                             : "memory");
+        }
+    }
+}
+
+// Second half of every item, shared by the evaluators: the item's reduction
+// partial, its selected-row offset (per-pass / per-warp counts, one warp's
+// prefix, the decoupled look-back over the program's earlier items) and the
+// ascending row ids of its selection.  s_mask holds the evaluator's per-pass
+// lane masks (bit u*KL+l of thread x = lane l of its u-th group).
+template <typename T, int NR>
+__device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, Acc (&acc)[NR], ItemPartial* part_item,
+                                              BatchOut* out, unsigned long long* status_prog, int* err,
+                                              ItemShared& sh) {
+    constexpr int KL = 32 / sizeof(T);
+    const ScanParams& p = bp.p;
+    uint32_t (*s_mask)[kBThreads] = sh.mask;
+    const uint64_t g0 = t * kItemGroups;
+    // reductions -> this item's partial
+    Acc* blk = sh.blk;
+    block_reduce<T, NR, kBThreads>(p, acc, blk);
+    if (threadIdx.x < NR && threadIdx.x < p.nred) {
+        part_item->u[threadIdx.x] = blk[threadIdx.x].u;
+        part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
+        part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
+    }
+    // Selected rows per (pass, warp), then one warp's exclusive prefix over
+    // them in pass-major order (= ascending row order), the item total, and
+    // the item's offset from the look-back: two block barriers per item.
+    constexpr int kWarps = kBThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        const unsigned c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popc(s_mask[w][threadIdx.x])));
+        if (lane == 0) sh.pw[w][warp] = c;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int kPer = kBW * kWarps / 32;  // entries per lane
+        uint32_t* flat = &sh.pw[0][0];
+        uint32_t loc[kPer], sum = 0;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            loc[e] = flat[lane * kPer + e];
+            sum += loc[e];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint32_t run = incl - sum;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            flat[lane * kPer + e] = run;
+            run += loc[e];
+        }
+        const uint32_t total_item = __shfl_sync(0xffffffffu, incl, 31);
+        const uint64_t e = lookback_exclusive_warp(status_prog, t, total_item, err);
+        if (lane == 0) {
+            sh.item_base = e;
+            if (t == bp.nitems - 1) out->sel_count = e + total_item;
+        }
+    }
+    __syncthreads();
+    if (!(bp.sel_mask && bp.want_sel)) return;
+    // row ids in ascending order: pass-major, then warp, then lane
+    const uint64_t ibase = sh.item_base;
+    bool ovf = false;
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        uint32_t m = s_mask[w][threadIdx.x];
+        const uint32_t c = __popc(m);
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint64_t pos = ibase + sh.pw[w][warp] + (incl - c);
+        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
+        while (m) {
+            int b = __ffs(m) - 1;
+            m &= m - 1;
+            uint64_t row = p.off0 + (jb + b / KL) * KL + (b % KL);
+            if (pos < bp.sel_cap) bp.sel_out[pos] = static_cast<uint32_t>(row);
+            else ovf = true;
+            ++pos;
+        }
+    }
+    if (ovf) out->overflow = 1;
+}
+
+// Range form (BatchProg::fast != 0): one column, one reduction whose predicate
+// is the conjunction of all atoms, rewritten on the host as lo <= x <= hi and
+// (NE) x != ne[0] and x != ne[1].  RK is the reduction kind.  Same results as
+// the atom-by-atom evaluation: every ordered atom is a closed interval in T's
+// order, and NaN fails every interval test as it fails every ordered atom.
+template <typename T, int RK, bool NE>
+__device__ __forceinline__ void process_range(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
+                                           unsigned long long* status_prog, int* err, ItemShared& sh) {
+    constexpr int KL = 32 / sizeof(T);
+    const ScanParams& p = bp.p;
+    const uint8_t accop = p.red[0].acc;
+    Acc acc[1];
+    acc[0].u = acc_identity(accop);
+    acc[0].k = {0.0, 0.0};
+    const uint64_t g0 = t * kItemGroups;
+    prefetch_item<T>(p, g0);
+    const uint64_t lastj = p.ngroups - 1, ndata = p.ndata, cnt = p.count[0], off0 = p.off0;
+    const bool vec = bp.vec != 0;
+    const T lo = from_bits<T>(bp.lo), hi = from_bits<T>(bp.hi);
+    const T n0 = from_bits<T>(bp.ne[0]), n1 = from_bits<T>(bp.ne[1]);
+    const Red& r0 = p.red[0];
+    const bool acol = r0.a.kind == kOpCol;
+    const T ac = r0.a.kind == kOpConst ? from_bits<T>(r0.a.bits) : T(0);
+    const T bc = r0.b.kind == kOpConst ? from_bits<T>(r0.b.bits) : T(0);
+#pragma unroll 1
+    for (int w = 0; w < kBW; ++w) {
+        uint32_t mask = 0;
+        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
+        T v[kBU][1][KL];
+#pragma unroll
+        for (int u = 0; u < kBU; ++u)
+            if (jb + u < ndata) load_group<T, 1>(p, jb + u, vec, v[u]);
+#pragma unroll
+        for (int u = 0; u < kBU; ++u) {
+            const uint64_t j = jb + u;
+            if (j >= ndata) continue;
+            uint32_t pm = 0;
+            T x[KL];
+#pragma unroll
+            for (int l = 0; l < KL; ++l) {
+                const T y = v[u][0][l];
+                bool pass = y >= lo && y <= hi;
+                if constexpr (NE) pass = pass && y != n0 && y != n1;
+                pm |= pass ? 1u << l : 0u;
+                x[l] = pass ? (acol ? y : ac) : bc;
+            }
+            const uint64_t res = reduce_group<T>(RK, x);
+            acc_fold<T>(acc[0], accop, res);
+            if (j == lastj) out->res.last[0] = res;
+            const uint64_t row0 = off0 + j * KL;
+            if (row0 + KL > cnt) pm &= row0 < cnt ? (1u << (cnt - row0)) - 1u : 0u;
+            mask |= pm << (u * KL);
+        }
+        sh.mask[w][threadIdx.x] = mask;
+    }
+    item_epilogue<T, 1>(bp, t, acc, part_item, out, status_prog, err, sh);
+}
+
 // NA = 0: the generic evaluator (scan_core.cuh) for any program shape;
 // NA = 1..4 (one column, one reduction, NA atoms): the same evaluation with the
 // program's fields held in registers for the whole item.
@@ -101,6 +274,7 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
         acc[r].k = {0.0, 0.0};
     }
     const uint64_t g0 = t * kItemGroups;
+    prefetch_item<T>(p, g0);
     const uint64_t lastj = p.ngroups - 1;
     const bool vec = bp.vec != 0;
     // fast path: the program in registers
@@ -193,80 +367,7 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
         }
         s_mask[w][threadIdx.x] = mask;
     }
-    // reductions -> this item's partial
-    Acc* blk = sh.blk;
-    block_reduce<T, NR, kBThreads>(p, acc, blk);
-    if (threadIdx.x < NR && threadIdx.x < p.nred) {
-        part_item->u[threadIdx.x] = blk[threadIdx.x].u;
-        part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
-        part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
-    }
-    // Selected rows per (pass, warp), then one warp's exclusive prefix over
-    // them in pass-major order (= ascending row order), the item total, and
-    // the item's offset from the look-back: two block barriers per item.
-    constexpr int kWarps = kBThreads / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll 1
-    for (int w = 0; w < kBW; ++w) {
-        const unsigned c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popc(s_mask[w][threadIdx.x])));
-        if (lane == 0) sh.pw[w][warp] = c;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        constexpr int kPer = kBW * kWarps / 32;  // entries per lane
-        uint32_t* flat = &sh.pw[0][0];
-        uint32_t loc[kPer], sum = 0;
-#pragma unroll
-        for (int e = 0; e < kPer; ++e) {
-            loc[e] = flat[lane * kPer + e];
-            sum += loc[e];
-        }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint32_t run = incl - sum;
-#pragma unroll
-        for (int e = 0; e < kPer; ++e) {
-            flat[lane * kPer + e] = run;
-            run += loc[e];
-        }
-        const uint32_t total_item = __shfl_sync(0xffffffffu, incl, 31);
-        const uint64_t e = lookback_exclusive_warp(status_prog, t, total_item, err);
-        if (lane == 0) {
-            sh.item_base = e;
-            if (t == bp.nitems - 1) out->sel_count = e + total_item;
-        }
-    }
-    __syncthreads();
-    if (!(bp.sel_mask && bp.want_sel)) return;
-    // row ids in ascending order: pass-major, then warp, then lane
-    const uint64_t ibase = sh.item_base;
-    bool ovf = false;
-#pragma unroll 1
-    for (int w = 0; w < kBW; ++w) {
-        uint32_t m = s_mask[w][threadIdx.x];
-        const uint32_t c = __popc(m);
-        uint32_t incl = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        uint64_t pos = ibase + sh.pw[w][warp] + (incl - c);
-        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
-        while (m) {
-            int b = __ffs(m) - 1;
-            m &= m - 1;
-            uint64_t row = p.off0 + (jb + b / KL) * KL + (b % KL);
-            if (pos < bp.sel_cap) bp.sel_out[pos] = static_cast<uint32_t>(row);
-            else ovf = true;
-            ++pos;
-        }
-    }
-    if (ovf) out->overflow = 1;
+    item_epilogue<T, NR>(bp, t, acc, part_item, out, status_prog, err, sh);
 }
 
 template <typename T, int NR>
@@ -299,8 +400,8 @@ __device__ __forceinline__ void finalize_program(const BatchProg& bp, const Item
 // reductions): blocks take the class's items from its own device work queue
 // (an atomic counter), so each kernel is compiled for one element type.
 // pids: the class's programs; cstart[k]: first class-local item of pids[k].
-template <typename T, int NR>
-__global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __restrict__ progs,
+template <typename T, int NR, int FAST>
+__global__ void __launch_bounds__(kBThreads, FAST ? kRangeBlocks : 2) batch_kernel(const BatchProg* __restrict__ progs,
                                                           const uint32_t* __restrict__ pids, uint32_t npc,
                                                           const uint64_t* __restrict__ cstart, uint64_t citems,
                                                           ItemPartial* parts, unsigned long long* status,
@@ -351,7 +452,10 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
         __syncthreads();
         const uint64_t t = ci - s_kbeg;
         const uint64_t it = s_bp.item0 + t;  // global item index
-        if constexpr (NR == 1) {
+        if constexpr (FAST) {
+            process_range<T, (FAST - 1) / 2, ((FAST - 1) & 1) != 0>(s_bp, t, parts + it, outs + pid,
+                                                                   status + s_bp.item0, err, sh);
+        } else if constexpr (NR == 1) {
             switch (s_bp.p.ncols == 1 ? s_bp.p.natoms : 0) {
             case 1: process_item<T, 1, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
             case 2: process_item<T, 1, 2>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
@@ -375,40 +479,174 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_kernel(const BatchProg* __
     }
 }
 
-constexpr int kClasses = 12;  // element type x (one reduction, several)
+// Program classes: element type x {8 range forms (reduction kind x excluded
+// values), one interpreted reduction, several}; each class has its own item
+// queue and kernel (one range form per kernel keeps its registers low).
+constexpr int kKinds = 10;
+constexpr int kClasses = 6 * kKinds;
+static_assert(kClasses == Batch::kClasses, "class count");
 
-template <typename T, int NR>
+int class_of(const BatchProg& bp) {
+    return bp.p.dtype * kKinds + (bp.fast ? static_cast<int>(bp.fast) - 1 : bp.p.nred <= 1 ? 8 : 9);
+}
+
+template <typename T, int NR, int FAST>
 int launch_class_t(const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
                    uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
                    unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
     static int per_sm = 0;
     if (!per_sm) {
-        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, NR>, kBThreads, 0));
+        VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, NR, FAST>, kBThreads, 0));
         if (per_sm < 1) per_sm = 1;
     }
     uint64_t grid = static_cast<uint64_t>(sm_count() > 0 ? sm_count() : 148) * per_sm;
     if (grid > citems) grid = citems;
-    batch_kernel<T, NR><<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(progs, pids, npc, cstart, citems, parts,
-                                                                        status, pdone, ctr, outs, err);
+    batch_kernel<T, NR, FAST><<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(progs, pids, npc, cstart, citems,
+                                                                              parts, status, pdone, ctr, outs, err);
     VX_CUDA(cudaGetLastError());
     return kOk;
+}
+
+template <typename T>
+int launch_kind(int kind, const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
+                uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
+                unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
+#define VX_K(NR, F) launch_class_t<T, NR, F>(progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
+    switch (kind) {
+    case 0: return VX_K(1, 1);
+    case 1: return VX_K(1, 2);
+    case 2: return VX_K(1, 3);
+    case 3: return VX_K(1, 4);
+    case 4: return VX_K(1, 5);
+    case 5: return VX_K(1, 6);
+    case 6: return VX_K(1, 7);
+    case 7: return VX_K(1, 8);
+    case 8: return VX_K(1, 0);
+    default: return VX_K(kBNR, 0);
+    }
+#undef VX_K
 }
 
 int launch_class(int cls, const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
                  uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
                  unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
-#define VX_CLASS(TT, NRR) \
-    launch_class_t<TT, NRR>(progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
-    const bool one = (cls & 1) == 0;
-    switch (cls >> 1) {
-    case F64: return one ? VX_CLASS(double, 1) : VX_CLASS(double, kBNR);
-    case F32: return one ? VX_CLASS(float, 1) : VX_CLASS(float, kBNR);
-    case I64: return one ? VX_CLASS(int64_t, 1) : VX_CLASS(int64_t, kBNR);
-    case I32: return one ? VX_CLASS(int32_t, 1) : VX_CLASS(int32_t, kBNR);
-    case U64: return one ? VX_CLASS(uint64_t, 1) : VX_CLASS(uint64_t, kBNR);
-    default: return one ? VX_CLASS(uint32_t, 1) : VX_CLASS(uint32_t, kBNR);
+#define VX_KIND(TT) launch_kind<TT>(cls % kKinds, progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
+    switch (cls / kKinds) {
+    case F64: return VX_KIND(double);
+    case F32: return VX_KIND(float);
+    case I64: return VX_KIND(int64_t);
+    case I32: return VX_KIND(int32_t);
+    case U64: return VX_KIND(uint64_t);
+    default: return VX_KIND(uint32_t);
     }
-#undef VX_CLASS
+#undef VX_KIND
+}
+
+// Host: the range form of a program (BatchProg::fast), when it has one.  The
+// conjunction of ordered atoms (EQ LT LE GT GE) on column 0 is the interval
+// [lo, hi] in T's order (x < t is x <= the next value below t, and so on; an
+// empty set is lo > hi); NE atoms stay as up to two excluded values (an NE
+// against a NaN threshold holds for every x and is dropped).  A program
+// qualifies with one column, one reduction whose predicate is all atoms and
+// whose false value is a constant, and at least one ordered atom.
+template <typename T>
+T host_from_bits(uint64_t b) {
+    T v;
+    if constexpr (sizeof(T) == 8) {
+        std::memcpy(&v, &b, 8);
+    } else {
+        const uint32_t w = static_cast<uint32_t>(b);
+        std::memcpy(&v, &w, 4);
+    }
+    return v;
+}
+
+template <typename T>
+uint64_t host_to_bits(T v) {
+    if constexpr (sizeof(T) == 8) {
+        uint64_t b;
+        std::memcpy(&b, &v, 8);
+        return b;
+    } else {
+        uint32_t w;
+        std::memcpy(&w, &v, 4);
+        return w;
+    }
+}
+
+template <typename T>
+bool range_form(BatchProg& bp) {
+    const ScanParams& p = bp.p;
+    if (p.ncols != 1 || p.nred != 1 || p.natoms < 1 || p.natoms > kMaxAtoms) return false;
+    const uint32_t all = (1u << p.natoms) - 1u;
+    const Red& r = p.red[0];
+    if (r.pmask != all || bp.sel_mask != all || r.kind > kRedMax) return false;
+    if (r.a.kind == kOpCol ? r.a.col != 0 : (r.a.kind != kOpConst && r.a.kind != kOpZero)) return false;
+    if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
+    constexpr bool kFloat = std::is_floating_point<T>::value;
+    const T lowest = kFloat ? -std::numeric_limits<T>::infinity() : std::numeric_limits<T>::lowest();
+    const T highest = kFloat ? std::numeric_limits<T>::infinity() : std::numeric_limits<T>::max();
+    T lo = lowest, hi = highest, ne[2] = {T(0), T(0)};
+    int nne = 0;
+    bool ordered = false, empty = false;
+    for (int a = 0; a < p.natoms; ++a) {
+        const Atom& at = p.atom[a];
+        if (at.col != 0 || at.op > 5) return false;
+        const T t = host_from_bits<T>(at.thr);
+        const bool nan = t != t;
+        if (at.op == 1) {  // NE
+            if (nan) continue;
+            if (nne == 2) return false;
+            ne[nne++] = t;
+            continue;
+        }
+        ordered = true;
+        if (nan) {
+            empty = true;
+            continue;
+        }
+        T l = lowest, h = highest;
+        switch (at.op) {
+        case 0: l = h = t; break;  // EQ
+        case 2:                    // LT
+            if (t == lowest) empty = true;
+            else if constexpr (kFloat) h = std::nextafter(t, lowest);
+            else h = static_cast<T>(t - 1);
+            break;
+        case 3: h = t; break;  // LE
+        case 4:                // GT
+            if (t == highest) empty = true;
+            else if constexpr (kFloat) l = std::nextafter(t, highest);
+            else l = static_cast<T>(t + 1);
+            break;
+        default: l = t; break;  // GE
+        }
+        if (l > lo) lo = l;
+        if (h < hi) hi = h;
+    }
+    if (!ordered) return false;
+    if (empty || lo > hi) {
+        lo = highest;
+        hi = lowest;
+    }
+    if (nne == 1) ne[1] = ne[0];
+    bp.lo = host_to_bits(lo);
+    bp.hi = host_to_bits(hi);
+    bp.ne[0] = host_to_bits(ne[0]);
+    bp.ne[1] = host_to_bits(ne[1]);
+    bp.fast = 1u + 2u * r.kind + (nne ? 1u : 0u);
+    return true;
+}
+
+bool set_range_form(BatchProg& bp) {
+    switch (bp.p.dtype) {
+    case F64: return range_form<double>(bp);
+    case F32: return range_form<float>(bp);
+    case I64: return range_form<int64_t>(bp);
+    case I32: return range_form<int32_t>(bp);
+    case U64: return range_form<uint64_t>(bp);
+    default: return range_form<uint32_t>(bp);
+    }
 }
 
 __global__ void clear_outs_kernel(BatchOut* outs, uint32_t n) {
@@ -424,6 +662,11 @@ Batch::~Batch() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
     if (capture_) cudaStreamDestroy(capture_);
+    for (int b = 0; b < kBranches; ++b) {
+        if (branch_[b]) cudaStreamDestroy(branch_[b]);
+        if (join_[b]) cudaEventDestroy(join_[b]);
+    }
+    if (fork_) cudaEventDestroy(fork_);
 }
 
 int Batch::add(int dtype, const uint32_t* code, size_t len, const uint64_t* regs, const void* d_col, uint64_t count,
@@ -449,6 +692,7 @@ int Batch::add(int dtype, const uint32_t* code, size_t len, const uint64_t* regs
     bp.sel_out = d_sel;
     uintptr_t a = reinterpret_cast<uintptr_t>(d_col) + bp.p.off0 * dtype_size(dtype);
     bp.vec = (a % 16) == 0;
+    set_range_form(bp);
     host_.push_back(bp);
     writes_.push_back(regions[0].writes);
     regs_.emplace_back(regs, regs + 64);
@@ -485,7 +729,7 @@ int Batch::upload(cudaStream_t s) {
         cls_[c].cs_off = static_cast<uint32_t>(cstart.size());
         uint64_t ci = 0;
         for (uint32_t i = 0; i < np; ++i) {
-            const int ic = host_[i].p.dtype * 2 + (host_[i].p.nred <= 1 ? 0 : 1);
+            const int ic = class_of(host_[i]);
             if (ic != c) continue;
             pids.push_back(i);
             cstart.push_back(ci);
@@ -500,7 +744,7 @@ int Batch::upload(cudaStream_t s) {
     if (d_pids_.n < np * 4 + 4) d_pids_ = DevBuf(np * 4 + 4);
     if (d_outs_.n < np * sizeof(BatchOut)) d_outs_ = DevBuf(np * sizeof(BatchOut) + 16);
     if (d_parts_.n < items * sizeof(ItemPartial)) d_parts_ = DevBuf(items * sizeof(ItemPartial) + 16);
-    if (d_status_.n < items * 8 + 64) d_status_ = DevBuf(items * 8 + 64);
+    if (d_status_.n < items * 8 + 8 * kClasses) d_status_ = DevBuf(items * 8 + 8 * kClasses);
     if (d_pdone_.n < np * 4 + 16) {
         d_pdone_ = DevBuf(np * 4 + 16);
         if (d_pdone_.p) VX_CUDA(cudaMemsetAsync(d_pdone_.p, 0, d_pdone_.n, s));
@@ -528,22 +772,45 @@ int Batch::upload(cudaStream_t s) {
     return kOk;
 }
 
-int Batch::enqueue(cudaStream_t s) {
+int Batch::enqueue(cudaStream_t s, bool branches) {
     const uint32_t np = static_cast<uint32_t>(host_.size());
-    VX_CUDA(cudaMemsetAsync(d_status_.p, 0, nitems_ * 8 + 64, s));
+    VX_CUDA(cudaMemsetAsync(d_status_.p, 0, nitems_ * 8 + 8 * kClasses, s));
     clear_outs_kernel<<<(np + 255) / 256, 256, 0, s>>>(d_outs_.as<BatchOut>(), np);
     VX_CUDA(cudaGetLastError());
+    // The class kernels are independent: when recording, spread them over
+    // parallel branches (largest class first, each to the least-loaded
+    // branch), so one kernel's tail overlaps the next one's start.
+    if (branches) {  // streams and events made before the recording began
+        VX_CUDA(cudaEventRecord(fork_, s));
+        for (int b = 0; b < kBranches; ++b) VX_CUDA(cudaStreamWaitEvent(branch_[b], fork_, 0));
+    }
+    std::vector<int> order;
+    for (int c = 0; c < kClasses; ++c)
+        if (cls_[c].np) order.push_back(c);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cls_[x].items > cls_[y].items; });
     // one item counter per class after the look-back status words
     unsigned int* ctr = reinterpret_cast<unsigned int*>(d_status_.as<unsigned long long>() + nitems_);
-    for (int c = 0; c < kClasses; ++c) {
-        if (!cls_[c].np) continue;
-        if (int st = launch_class(c, d_progs_.as<BatchProg>(), d_pids_.as<uint32_t>() + cls_[c].pid_off, cls_[c].np,
-                                  d_start_.as<uint64_t>() + cls_[c].cs_off, cls_[c].items, d_parts_.as<ItemPartial>(),
-                                  d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr + c,
-                                  d_outs_.as<BatchOut>(), d_err_.as<int>(), s))
-            return st;
+    uint64_t load[kBranches] = {};
+    int st = kOk;
+    for (int c : order) {
+        int b = 0;
+        if (branches)
+            for (int k = 1; k < kBranches; ++k)
+                if (load[k] < load[b]) b = k;
+        load[b] += cls_[c].items;
+        st = launch_class(c, d_progs_.as<BatchProg>(), d_pids_.as<uint32_t>() + cls_[c].pid_off, cls_[c].np,
+                          d_start_.as<uint64_t>() + cls_[c].cs_off, cls_[c].items, d_parts_.as<ItemPartial>(),
+                          d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr + c,
+                          d_outs_.as<BatchOut>(), d_err_.as<int>(), branches ? branch_[b] : s);
+        if (st) break;
     }
-    return kOk;
+    if (branches) {  // join every branch, also after a failed launch, so the recording can end
+        for (int b = 0; b < kBranches; ++b) {
+            cudaEventRecord(join_[b], branch_[b]);
+            cudaStreamWaitEvent(s, join_[b], 0);
+        }
+    }
+    return st;
 }
 
 int Batch::launch(cudaStream_t s, bool use_graph) {
@@ -551,13 +818,18 @@ int Batch::launch(cudaStream_t s, bool use_graph) {
     if (dirty_) {
         if (int st = upload(s)) return st;
     }
-    if (!use_graph) return enqueue(s);
+    if (!use_graph) return enqueue(s, false);
     if (!graph_exec_) {
         // Recorded on a private stream: the caller's stream may be the legacy
         // default stream, which cannot be captured.  Recording runs nothing.
         if (!capture_) VX_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
+        for (int b = 0; b < kBranches; ++b) {
+            if (!branch_[b]) VX_CUDA(cudaStreamCreateWithFlags(&branch_[b], cudaStreamNonBlocking));
+            if (!join_[b]) VX_CUDA(cudaEventCreateWithFlags(&join_[b], cudaEventDisableTiming));
+        }
+        if (!fork_) VX_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
         VX_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
-        int st = enqueue(capture_);
+        int st = enqueue(capture_, true);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(capture_, &g);
         if (st) return st;
@@ -641,6 +913,12 @@ int voxel_batch_results_all(const void* b, uint64_t* regs64, uint64_t* sel_count
         if (overflows) overflows[i] = B->out(i).overflow;
     }
     return kOk;
+}
+
+int voxel_batch_form(const void* b, size_t prog) {
+    const Batch* B = static_cast<const Batch*>(b);
+    if (prog >= B->size()) return -1;
+    return static_cast<int>(B->prog(prog).fast);
 }
 
 int voxel_batch_result(const void* b, size_t prog, uint64_t* regs64, uint64_t* sel_count, int* overflow) {

@@ -21,6 +21,12 @@ struct __align__(16) BatchProg {
     uint64_t item0;       // first work item of this program
     uint32_t nitems;
     uint32_t vec;         // 16-byte aligned column: vector loads
+    // range form (0: none): 1 + 2 * reduction kind + (excluded values present);
+    // the predicate is lo <= x <= hi, x != ne[0], x != ne[1] (T bits)
+    uint32_t fast;
+    uint32_t pad0;
+    uint64_t lo, hi;
+    uint64_t ne[2];
 };
 
 struct BatchOut {
@@ -32,6 +38,8 @@ struct BatchOut {
 
 class Batch {
 public:
+    static constexpr int kClasses = 60;  // element type x {8 range forms, one reduction, several}
+    static constexpr int kBranches = 4;  // parallel graph branches the class kernels are spread over
     ~Batch();
     int add(int dtype, const uint32_t* code, size_t len, const uint64_t* regs, const void* d_col, uint64_t count,
             bool want_sel, uint64_t sel_cap, uint32_t* d_sel);
@@ -48,7 +56,7 @@ public:
 
 private:
     int upload(cudaStream_t s);
-    int enqueue(cudaStream_t s);
+    int enqueue(cudaStream_t s, bool branches);
 
     std::vector<BatchProg> host_;
     std::vector<std::vector<RegWrite>> writes_;
@@ -56,17 +64,19 @@ private:
     std::vector<BatchOut> outs_;
     DevBuf d_progs_, d_start_, d_pids_, d_outs_, d_parts_, d_status_, d_pdone_, d_err_;
     uint64_t nitems_ = 0;
-    // per class (element type x one / several reductions): its programs
+    // per class: its programs
     // (d_pids_ + pid_off), item starts (d_start_ + cs_off) and item count
     struct ClassQueue {
         uint32_t pid_off = 0, cs_off = 0, np = 0;
         uint64_t items = 0;
     };
-    ClassQueue cls_[12];
+    ClassQueue cls_[kClasses];
     bool dirty_ = true;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     cudaStream_t capture_ = nullptr;  // private stream the graph is recorded on
+    cudaStream_t branch_[kBranches] = {};
+    cudaEvent_t fork_ = nullptr, join_[kBranches] = {};
 };
 
 }  // namespace vx
