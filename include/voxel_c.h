@@ -372,6 +372,13 @@ int       voxel_batch_results_all(const void* batch, uint64_t* regs64, uint64_t*
  * 1 + 2 * reduction kind SUM/COUNT/MIN/MAX + excluded values present);
  * -1 for an invalid index */
 int       voxel_batch_form(const void* batch, size_t prog);
+/* after fetch: re-run programs progs[0..n) (e.g. those that overflowed) with
+ * selection capacities capacities[k], writing program k's row ids at
+ * d_pool + capacities[0] + ... + capacities[k-1]; one launch from the
+ * programs' already-lowered descriptors; their results then replace the
+ * fetched ones (voxel_batch_result / _results_all) */
+int       voxel_batch_rerun(void* batch, size_t n, const size_t* progs, const size_t* capacities,
+                            uint32_t* d_pool, void* stream);
 
 /* ================================================================
  * Additive: serving loop (no reference counterpart).  Requests arrive from

@@ -214,3 +214,36 @@ def test_batch_range_form_edge_cases():
                 assert r in facc and ((np.isnan(g) and np.isnan(w)) or abs(g - w) <= F64_RTOL * max(abs(w), 1e-300)), \
                     (i, forms[i], prog.preds, prog.agg, r, regs[r], want[r])
     L.voxel_batch_destroy(b)
+
+
+@pytest.mark.parametrize("margin,slack", [(4.0, 1024), (0.0, 0)])
+def test_learned_batch_run_matches_plain_two_pass(margin, slack):
+    """LearnedBatch.run (graph launch, bulk results, exact re-run of programs
+    whose estimated buffer was too small) equals one exact two-pass launch per
+    program: registers, counts and selection vectors.  With no margin every
+    program with a selected row is re-run."""
+    from voxel_b200 import batch as B
+
+    rng = np.random.default_rng(45)
+    dev = torch.device("cuda", 0)
+    progs, cols = [], []
+    for i in range(60):
+        dt = i % 6
+        n = int(T.K_LANES[dt] * rng.integers(1, 20000))
+        progs.append(T.random_program(dt, rng))
+        cols.append(torch.from_numpy(T.make_column(dt, n, rng)).to(dev))
+    stream = torch.cuda.Stream(dev)
+    lb = B.LearnedBatch(None, margin=margin, slack=slack)
+    for p, c in zip(progs, cols):
+        lb.add(p, c)
+    lb.prepare(stream)
+    plain = B.plain_two_pass(progs, cols, stream)
+    for _ in range(2):
+        res = lb.run()
+        assert len(res) == len(progs)
+        if margin == 0.0:
+            assert lb.last_timing["reruns"] == sum(r.count > 0 for r in plain)
+        for a, b in zip(res, plain):
+            assert np.array_equal(np.asarray(a.registers, np.uint64), np.asarray(b.registers, np.uint64))
+            assert a.count == b.count and torch.equal(a.selection, b.selection)
+    lb.close()

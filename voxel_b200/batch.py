@@ -16,6 +16,7 @@ count, then one more to write into an exactly sized buffer.
 """
 from __future__ import annotations
 
+from collections.abc import Sequence
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -50,6 +51,32 @@ class ProgramResult:
     def selection(self, v):
         self._sel = v
         self._pool = None
+
+
+class BatchResults(Sequence):
+    """The results of one batch run, one ProgramResult per program, made on
+    access from the host arrays the run fetched (registers, counts, overflow
+    flags) and the device selection buffers."""
+
+    def __init__(self, regs, counts, est, overflowed, pool, offs, extra):
+        self.registers = regs          # (programs, 64) uint64
+        self.counts = counts           # (programs,) uint64
+        self._est, self._ovf, self._pool, self._offs, self._extra = est, overflowed, pool, offs, extra
+        self._cache = [None] * len(counts)
+
+    def __len__(self):
+        return len(self._cache)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[k] for k in range(*i.indices(len(self)))]
+        r = self._cache[i]
+        if r is None:
+            sel = self._extra.get(i)
+            r = ProgramResult(self.registers[i], int(self.counts[i]), sel, float(self._est[i]), bool(self._ovf[i]),
+                              None if sel is not None else self._pool, int(self._offs[i]))
+            self._cache[i] = r
+        return r
 
 
 def _batch_add(L, b, prog, dcol, n, want, cap, sel_ptr):
@@ -123,8 +150,9 @@ class LearnedBatch:
 
     # -- execution ------------------------------------------------------------
     def run(self):
-        """One graph launch of every program; undersized buffers are re-run
-        exactly.  Returns a list of ProgramResult."""
+        """One graph launch of every program; programs whose selection did not
+        fit are re-run once with exactly sized buffers.  Returns a
+        BatchResults (a sequence of ProgramResult)."""
         import torch  # noqa: PLC0415
 
         import time  # noqa: PLC0415
@@ -141,35 +169,30 @@ class LearnedBatch:
         ovfs = np.zeros(n, np.int32)
         if L.voxel_batch_results_all(self.b, regs.ctypes.data, cnts.ctypes.data, ovfs.ctypes.data):
             raise RuntimeError(capi.last_error())
-        redo = np.flatnonzero(ovfs).tolist()
-        cl, ol, el = cnts.tolist(), self.offs.tolist(), self.est.tolist()
-        out = [ProgramResult(regs[i], cl[i], None, el[i], bool(ovfs[i]), None if ovfs[i] else self.pool, ol[i])
-               for i in range(n)]
+        redo = np.flatnonzero(ovfs)
         t2 = time.perf_counter()
-        if redo:  # exact write pass for the programs whose estimate was low
-            b2 = L.voxel_batch_create()
-            try:
-                sizes = [out[i].count for i in redo]
-                offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-                pool2 = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=self.pool.device)
-                base = pool2.data_ptr()
-                for k, i in enumerate(redo):
-                    _batch_add(L, b2, self.programs[i], self.columns[i], self.columns[i].numel(), 1, sizes[k],
-                               base + 4 * int(offs[k]))
-                if L.voxel_batch_launch(b2, 0, sh) or L.voxel_batch_fetch(b2, sh):
+        extra = {}
+        if redo.size:  # exact write pass for the programs whose estimate was low
+            sizes = cnts[redo]
+            offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+            pool2 = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=self.pool.device)
+            idx = redo.astype(np.uint64)
+            caps = sizes.astype(np.uint64)
+            if L.voxel_batch_rerun(self.b, redo.size, idx.ctypes.data, caps.ctypes.data, pool2.data_ptr(), sh):
+                raise RuntimeError(capi.last_error())
+            cnt2 = np.zeros(redo.size, np.uint64)
+            ovf2 = np.zeros(redo.size, np.int32)
+            regs2 = np.zeros((redo.size, 64), np.uint64)
+            for k, i in enumerate(redo.tolist()):
+                if L.voxel_batch_result(self.b, i, regs2[k].ctypes.data, cnt2[k:].ctypes.data, ovf2[k:].ctypes.data):
                     raise RuntimeError(capi.last_error())
-                cnt2 = np.zeros(len(redo), np.uint64)
-                ovf2 = np.zeros(len(redo), np.int32)
-                if L.voxel_batch_results_all(b2, None, cnt2.ctypes.data, ovf2.ctypes.data):
-                    raise RuntimeError(capi.last_error())
-                if ovf2.any() or (cnt2 != np.asarray(sizes, np.uint64)).any():
-                    raise RuntimeError("exact re-run disagrees with the batch")
-                for k, i in enumerate(redo):
-                    out[i].selection = pool2[int(offs[k]):int(offs[k]) + sizes[k]]
-            finally:
-                L.voxel_batch_destroy(b2)
+            if ovf2.any() or (cnt2 != sizes).any() or (regs2 != regs[redo]).any():
+                raise RuntimeError("exact re-run disagrees with the batch")
+            for k, i in enumerate(redo.tolist()):
+                extra[i] = pool2[int(offs[k]):int(offs[k + 1])]
+        out = BatchResults(regs, cnts, self.est, ovfs, self.pool, self.offs, extra)
         self.last_timing = {"launch_fetch_ms": (t1 - t0) * 1e3, "results_ms": (t2 - t1) * 1e3,
-                            "rerun_ms": (time.perf_counter() - t2) * 1e3, "reruns": len(redo)}
+                            "rerun_ms": (time.perf_counter() - t2) * 1e3, "reruns": int(redo.size)}
         return out
 
     def close(self):

@@ -41,12 +41,19 @@ constexpr int kBW = 8;          // passes per item
 constexpr int kBNR = 4;         // reductions per batched program
 constexpr uint64_t kItemGroups = static_cast<uint64_t>(kBThreads) * kBU * kBW;
 constexpr int kRangeBlocks = 4;  // resident blocks per SM of the range-form kernels
+// The accumulator fold a range-form program uses for each reduction kind
+// (SUM: ADDF on floats, ADD on integers; COUNT: ADD; MIN / MAX: MIN / MAX).
+__host__ __device__ constexpr uint8_t range_acc(int rk, bool is_float) {
+    return rk == kRedSum ? (is_float ? kAccAddF : kAccAdd) : rk == kRedCount ? kAccAdd : rk == kRedMin ? kAccMin : kAccMax;
+}
 
 // shared memory of one block's current item (one copy for every element type)
 struct ItemShared {
     uint32_t mask[kBW][kBThreads];  // selected lanes per pass (bit u*KL+l)
     uint32_t pw[kBW][kBThreads / 32];  // selected rows per (pass, warp), then their exclusive prefix
     Acc blk[kBNR];
+    Acc wacc[kBThreads / 32][kBNR];  // per-warp reduction partials
+    uint32_t stage[kBThreads / 32][32 * 8 * kBU];  // one warp's row ids of one pass (8 lanes per group at most)
     uint64_t item_base;
 };
 
@@ -124,19 +131,26 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
     const ScanParams& p = bp.p;
     uint32_t (*s_mask)[kBThreads] = sh.mask;
     const uint64_t g0 = t * kItemGroups;
-    // reductions -> this item's partial
-    Acc* blk = sh.blk;
-    block_reduce<T, NR, kBThreads>(p, acc, blk);
-    if (threadIdx.x < NR && threadIdx.x < p.nred) {
-        part_item->u[threadIdx.x] = blk[threadIdx.x].u;
-        part_item->s[threadIdx.x] = blk[threadIdx.x].k.s;
-        part_item->c[threadIdx.x] = blk[threadIdx.x].k.c;
-    }
-    // Selected rows per (pass, warp), then one warp's exclusive prefix over
-    // them in pass-major order (= ascending row order), the item total, and
-    // the item's offset from the look-back: two block barriers per item.
+    // Per warp: its reduction partials and its selected rows per pass; after
+    // one barrier warp 0 merges the partials into the item's partial, takes
+    // the exclusive prefix of the (pass, warp) counts in pass-major order
+    // (= ascending row order), and gets the item's offset from the look-back.
     constexpr int kWarps = kBThreads / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        if (r >= p.nred) break;
+        const uint8_t op = p.red[r].acc;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            Acc o;
+            o.u = shfl_down_u64(acc[r].u, d);
+            o.k.s = shfl_down_f64(acc[r].k.s, d);
+            o.k.c = shfl_down_f64(acc[r].k.c, d);
+            acc_merge<T>(acc[r], op, o);
+        }
+        if (lane == 0) sh.wacc[warp][r] = acc[r];
+    }
 #pragma unroll 1
     for (int w = 0; w < kBW; ++w) {
         const unsigned c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popc(s_mask[w][threadIdx.x])));
@@ -144,6 +158,28 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
     }
     __syncthreads();
     if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            if (r >= p.nred) break;
+            const uint8_t op = p.red[r].acc;
+            Acc a;
+            a.u = acc_identity(op);
+            a.k = {0.0, 0.0};
+            if (lane < kWarps) a = sh.wacc[lane][r];
+#pragma unroll
+            for (int d = kWarps / 2; d > 0; d >>= 1) {
+                Acc o;
+                o.u = shfl_down_u64(a.u, d);
+                o.k.s = shfl_down_f64(a.k.s, d);
+                o.k.c = shfl_down_f64(a.k.c, d);
+                acc_merge<T>(a, op, o);
+            }
+            if (lane == 0) {
+                part_item->u[r] = a.u;
+                part_item->s[r] = a.k.s;
+                part_item->c[r] = a.k.c;
+            }
+        }
         constexpr int kPer = kBW * kWarps / 32;  // entries per lane
         uint32_t* flat = &sh.pw[0][0];
         uint32_t loc[kPer], sum = 0;
@@ -173,8 +209,15 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
     }
     __syncthreads();
     if (!(bp.sel_mask && bp.want_sel)) return;
-    // row ids in ascending order: pass-major, then warp, then lane
+    // Row ids in ascending order: pass-major, then warp, then lane.  Each warp
+    // gathers its rows of a pass in shared memory and stores them as one
+    // contiguous run (whole sectors instead of one scattered word per lane).
+    // Row ids are 32-bit, so the item's first row is taken mod 2^32.
     const uint64_t ibase = sh.item_base;
+    const uint32_t row_item = static_cast<uint32_t>(p.off0 + g0 * KL);
+    uint32_t* const sel_out = bp.sel_out;
+    const uint64_t sel_cap = bp.sel_cap;
+    uint32_t* const stage = sh.stage[warp];
     bool ovf = false;
 #pragma unroll 1
     for (int w = 0; w < kBW; ++w) {
@@ -186,16 +229,26 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
             const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        uint64_t pos = ibase + sh.pw[w][warp] + (incl - c);
-        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
+        const uint32_t wtot = __shfl_sync(0xffffffffu, incl, 31);
+        if (wtot == 0) continue;  // uniform over the warp
+        uint32_t k = incl - c;
+        const uint32_t row0 = row_item + (static_cast<uint32_t>(w) * kBThreads * kBU + threadIdx.x * kBU) * KL;
         while (m) {
-            int b = __ffs(m) - 1;
+            const int b = __ffs(m) - 1;  // bit u*KL+l = row (jb+u)*KL+l of the item
             m &= m - 1;
-            uint64_t row = p.off0 + (jb + b / KL) * KL + (b % KL);
-            if (pos < bp.sel_cap) bp.sel_out[pos] = static_cast<uint32_t>(row);
-            else ovf = true;
-            ++pos;
+            stage[k++] = row0 + static_cast<uint32_t>(b);
         }
+        __syncwarp();
+        const uint64_t gpos = ibase + sh.pw[w][warp];
+        if (gpos + wtot <= sel_cap) {
+            for (uint32_t i = lane; i < wtot; i += 32) sel_out[gpos + i] = stage[i];
+        } else {
+            for (uint32_t i = lane; i < wtot; i += 32) {
+                if (gpos + i < sel_cap) sel_out[gpos + i] = stage[i];
+                else ovf = true;
+            }
+        }
+        __syncwarp();
     }
     if (ovf) out->overflow = 1;
 }
@@ -210,51 +263,86 @@ __device__ __forceinline__ void process_range(const BatchProg& bp, uint64_t t, I
                                            unsigned long long* status_prog, int* err, ItemShared& sh) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
-    const uint8_t accop = p.red[0].acc;
+    constexpr uint8_t accop = range_acc(RK, Traits<T>::kFloat);
     Acc acc[1];
     acc[0].u = acc_identity(accop);
     acc[0].k = {0.0, 0.0};
     const uint64_t g0 = t * kItemGroups;
     prefetch_item<T>(p, g0);
-    const uint64_t lastj = p.ngroups - 1, ndata = p.ndata, cnt = p.count[0], off0 = p.off0;
+    // Everything the loop needs, in registers, in item-relative 32-bit units
+    // (the descriptor lives in shared memory; reading it per group costs as
+    // much as the evaluation).
+    const uint64_t ibeg = p.off0 + g0 * KL;  // first row of the item
+    const uint64_t cnt = p.count[0];
+    const uint32_t ngi = static_cast<uint32_t>(min(static_cast<uint64_t>(kItemGroups), p.ndata - min(p.ndata, g0)));
+    const uint32_t rleft = static_cast<uint32_t>(min(cnt - min(cnt, ibeg), kItemGroups * KL));
+    const uint64_t lastj = p.ngroups - 1;
+    const uint32_t llast = (lastj >= g0 && lastj - g0 < kItemGroups) ? static_cast<uint32_t>(lastj - g0) : 0xFFFFFFFFu;
+    const T* __restrict__ ip = static_cast<const T*>(p.col[0]) + ibeg;  // dereferenced below rleft only
     const bool vec = bp.vec != 0;
     const T lo = from_bits<T>(bp.lo), hi = from_bits<T>(bp.hi);
     const T n0 = from_bits<T>(bp.ne[0]), n1 = from_bits<T>(bp.ne[1]);
     const Red& r0 = p.red[0];
-    const bool acol = r0.a.kind == kOpCol;
     const T ac = r0.a.kind == kOpConst ? from_bits<T>(r0.a.bits) : T(0);
     const T bc = r0.b.kind == kOpConst ? from_bits<T>(r0.b.bits) : T(0);
+    // COUNT of the constants: lanes that pass count when ac is nonzero (and
+    // not NaN), the others when bc is
+    const uint32_t cnt_pass = (!t_isnan<T>(ac) && ac != T(0)) ? 1u : 0u;
+    const uint32_t cnt_fail = (!t_isnan<T>(bc) && bc != T(0)) ? 1u : 0u;
+    uint64_t last_res = 0;
+    bool has_last = false;
 #pragma unroll 1
     for (int w = 0; w < kBW; ++w) {
         uint32_t mask = 0;
-        const uint64_t jb = g0 + static_cast<uint64_t>(w) * kBThreads * kBU + static_cast<uint64_t>(threadIdx.x) * kBU;
-        T v[kBU][1][KL];
-#pragma unroll
-        for (int u = 0; u < kBU; ++u)
-            if (jb + u < ndata) load_group<T, 1>(p, jb + u, vec, v[u]);
+        const uint32_t jb = static_cast<uint32_t>(w) * kBThreads * kBU + threadIdx.x * kBU;
+        T v[kBU][KL];
 #pragma unroll
         for (int u = 0; u < kBU; ++u) {
-            const uint64_t j = jb + u;
-            if (j >= ndata) continue;
+            const uint32_t r = (jb + u) * KL;
+            if (jb + u >= ngi) continue;
+            if (vec && r + KL <= rleft) {
+                const uint4* q = reinterpret_cast<const uint4*>(ip + r);
+                const uint4 a = __ldcs(q), b = __ldcs(q + 1);
+                *reinterpret_cast<uint4*>(&v[u][0]) = a;
+                *reinterpret_cast<uint4*>(&v[u][KL / 2]) = b;
+            } else {
+#pragma unroll
+                for (int l = 0; l < KL; ++l) v[u][l] = r + l < rleft ? ip[r + l] : T(0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBU; ++u) {
+            const uint32_t lj = jb + u;
+            if (lj >= ngi) continue;
             uint32_t pm = 0;
             T x[KL];
 #pragma unroll
             for (int l = 0; l < KL; ++l) {
-                const T y = v[u][0][l];
+                const T y = v[u][l];
                 bool pass = y >= lo && y <= hi;
                 if constexpr (NE) pass = pass && y != n0 && y != n1;
                 pm |= pass ? 1u << l : 0u;
-                x[l] = pass ? (acol ? y : ac) : bc;
+                if constexpr (RK != kRedCount) x[l] = pass ? y : bc;
             }
-            const uint64_t res = reduce_group<T>(RK, x);
+            uint64_t res;
+            if constexpr (RK == kRedCount) {
+                const uint32_t np = __popc(pm);
+                res = cnt_pass * np + cnt_fail * (KL - np);
+            } else {
+                res = reduce_group<T>(RK, x);
+            }
             acc_fold<T>(acc[0], accop, res);
-            if (j == lastj) out->res.last[0] = res;
-            const uint64_t row0 = off0 + j * KL;
-            if (row0 + KL > cnt) pm &= row0 < cnt ? (1u << (cnt - row0)) - 1u : 0u;
+            if (lj == llast) {
+                last_res = res;
+                has_last = true;
+            }
+            const uint32_t r = lj * KL;
+            if (r + KL > rleft) pm &= r < rleft ? (1u << (rleft - r)) - 1u : 0u;
             mask |= pm << (u * KL);
         }
         sh.mask[w][threadIdx.x] = mask;
     }
+    if (has_last) out->res.last[0] = last_res;
     item_epilogue<T, 1>(bp, t, acc, part_item, out, status_prog, err, sh);
 }
 
@@ -413,43 +501,44 @@ __global__ void __launch_bounds__(kBThreads, FAST ? kRangeBlocks : 2) batch_kern
     __shared__ bool s_last;
     __shared__ ItemShared sh;
     uint32_t cached = 0xFFFFFFFFu;
-    // thread 0 claims the next item only when the block is ready for it (an
+    // Thread 0 claims an item only when the block is about to start it (an
     // item must never wait behind an item a block holds but has not started:
-    // the look-back relies on claimed items making progress); the owning
-    // program is looked up only when an item falls outside the block's
-    // current program
+    // the look-back relies on claimed items making progress; finalising a
+    // program waits on nothing).  The owning program is looked up only when
+    // an item falls outside the block's current program.
+    auto claim = [&]() {
+        const uint64_t ci = atomicAdd(item_ctr, 1u);
+        s_item = ci;
+        if (ci < citems && (ci < s_kbeg || ci >= s_kend)) {
+            // class program owning item ci: last start <= ci
+            uint32_t lo = 0, hi = npc;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (cstart[mid] <= ci) lo = mid;
+                else hi = mid;
+            }
+            s_k = lo;
+            s_kbeg = cstart[lo];
+            s_kend = cstart[lo + 1];
+        }
+    };
     if (threadIdx.x == 0) {
         s_kbeg = 1;
         s_kend = 0;
+        claim();
     }
+    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) {
-            const uint64_t ci = atomicAdd(item_ctr, 1u);
-            s_item = ci;
-            if (ci < citems && (ci < s_kbeg || ci >= s_kend)) {
-                // class program owning item ci: last start <= ci
-                uint32_t lo = 0, hi = npc;
-                while (hi - lo > 1) {
-                    uint32_t mid = (lo + hi) >> 1;
-                    if (cstart[mid] <= ci) lo = mid; else hi = mid;
-                }
-                s_k = lo;
-                s_kbeg = cstart[lo];
-                s_kend = cstart[lo + 1];
-            }
-        }
-        __syncthreads();
         const uint64_t ci = s_item;
         if (ci >= citems) break;
-        const uint32_t k = s_k;
-        const uint32_t pid = pids[k];
-        if (pid != cached) {
+        const uint32_t pid = pids[s_k];
+        if (pid != cached) {  // uniform: every thread holds the same pid and cache
             const int4* src = reinterpret_cast<const int4*>(progs + pid);
             int4* dst = reinterpret_cast<int4*>(&s_bp);
             for (uint32_t i = threadIdx.x; i < sizeof(BatchProg) / 16; i += blockDim.x) dst[i] = src[i];
             cached = pid;
+            __syncthreads();
         }
-        __syncthreads();
         const uint64_t t = ci - s_kbeg;
         const uint64_t it = s_bp.item0 + t;  // global item index
         if constexpr (FAST) {
@@ -466,16 +555,21 @@ __global__ void __launch_bounds__(kBThreads, FAST ? kRangeBlocks : 2) batch_kern
         } else {
             process_item<T, NR, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh);
         }
+        // the item's partial and row ids are written: count it done, and take
+        // the next item in the same step
         __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;
+        if (threadIdx.x == 0) {
+            s_last = atomicAdd(&pdone[pid], 1u) == s_bp.nitems - 1;
+            claim();
+        }
         __syncthreads();
-        if (s_last) {
+        if (s_last) {  // uniform
             __threadfence();
             finalize_program<T, NR>(s_bp, parts + s_bp.item0, outs + pid, sh);
             if (threadIdx.x == 0) pdone[pid] = 0;
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -581,9 +675,12 @@ bool range_form(BatchProg& bp) {
     const uint32_t all = (1u << p.natoms) - 1u;
     const Red& r = p.red[0];
     if (r.pmask != all || bp.sel_mask != all || r.kind > kRedMax) return false;
-    if (r.a.kind == kOpCol ? r.a.col != 0 : (r.a.kind != kOpConst && r.a.kind != kOpZero)) return false;
-    if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
     constexpr bool kFloat = std::is_floating_point<T>::value;
+    if (r.acc != range_acc(r.kind, kFloat)) return false;
+    // COUNT counts a constant (the VCOUNT of M & one); the others reduce the column
+    if (r.kind == kRedCount ? (r.a.kind != kOpConst && r.a.kind != kOpZero) : (r.a.kind != kOpCol || r.a.col != 0))
+        return false;
+    if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
     const T lowest = kFloat ? -std::numeric_limits<T>::infinity() : std::numeric_limits<T>::lowest();
     const T highest = kFloat ? std::numeric_limits<T>::infinity() : std::numeric_limits<T>::max();
     T lo = lowest, hi = highest, ne[2] = {T(0), T(0)};
@@ -857,6 +954,39 @@ int Batch::fetch(cudaStream_t s) {
     return kOk;
 }
 
+int Batch::rerun(size_t n, const size_t* idx, const size_t* caps, uint32_t* d_pool, cudaStream_t s) {
+    if (outs_.size() != host_.size()) {
+        set_error(kErrInvalidArg, "batch re-run before fetch");
+        return kErrInvalidArg;
+    }
+    if (!n) return kOk;
+    if (!sub_) sub_.reset(new Batch());
+    Batch& b = *sub_;
+    b.host_.clear();
+    b.writes_.clear();
+    b.regs_.clear();
+    uint64_t off = 0;
+    for (size_t k = 0; k < n; ++k) {
+        if (idx[k] >= host_.size()) {
+            set_error(kErrInvalidArg, "batch re-run: program %zu out of range", idx[k]);
+            return kErrInvalidArg;
+        }
+        BatchProg bp = host_[idx[k]];
+        bp.want_sel = 1;
+        bp.sel_cap = caps[k];
+        bp.sel_out = d_pool + off;
+        off += caps[k];
+        b.host_.push_back(bp);
+        b.writes_.push_back(writes_[idx[k]]);
+        b.regs_.push_back(regs_[idx[k]]);
+    }
+    b.dirty_ = true;
+    if (int st = b.launch(s, false)) return st;
+    if (int st = b.fetch(s)) return st;
+    for (size_t k = 0; k < n; ++k) outs_[idx[k]] = b.outs_[k];
+    return kOk;
+}
+
 void Batch::registers(size_t i, uint64_t* regs) const {
     std::memcpy(regs, regs_[i].data(), 64 * 8);
     const BatchOut& o = outs_[i];
@@ -913,6 +1043,12 @@ int voxel_batch_results_all(const void* b, uint64_t* regs64, uint64_t* sel_count
         if (overflows) overflows[i] = B->out(i).overflow;
     }
     return kOk;
+}
+
+int voxel_batch_rerun(void* b, size_t n, const size_t* progs, const size_t* capacities, uint32_t* d_pool,
+                      void* stream) {
+    clear_error();
+    return static_cast<Batch*>(b)->rerun(n, progs, capacities, d_pool, static_cast<cudaStream_t>(stream));
 }
 
 int voxel_batch_form(const void* b, size_t prog) {

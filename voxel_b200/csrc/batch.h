@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "lower.h"
@@ -52,6 +53,11 @@ public:
     const BatchOut& out(size_t i) const { return outs_[i]; }
     const BatchProg& prog(size_t i) const { return host_[i]; }
     void registers(size_t i, uint64_t* regs) const;
+    // After fetch: re-runs programs idx[0..n) with selection capacities caps[k]
+    // into d_pool (program k's rows at d_pool + caps[0] + ... + caps[k-1]),
+    // from their already-lowered descriptors, one launch, and takes their
+    // outputs in place of the fetched ones.
+    int rerun(size_t n, const size_t* idx, const size_t* caps, uint32_t* d_pool, cudaStream_t s);
     uint64_t items() const { return nitems_; }
 
 private:
@@ -75,6 +81,7 @@ private:
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     cudaStream_t capture_ = nullptr;  // private stream the graph is recorded on
+    std::unique_ptr<Batch> sub_;      // re-run batch (its device buffers are reused)
     cudaStream_t branch_[kBranches] = {};
     cudaEvent_t fork_ = nullptr, join_[kBranches] = {};
 };
