@@ -546,6 +546,27 @@ def workload_batch(args, L, rank, world, local, dist, dev):
             ev_ms.append(em)
             wall_ms.append(wm)
     step_ms = _max_over_ranks(dist, dev, statistics.mean(wall_ms))
+    # roofline of the graph launch alone (every class kernel of the batch):
+    # column bytes read + 4 B per selection row written into the sized buffers
+    launch_ev = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if L.voxel_batch_launch(lb.b, 1, stream.cuda_stream):
+            raise RuntimeError("batch launch failed")
+        e1.record(stream)
+        stream.synchronize()
+        launch_ev.append(e0.elapsed_time(e1))
+    if L.voxel_batch_fetch(lb.b, stream.cuda_stream):
+        raise RuntimeError("batch fetch failed")
+    launch_ms = _max_over_ranks(dist, dev, statistics.mean(launch_ev))
+    written = int(sum(min(r.count, c) for r, c in zip(res, lb.caps)))
+    # kernels per step: the output clear + one per non-empty program class,
+    # and the same for the exact re-run of overflowed programs
+    forms = [L.voxel_batch_form(lb.b, i) for i in range(len(progs))]
+    cls_of = [(p_.dtype, f) for p_, f in zip(progs, forms)]
+    redo = [i for i, r in enumerate(res) if r.overflowed]
+    launches_per_step = 1 + len(set(cls_of)) + ((1 + len({cls_of[i] for i in redo})) if redo else 0)
     plain, p_ev, p_wall = timed(lambda: B.plain_two_pass(progs, cols, stream))
     p_wall = _max_over_ranks(dist, dev, p_wall)
     # the batch must reproduce the plain kernels exactly
@@ -573,11 +594,12 @@ def workload_batch(args, L, rank, world, local, dist, dev):
          "estimator": {"training_runs": int(nruns), "train_s": train_s, "prepare_s": prep_s,
                        "heldout_q_median_mlp": float(np.median(q_m)), "heldout_q_p90_mlp": float(np.percentile(q_m, 90)),
                        "heldout_q_median_hist": float(np.median(q_b)), "heldout_q_p90_hist": float(np.percentile(q_b, 90))},
-         "l2": "columns (tens of GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
-        None, None,
+         "l2": "columns (tens of GB) larger than L2; no flush", "parallelism": f"replicas x{world}",
+         "graph_launch_ms": launch_ms, "selection_bytes_in_launch": 4 * written},
+        _roofline("batch_kernel", nbytes + 4 * written, launch_ms), None,
         {"value": None, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": args.programs * 528,
          "note": "device-resident columns; per step the program results (registers, counts) come back to the host"},
-        clk.summary(), args.steps * 1, "mixed")
+        clk.summary(), args.steps * launches_per_step, "mixed")
     return line
 
 

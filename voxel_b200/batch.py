@@ -180,13 +180,12 @@ class LearnedBatch:
             caps = sizes.astype(np.uint64)
             if L.voxel_batch_rerun(self.b, redo.size, idx.ctypes.data, caps.ctypes.data, pool2.data_ptr(), sh):
                 raise RuntimeError(capi.last_error())
-            cnt2 = np.zeros(redo.size, np.uint64)
-            ovf2 = np.zeros(redo.size, np.int32)
-            regs2 = np.zeros((redo.size, 64), np.uint64)
-            for k, i in enumerate(redo.tolist()):
-                if L.voxel_batch_result(self.b, i, regs2[k].ctypes.data, cnt2[k:].ctypes.data, ovf2[k:].ctypes.data):
-                    raise RuntimeError(capi.last_error())
-            if ovf2.any() or (cnt2 != sizes).any() or (regs2 != regs[redo]).any():
+            regs2 = np.zeros((n, 64), np.uint64)
+            cnt2 = np.zeros(n, np.uint64)
+            ovf2 = np.zeros(n, np.int32)
+            if L.voxel_batch_results_all(self.b, regs2.ctypes.data, cnt2.ctypes.data, ovf2.ctypes.data):
+                raise RuntimeError(capi.last_error())
+            if ovf2[redo].any() or (cnt2[redo] != sizes).any() or (regs2[redo] != regs[redo]).any():
                 raise RuntimeError("exact re-run disagrees with the batch")
             for k, i in enumerate(redo.tolist()):
                 extra[i] = pool2[int(offs[k]):int(offs[k + 1])]
