@@ -702,7 +702,157 @@ def workload_serve(args, L, rank, world, local, dist, dev):
     return line
 
 
+def workload_ops(args, L, rank, world, local, dist, dev):
+    """Filter, selection and decoder kernels (VectorFilter, ColumnFilter::AndWith,
+    SelectionVector, BitPacked / Dictionary / RLE decode) on device-resident
+    columns of 2^28 rows, each timed alone with CUDA events on its stream, L2
+    flushed before every timed launch."""
+    import torch
+
+    n = args.rows if args.rows != ROWS else 1 << 28
+    g = torch.Generator(device=dev)
+    g.manual_seed(5001 + rank)
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    words = (n + 63) // 64
+    W, card = 10, 1024
+    nw = (n * W + 63) // 64
+    with torch.cuda.stream(stream):
+        f64 = torch.rand(n, generator=g, device=dev, dtype=torch.float64) * 1000.0
+        i32 = torch.randint(0, 1000, (n,), generator=g, device=dev, dtype=torch.int32)
+        bm_a = torch.empty(words, dtype=torch.int64, device=dev)
+        bm_b = torch.empty(words, dtype=torch.int64, device=dev)
+        bm_o = torch.empty(words, dtype=torch.int64, device=dev)
+        cnt = torch.zeros(4, dtype=torch.int64, device=dev)
+        sel = torch.empty(n, dtype=torch.int32, device=dev)
+        packed = torch.randint(-(1 << 62), 1 << 62, (nw,), generator=g, device=dev, dtype=torch.int64)
+        dict32 = torch.randint(-(1 << 31), (1 << 31) - 1, (card,), generator=g, device=dev, dtype=torch.int32)
+        out32 = torch.empty(n, dtype=torch.int32, device=dev)
+        idx = torch.randint(0, card, (n,), generator=g, device=dev, dtype=torch.int32)
+        dictf = torch.rand(card, generator=g, device=dev, dtype=torch.float64)
+        outf = torch.empty(n, dtype=torch.float64, device=dev)
+        nruns = n // 8
+        runs = torch.randint(1, 16, (nruns,), generator=g, device=dev, dtype=torch.int32)
+        rvals = torch.randint(-(1 << 62), 1 << 62, (nruns,), generator=g, device=dev, dtype=torch.int64)
+        rrows = int(runs.sum().item())
+        outi = torch.empty(rrows, dtype=torch.int64, device=dev)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream.synchronize()
+    f8 = lambda x: int(np.array([x], np.float64).view(np.uint64)[0])  # noqa: E731
+    c = cnt.data_ptr()
+
+    def ok(st):
+        if st:
+            raise RuntimeError(capi.last_error())
+
+    bm_ptrs = (C.c_void_p * 2)(bm_a.data_ptr(), bm_b.data_ptr())
+
+    ops = {
+        "vfilter_f64_gt": (lambda: ok(L.voxel_vfilter_dev(0, 4, f64.data_ptr(), n, f8(900.0), 0, bm_a.data_ptr(), c, sh)),
+                           n * 8 + words * 8),
+        "vfilter_i32_between": (lambda: ok(L.voxel_vfilter_dev(3, 6, i32.data_ptr(), n, 100, 499, bm_b.data_ptr(),
+                                                              c + 8, sh)), n * 4 + words * 8),
+        "bitmap_and_2": (lambda: ok(L.voxel_bitmap_and_dev(C.addressof(bm_ptrs), 2, n, bm_o.data_ptr(), c + 16, sh)),
+                         3 * words * 8),
+        "selection_from_bitmap": (lambda: ok(L.voxel_selection_from_bitmap_dev(bm_a.data_ptr(), n, sel.data_ptr(),
+                                                                             c + 24, sh)), None),
+        "bitpack_decode_w10": (lambda: ok(L.voxel_bitpack_decode_dev(packed.data_ptr(), nw, W, n, 0, n, out32.data_ptr(),
+                                                                     sh)), nw * 8 + n * 4),
+        "dict_bitpack_decode_i32": (lambda: ok(L.voxel_dict_bitpack_decode_i32_dev(
+            packed.data_ptr(), nw, W, dict32.data_ptr(), card, n, 0, n, out32.data_ptr(), sh)), nw * 8 + n * 4 + card * 4),
+        "dict_decode_f64": (lambda: ok(L.voxel_dict_decode_dev(0, dictf.data_ptr(), card, idx.data_ptr(), n,
+                                                               outf.data_ptr(), sh)), n * 4 + n * 8 + card * 8),
+        "rle_decode_i64": (lambda: ok(L.voxel_rle_decode_i64_dev(rvals.data_ptr(), runs.data_ptr(), nruns, 0, rrows,
+                                                                 outi.data_ptr(), sh)), nruns * 12 + rrows * 8),
+    }
+    launches = {"rle_decode_i64": 2}
+    res = {}
+    total_bytes, total_ms, nl = 0, 0.0, 0
+    peak, kind = measured_peak()
+    with ClockSampler(local) as clk:
+        for name, (fn, nbytes) in ops.items():
+            for _ in range(args.warmup):
+                fn()
+            stream.synchronize()
+            ms = []
+            for _ in range(args.steps):
+                flush.zero_()  # on the current stream: evict the previous launch's lines from L2
+                torch.cuda.current_stream().synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            if nbytes is None:  # selection: bitmap read + 4 B per selected row
+                nbytes = words * 8 + 4 * int(cnt[3].item())
+            m = _max_over_ranks(dist, dev, statistics.mean(ms))
+            gbs = nbytes / (m * 1e-3) / 1e9
+            res[name] = {"ms": m, "GB/s": gbs, "frac": gbs / peak, "bytes": nbytes,
+                         "M_rows/s": (rrows if name == "rle_decode_i64" else n) / (m * 1e-3) / 1e6}
+            total_bytes += nbytes
+            total_ms += m
+            nl += args.steps * launches.get(name, 1)
+    # spot checks against torch on the device
+    checks = {
+        "vfilter_count": int(cnt[0].item()) == int((f64 > 900.0).sum().item()),
+        "between_count": int(cnt[1].item()) == int(((i32 >= 100) & (i32 <= 499)).sum().item()),
+        "and_count": int(cnt[2].item()) == int(((f64 > 900.0) & (i32 >= 100) & (i32 <= 499)).sum().item()),
+        "selection": bool(torch.equal(sel[:int(cnt[3].item())].long(),
+                                      torch.nonzero(f64 > 900.0).flatten())),
+        "dict_decode": bool(torch.equal(outf, dictf[idx.long()])),
+        "rle_decode": bool(torch.equal(outi, torch.repeat_interleave(rvals, runs.long()))),
+    }
+    # e2e: the host entry point of the f64 filter (pinned host column in, bitmap out)
+    hcol = f64.cpu().pin_memory()
+    hbm = np.empty(words, np.uint64)
+    L.voxel_vfilter(0, 4, hcol.data_ptr(), n, f8(900.0), 0, hbm.ctypes.data)
+    w0 = time.perf_counter()
+    e_steps = 3
+    for _ in range(e_steps):
+        r = L.voxel_vfilter(0, 4, hcol.data_ptr(), n, f8(900.0), 0, hbm.ctypes.data)
+        if r == (1 << 64) - 1:
+            raise RuntimeError(capi.last_error())
+    e_ms = (time.perf_counter() - w0) * 1e3 / e_steps
+    e2e = {"value": n * 8 / (e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": n * 8,
+           "d2h_bytes_per_step": words * 8, "ms_per_step": e_ms, "op": "voxel_vfilter f64 GT, host buffers"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.have_ref():
+            R = oracle.ref()
+            R.vref_vfilter_f64.restype = C.c_size_t
+            R.vref_vfilter_f64.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_double, C.c_double, C.c_void_p]
+            m_ = min(n, 1 << 27)
+            hx = hcol.numpy()[:m_]
+            hb = np.empty((m_ + 63) // 64, np.uint64)
+            ts = []
+            t_end = time.perf_counter() + 15.0
+            while time.perf_counter() < t_end and len(ts) < 20:
+                t0 = time.perf_counter()
+                R.vref_vfilter_f64(4, hx.ctypes.data, m_, 900.0, 0.0, hb.ctypes.data)
+                ts.append(time.perf_counter() - t0)
+            med = statistics.median(ts)
+            cpu = {"value": m_ * 8 / med / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"VectorFilter<f64>::ApplyGT on the first {m_} rows x {len(ts)} runs (median), "
+                             "single-threaded as in the reference"}
+    top = max(res, key=lambda k: res[k]["ms"])
+    value = world * total_bytes / (total_ms * 1e-3) / 1e9
+    roof = _roofline("ops_kernels", total_bytes, total_ms)
+    roof["note"] = "aggregate of the eight kernels (sum of algorithmic bytes / sum of launch times); per kernel in config.ops"
+    return _common_line(
+        "filter/decode kernels GB/s (sum of bytes / sum of times)", UNIT, value, world, args, total_ms,
+        {"workload": f"{n} rows per column: f64 U[0,1000) > 900, i32 U[0,1000) BETWEEN 100 AND 499, AND of the two "
+                     f"bitmaps, selection vector of the f64 bitmap, 10-bit unpack, dictionary ({card}) decode of the "
+                     f"packed indices and of u32 indices into f64, RLE i64 ({nruns} runs of 1-15 rows)",
+         "ops": res, "checks": checks, "slowest": top, "l2": "256 MB written before every timed launch",
+         "parallelism": f"replicas x{world}"},
+        roof, cpu, e2e, clk.summary(), nl, "mixed")
+
+
 WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join, "batch": workload_batch,
+             "ops": workload_ops,
              "serve": workload_serve}
 
 
@@ -736,7 +886,7 @@ def main() -> None:
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve"],
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve", "ops"],
                     help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
                          "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29; batch: 4096 "
                          "programs, batched + learned sizing against plain two-pass kernels; serve: serving loop, "

@@ -208,6 +208,10 @@ int       voxel_vfilter_dev(int dtype, int op, const void* d_data, size_t n, uin
                             uint64_t hi_bits, uint64_t* d_bitmap, uint64_t* d_count, void* stream);
 int       voxel_selection_from_bitmap_dev(const uint64_t* d_bitmap, size_t rows, uint32_t* d_out,
                                           uint64_t* d_count, void* stream);
+/* ColumnFilter::AndWith over device bitmaps: d_bitmaps is a host array of nbm
+ * device pointers; *d_count receives the popcount of the result */
+int       voxel_bitmap_and_dev(const uint64_t* const* d_bitmaps, size_t nbm, size_t rows, uint64_t* d_out,
+                               uint64_t* d_count, void* stream);
 
 /* ================================================================
  * Additive: decoders (reference include/voxel/data/encoding.hpp)
@@ -230,6 +234,13 @@ int       voxel_bitpack_decode_dev(const uint64_t* d_words, size_t nwords, uint3
                                    void* stream);
 int       voxel_rle_decode_i64_dev(const int64_t* d_values, const uint32_t* d_runs, size_t nruns,
                                    size_t offset, size_t count, int64_t* d_out, void* stream);
+/* device variants of the dictionary decoders; they return after the kernel
+ * (an index outside the dictionary is reported as VOXEL_EINVAL) */
+int       voxel_dict_bitpack_decode_i32_dev(const uint64_t* d_words, size_t nwords, uint32_t width,
+                                            const int32_t* d_dict, size_t card, size_t value_count,
+                                            size_t offset, size_t count, int32_t* d_out, void* stream);
+int       voxel_dict_decode_dev(int dtype, const void* d_dict, size_t card, const uint32_t* d_indices,
+                                size_t count, void* d_out, void* stream);
 
 /* ================================================================
  * Additive: fused scan + group-by (decode key, two predicates, group SUM of a

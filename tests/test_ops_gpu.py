@@ -185,3 +185,42 @@ def test_hashjoin_golden_and_properties(golden):
     wm = oracle.port().vo_hashjoin_i64(b.ctypes.data, b.size, p.ctypes.data, p.size, wl.ctypes.data, wr.ctypes.data,
                                        100, 1)
     assert m == wm == 100 and (l == wl).all() and (r == wr).all()
+
+
+def test_device_entry_points_equal_host_ones():
+    """The device-pointer variants (bitmap AND, dictionary decoders) give the
+    host entry points' results; an index outside the dictionary is an error."""
+    import ctypes
+
+    import torch
+
+    L = capi.lib()
+    dev = torch.device("cuda", 0)
+    n = 1_000_003
+    a, b = inputs.bitmap(n, 31), inputs.bitmap(n, 32)
+    words = (n + 63) // 64
+    host_ptrs = (ctypes.c_void_p * 2)(a.ctypes.data, b.ctypes.data)
+    want = np.zeros(words, np.uint64)
+    wc = L.voxel_bitmap_and(host_ptrs, 2, n, want.ctypes.data)
+    da, db = torch.from_numpy(a.view(np.int64)).to(dev), torch.from_numpy(b.view(np.int64)).to(dev)
+    dout = torch.zeros(words, dtype=torch.int64, device=dev)
+    dcnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    dptrs = (ctypes.c_void_p * 2)(da.data_ptr(), db.data_ptr())
+    assert L.voxel_bitmap_and_dev(ctypes.addressof(dptrs), 2, n, dout.data_ptr(), dcnt.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert int(dcnt.item()) == wc and (dout.cpu().numpy().view(np.uint64) == want).all()
+    d = inputs.config2(1 << 20, 2003)
+    pw, dd = torch.from_numpy(d["packed"].view(np.int64)).to(dev), torch.from_numpy(d["dict"]).to(dev)
+    o = torch.zeros(d["n"], dtype=torch.int32, device=dev)
+    assert L.voxel_dict_bitpack_decode_i32_dev(pw.data_ptr(), d["packed"].size, d["width"], dd.data_ptr(),
+                                               d["dict"].size, d["n"], 0, d["n"], o.data_ptr(), None) == 0
+    assert (o.cpu().numpy() == d["key"]).all()
+    idx = torch.from_numpy(d["idx"].astype(np.int32)).to(dev)
+    o2 = torch.zeros(d["n"], dtype=torch.int32, device=dev)
+    assert L.voxel_dict_decode_dev(T.I32, dd.data_ptr(), d["dict"].size, idx.data_ptr(), d["n"], o2.data_ptr(),
+                                   None) == 0
+    assert (o2.cpu().numpy() == d["key"]).all()
+    bad = idx.clone()
+    bad[777] = d["dict"].size  # one index past the dictionary
+    st = L.voxel_dict_decode_dev(T.I32, dd.data_ptr(), d["dict"].size, bad.data_ptr(), d["n"], o2.data_ptr(), None)
+    assert st == 1  # VOXEL_EINVAL

@@ -129,6 +129,9 @@ _SIGS = {
     "voxel_rle_decode_i64": (C.c_int, [vp, vp, sz, sz, sz, vp]),
     "voxel_bitpack_decode_dev": (C.c_int, [vp, sz, u32, sz, sz, sz, vp, vp]),
     "voxel_rle_decode_i64_dev": (C.c_int, [vp, vp, sz, sz, sz, vp, vp]),
+    "voxel_dict_bitpack_decode_i32_dev": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp, vp]),
+    "voxel_dict_decode_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, vp]),
+    "voxel_bitmap_and_dev": (C.c_int, [vp, sz, sz, vp, vp, vp]),
     "voxel_scan_groupby": (sz, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32, vp, vp, vp, vp, vp]),
     "voxel_scan_groupby_dev": (C.c_int, [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32,
                                           vp, vp, vp, vp, vp, vp, vp]),

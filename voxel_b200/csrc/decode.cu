@@ -20,55 +20,90 @@ namespace vx {
 namespace {
 
 constexpr int kDThreads = 256;
+constexpr size_t kGatherSmem = 32768;  // dictionaries up to 32 KB are read from shared memory
 
-__device__ __forceinline__ uint32_t unpack_row(const uint64_t* __restrict__ words, uint64_t nwords, uint64_t row,
-                                               uint32_t w, uint64_t mask) {
-    uint64_t bit = row * w;
-    uint64_t wi = bit >> 6;
-    uint32_t sh = static_cast<uint32_t>(bit & 63);
-    uint64_t v = __ldg(words + wi) >> sh;
-    if (sh + w > 64 && wi + 1 < nwords) v |= __ldg(words + wi + 1) << (64 - sh);
-    return static_cast<uint32_t>(v & mask);
-}
+// Bit-unpack (and dictionary lookup) per tile of kUnpackRows rows: the block
+// stages the tile's packed words in shared memory with independent coalesced
+// loads, then each thread decodes rows j, j+256, ... (coalesced stores).
+// Words past nwords read as zero.
+constexpr int kUnpackRows = 4096;
+constexpr int kUnpackWords = kUnpackRows * 32 / 64 + 2;  // widths up to 32
 
-__global__ void bitunpack_kernel(const uint64_t* __restrict__ words, uint64_t nwords, uint32_t w, uint64_t offset,
-                                 uint64_t count, uint32_t* __restrict__ out) {
+template <bool DICT>
+__global__ void __launch_bounds__(kDThreads) unpack_tile_kernel(const uint64_t* __restrict__ words, uint64_t nwords,
+                                                                uint32_t w, const int32_t* __restrict__ dict,
+                                                                uint32_t card, uint64_t offset, uint64_t count,
+                                                                uint32_t* __restrict__ out, int* err) {
+    __shared__ uint64_t s_w[kUnpackWords];
+    extern __shared__ __align__(16) int32_t s_dict[];
+    const bool dict_smem = DICT && card <= 8192;
+    if (dict_smem)
+        for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) s_dict[i] = dict[i];
     const uint64_t mask = w >= 64 ? ~0ull : ((1ull << w) - 1);
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        out[i] = unpack_row(words, nwords, offset + i, w, mask);
+    bool bad = false;
+    for (uint64_t tile = blockIdx.x; tile * kUnpackRows < count; tile += gridDim.x) {
+        const uint64_t r0 = offset + tile * kUnpackRows;
+        const uint32_t nb = static_cast<uint32_t>(min(static_cast<uint64_t>(kUnpackRows), count - tile * kUnpackRows));
+        const uint64_t wi0 = (r0 * w) >> 6;
+        uint64_t wi1 = ((r0 + nb) * w + 63) >> 6;  // past the last row's last bit: at most nb*w/64 + 2 words
+        if (wi1 > nwords) wi1 = nwords;
+        const uint32_t nwl = wi1 > wi0 ? static_cast<uint32_t>(wi1 - wi0) : 0;
+        for (uint32_t i = threadIdx.x; i < nwl; i += blockDim.x) s_w[i] = __ldg(words + wi0 + i);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+            const uint64_t bit = (r0 + j) * w - wi0 * 64;
+            const uint32_t li = static_cast<uint32_t>(bit >> 6), sh = static_cast<uint32_t>(bit & 63);
+            uint64_t v = li < nwl ? s_w[li] >> sh : 0;
+            if (sh + w > 64 && li + 1 < nwl) v |= s_w[li + 1] << (64 - sh);
+            const uint32_t k = static_cast<uint32_t>(v & mask);
+            uint32_t o = k;
+            if constexpr (DICT) {
+                if (k >= card) {
+                    bad = true;
+                    o = 0;
+                } else {
+                    o = static_cast<uint32_t>(dict_smem ? s_dict[k] : __ldg(dict + k));
+                }
+            }
+            out[tile * kUnpackRows + j] = o;
+        }
+        __syncthreads();
+    }
+    if (DICT && bad) atomicOr(err, 2);
 }
 
+// out[i] = dict[idx[i]]: four rows in flight per thread, the dictionary in
+// shared memory when it fits (dynamic shared memory of card entries).
 template <typename T>
-__global__ void dict_bitunpack_kernel(const uint64_t* __restrict__ words, uint64_t nwords, uint32_t w,
-                                      const T* __restrict__ dict, uint32_t card, uint64_t offset, uint64_t count,
-                                      T* __restrict__ out, int* err) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    T* sd = reinterpret_cast<T*>(sm);
-    const bool in_smem = card <= 8192;
+__global__ void __launch_bounds__(kDThreads) dict_gather_kernel(const T* __restrict__ dict, uint32_t card,
+                                                                const uint32_t* __restrict__ idx, uint64_t count,
+                                                                T* __restrict__ out, int* err) {
+    extern __shared__ __align__(16) unsigned char g_sm[];
+    T* sd = reinterpret_cast<T*>(g_sm);
+    const bool in_smem = card * sizeof(T) <= kGatherSmem;
     if (in_smem)
         for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) sd[i] = dict[i];
     __syncthreads();
-    const uint64_t mask = w >= 64 ? ~0ull : ((1ull << w) - 1);
     bool bad = false;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t k = unpack_row(words, nwords, offset + i, w, mask);
-        if (k >= card) { bad = true; out[i] = T(0); continue; }
-        out[i] = in_smem ? sd[k] : __ldg(dict + k);
-    }
-    if (bad) atomicOr(err, 2);
-}
-
-template <typename T>
-__global__ void dict_gather_kernel(const T* __restrict__ dict, uint32_t card, const uint32_t* __restrict__ idx,
-                                   uint64_t count, T* __restrict__ out, int* err) {
-    bool bad = false;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t k = __ldcs(idx + i);
-        if (k >= card) { bad = true; out[i] = T(0); continue; }
-        out[i] = __ldg(dict + k);
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < count; i0 += 4 * stride) {
+        uint32_t k[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t i = i0 + u * stride;
+            k[u] = i < count ? __ldcs(idx + i) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t i = i0 + u * stride;
+            if (i >= count) break;
+            if (k[u] >= card) {
+                bad = true;
+                out[i] = T(0);
+            } else {
+                out[i] = in_smem ? sd[k[u]] : __ldg(dict + k[u]);
+            }
+        }
     }
     if (bad) atomicOr(err, 2);
 }
@@ -125,43 +160,95 @@ __global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* _
     }
 }
 
-// rows [offset, offset+count): block b expands rows [b*R, (b+1)*R) of the output
+// rows [offset, offset+count): block b expands rows [b*R, (b+1)*R) of the
+// output.  The block knows the run covering its first row, marks each later
+// run's first row in shared memory with its run index, takes an
+// inclusive max-scan over the R rows (each row's covering run is the last
+// run starting at or before it), and writes the rows' values coalesced.
 constexpr int kRleRows = 4096;
+constexpr int kRlePer = kRleRows / kDThreads;  // rows per thread in the scan
+__device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + (j >> 5); }  // bank-conflict padding
 
 template <typename T>
 __global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restrict__ values,
                                                                const uint64_t* __restrict__ starts, uint64_t nruns,
                                                                uint64_t offset, uint64_t count, T* __restrict__ out) {
-    __shared__ uint64_t s_lo;
+    __shared__ uint32_t s_idx[kRleRows + kRleRows / 32];
+    __shared__ uint32_t s_wmax[kDThreads / 32];
+    __shared__ uint64_t s_k0;
     const uint64_t total = starts[nruns];
-    for (uint64_t blk = blockIdx.x; blk * kRleRows < count; blk += gridDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // each block expands a contiguous range of tiles: one binary search for
+    // its first tile, then the covering run of each next tile's first row is
+    // found by walking forward from the previous tile's last run
+    const uint64_t ntiles = (count + kRleRows - 1) / kRleRows;
+    const uint64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const uint64_t tb = blockIdx.x * per, te = min(ntiles, tb + per);
+    if (threadIdx.x == 0 && tb < te) {
+        const uint64_t key = offset + tb * kRleRows;
+        uint64_t lo = 0, hi = nruns;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (starts[mid] <= key) lo = mid + 1;
+            else hi = mid;
+        }
+        s_k0 = lo ? lo - 1 : 0;
+    }
+    for (uint64_t blk = tb; blk < te; ++blk) {
         const uint64_t row0 = offset + blk * kRleRows;
-        if (threadIdx.x == 0) {
-            // last run whose start <= row0 (upper_bound - 1)
-            uint64_t lo = 0, hi = nruns;
-            while (lo < hi) {
-                uint64_t mid = (lo + hi) >> 1;
-                if (starts[mid] <= row0) lo = mid + 1; else hi = mid;
-            }
-            s_lo = lo ? lo - 1 : 0;
+        const uint32_t nb = static_cast<uint32_t>(min(static_cast<uint64_t>(kRleRows), count - blk * kRleRows));
+        for (uint32_t j = threadIdx.x; j < kRleRows; j += kDThreads) s_idx[rle_pad(j)] = 0;
+        __syncthreads();
+        const uint64_t k0 = s_k0;
+        // runs after k0 start after row0 (starts are non-decreasing); each
+        // thread stops at its first run past the tile
+        for (uint64_t k = k0 + 1 + threadIdx.x; k < nruns; k += kDThreads) {
+            const uint64_t st = __ldg(starts + k);
+            if (st - row0 >= nb) break;
+            atomicMax(&s_idx[rle_pad(static_cast<uint32_t>(st - row0))], static_cast<uint32_t>(k - k0));
         }
         __syncthreads();
-        const uint64_t k0 = s_lo;
-        for (uint32_t j = threadIdx.x; j < kRleRows; j += blockDim.x) {
-            uint64_t i = blk * kRleRows + j;
-            if (i >= count) break;
-            uint64_t row = offset + i;
-            if (row >= total) { out[i] = T(0); continue; }
-            // runs are >= 1 row long, so the covering run is within j+1 runs of k0
-            uint64_t lo = k0, hi = k0 + j + 2 < nruns ? k0 + j + 2 : nruns;
-            while (lo < hi) {
-                uint64_t mid = (lo + hi) >> 1;
-                if (__ldg(starts + mid) <= row) lo = mid + 1; else hi = mid;
-            }
-            out[i] = __ldg(values + (lo - 1));
+        // inclusive max-scan: each thread a segment of kRlePer rows, then warps, then the block
+        uint32_t loc[kRlePer], m = 0;
+#pragma unroll
+        for (int e = 0; e < kRlePer; ++e) {
+            m = max(m, s_idx[rle_pad(threadIdx.x * kRlePer + e)]);
+            loc[e] = m;
+        }
+        uint32_t inc = m;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc = max(inc, y);
+        }
+        if (lane == 31) s_wmax[warp] = inc;
+        __syncthreads();
+        uint32_t pre = __shfl_up_sync(0xffffffffu, inc, 1);
+        if (lane == 0) pre = 0;
+        for (int w = 0; w < warp; ++w) pre = max(pre, s_wmax[w]);
+#pragma unroll
+        for (int e = 0; e < kRlePer; ++e) s_idx[rle_pad(threadIdx.x * kRlePer + e)] = max(pre, loc[e]);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nb; j += kDThreads) {
+            const uint64_t row = row0 + j;
+            out[blk * kRleRows + j] = row < total ? __ldg(values + k0 + s_idx[rle_pad(j)]) : T(0);
+        }
+        if (threadIdx.x == 0) {  // the next tile's first row: from the run covering this tile's last row
+            uint64_t k = k0 + s_idx[rle_pad(nb - 1)];
+            const uint64_t next = row0 + nb;
+            while (k + 1 < nruns && __ldg(starts + k + 1) <= next) ++k;
+            s_k0 = k;
         }
         __syncthreads();
     }
+}
+
+int unpack_grid(uint64_t count) {
+    int sms = sm_count() > 0 ? sm_count() : 148;
+    uint64_t b = (count + kUnpackRows - 1) / kUnpackRows;
+    uint64_t cap = static_cast<uint64_t>(sms) * 8;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : static_cast<int>(b);
 }
 
 int grid_for(uint64_t n, int per_sm = 8) {
@@ -183,7 +270,8 @@ int launch_bitunpack(const uint64_t* words, uint64_t nwords, uint32_t w, uint64_
     if (offset >= value_count) return kOk;
     if (count > value_count - offset) count = value_count - offset;  // reference stops at ValueCount
     if (!count) return kOk;
-    bitunpack_kernel<<<grid_for(count), kDThreads, 0, s>>>(words, nwords, w, offset, count, out);
+    unpack_tile_kernel<false><<<unpack_grid(count), kDThreads, 0, s>>>(words, nwords, w, nullptr, 0, offset, count,
+                                                                      out, nullptr);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -199,8 +287,8 @@ int launch_dict_bitunpack_i32(const uint64_t* words, uint64_t nwords, uint32_t w
     if (count > value_count - offset) count = value_count - offset;
     if (!count) return kOk;
     size_t smem = card <= 8192 ? card * sizeof(int32_t) : 0;
-    dict_bitunpack_kernel<int32_t><<<grid_for(count), kDThreads, smem, s>>>(words, nwords, w, dict, card, offset,
-                                                                           count, out, err);
+    unpack_tile_kernel<true><<<unpack_grid(count), kDThreads, smem, s>>>(words, nwords, w, dict, card, offset, count,
+                                                                        reinterpret_cast<uint32_t*>(out), err);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -208,18 +296,20 @@ int launch_dict_bitunpack_i32(const uint64_t* words, uint64_t nwords, uint32_t w
 int launch_dict_gather(int dtype, const void* dict, uint32_t card, const uint32_t* idx, uint64_t count, void* out,
                        int* err, cudaStream_t s) {
     if (!count) return kOk;
+    const size_t es = dtype_size(dtype);
+    const size_t smem = card * es <= kGatherSmem ? card * es : 0;
     if (dtype == F64)
-        dict_gather_kernel<double><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const double*>(dict), card, idx,
+        dict_gather_kernel<double><<<grid_for(count), kDThreads, smem, s>>>(static_cast<const double*>(dict), card, idx,
                                                                          count, static_cast<double*>(out), err);
     else if (dtype == I32)
-        dict_gather_kernel<int32_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const int32_t*>(dict), card,
+        dict_gather_kernel<int32_t><<<grid_for(count), kDThreads, smem, s>>>(static_cast<const int32_t*>(dict), card,
                                                                           idx, count, static_cast<int32_t*>(out), err);
     else if (dtype == I64 || dtype == U64)
-        dict_gather_kernel<uint64_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const uint64_t*>(dict), card,
+        dict_gather_kernel<uint64_t><<<grid_for(count), kDThreads, smem, s>>>(static_cast<const uint64_t*>(dict), card,
                                                                            idx, count, static_cast<uint64_t*>(out),
                                                                            err);
     else
-        dict_gather_kernel<uint32_t><<<grid_for(count), kDThreads, 0, s>>>(static_cast<const uint32_t*>(dict), card,
+        dict_gather_kernel<uint32_t><<<grid_for(count), kDThreads, smem, s>>>(static_cast<const uint32_t*>(dict), card,
                                                                            idx, count, static_cast<uint32_t*>(out),
                                                                            err);
     VX_CUDA(cudaGetLastError());
@@ -341,6 +431,30 @@ int voxel_dict_decode(int dtype, const void* dict, size_t card, const uint32_t* 
     if (int st = launch_dict_gather(dtype, dd.p, static_cast<uint32_t>(card), di.as<uint32_t>(), m, o.p, e, s))
         return st;
     if (int st = d2h(out, o.p, m * es, s)) return st;
+    return check(e, s);
+}
+
+int voxel_dict_bitpack_decode_i32_dev(const uint64_t* d_words, size_t nwords, uint32_t width, const int32_t* d_dict,
+                                      size_t card, size_t value_count, size_t offset, size_t count, int32_t* d_out,
+                                      void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    int* e = derr(s);
+    if (int st = launch_dict_bitunpack_i32(d_words, nwords, width, d_dict, static_cast<uint32_t>(card), value_count,
+                                           offset, count, d_out, e, s))
+        return st;
+    return check(e, s);
+}
+
+int voxel_dict_decode_dev(int dtype, const void* d_dict, size_t card, const uint32_t* d_indices, size_t count,
+                          void* d_out, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    int* e = derr(s);
+    if (int st = launch_dict_gather(dtype, d_dict, static_cast<uint32_t>(card), d_indices, count, d_out, e, s))
+        return st;
     return check(e, s);
 }
 

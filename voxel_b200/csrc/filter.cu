@@ -20,7 +20,9 @@ namespace vx {
 namespace {
 
 constexpr int kFThreads = 256;
-constexpr int kWordsPerWarp = 4;  // 256 rows per warp iteration
+// bitmap words per warp iteration (256 rows; 8 loads in flight per thread)
+template <typename T>
+constexpr int words_per_warp() { return 4; }
 
 template <typename T>
 __device__ __forceinline__ bool pred(T v, int op, T a, T b) {
@@ -36,6 +38,7 @@ __global__ void __launch_bounds__(kFThreads) vfilter_kernel(const T* __restrict_
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const uint64_t nwords = (n + 63) / 64;
+    constexpr int kWordsPerWarp = words_per_warp<T>();
     unsigned int cnt = 0;
     for (uint64_t w0 = warp * kWordsPerWarp; w0 < nwords; w0 += nwarps * kWordsPerWarp) {
         T v[kWordsPerWarp][2];
@@ -68,25 +71,50 @@ __global__ void __launch_bounds__(kFThreads) vfilter_kernel(const T* __restrict_
     }
 }
 
+constexpr int kAndMax = 64;  // bitmaps whose pointers are held in shared memory
+
 __global__ void bitmap_and_kernel(const uint64_t* const* bms, int nbm, uint64_t rows, uint64_t* out,
                                   unsigned long long* count) {
+    __shared__ const uint64_t* s_bm[kAndMax];
+    const int nsm = nbm < kAndMax ? nbm : kAndMax;
+    for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_bm[k] = bms[k];
+    __syncthreads();
     const uint64_t nwords = (rows + 63) / 64;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     unsigned int cnt = 0;
-    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
-         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint64_t x = ~0ull;
-        if (w == nwords - 1 && (rows & 63)) x = (1ull << (rows & 63)) - 1;
-        for (int k = 0; k < nbm; ++k) x &= bms[k][w];
-        out[w] = x;
-        cnt += __popcll(x);
+    for (uint64_t w0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w0 < nwords; w0 += 2 * stride) {
+        uint64_t x[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const uint64_t w = w0 + u * stride;
+            x[u] = ~0ull;
+            if (w == nwords - 1 && (rows & 63)) x[u] = (1ull << (rows & 63)) - 1;
+        }
+        for (int k = 0; k < nbm; ++k) {
+            const uint64_t* b = k < kAndMax ? s_bm[k] : bms[k];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (w0 + u * stride < nwords) x[u] &= __ldcs(b + w0 + u * stride);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const uint64_t w = w0 + u * stride;
+            if (w >= nwords) break;
+            out[w] = x[u];
+            cnt += __popcll(x[u]);
+        }
     }
     for (int d = 16; d > 0; d >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, d);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(count, static_cast<unsigned long long>(cnt));
 }
 
-// Selection vector: tile = kSelWords words per block iteration.
-constexpr int kSelThreads = 256;
-constexpr int kSelWords = kSelThreads * 4;  // 1024 words = 65536 rows per tile
+// Selection vector: tile = kSelWords words per block iteration.  Warp w of the
+// block takes words [w*512, w*512+512) of the tile in 16 rounds of 32 (lane l
+// reads word round*32 + l, coalesced); a round's rows are gathered in the
+// warp's shared-memory stage and stored as one contiguous run.
+constexpr int kSelThreads = 128;
+constexpr int kSelRounds = 16;
+constexpr int kSelWords = kSelThreads * kSelRounds;  // 2048 words = 131072 rows per tile
 
 __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* __restrict__ bitmap, uint64_t nwords,
                                                                 uint64_t rows, uint32_t* __restrict__ out,
@@ -94,59 +122,68 @@ __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* 
                                                                 unsigned long long* status, unsigned int* tile_ctr,
                                                                 int* err) {
     __shared__ uint64_t s_tile;
-    __shared__ unsigned int s_warp[kSelThreads / 32];
+    __shared__ uint64_t s_warp[kSelThreads / 32];
     __shared__ uint64_t s_base;
+    __shared__ uint32_t s_stage[kSelThreads / 32][32 * 64];
     const uint64_t ntiles = (nwords + kSelWords - 1) / kSelWords;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* const stage = s_stage[warp];
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
         __syncthreads();
         const uint64_t tile = s_tile;
         if (tile >= ntiles) break;
-        const uint64_t w0 = tile * kSelWords + threadIdx.x * 4;
-        uint64_t wv[4];
-        unsigned int c = 0;
+        const uint64_t wbase = tile * kSelWords + static_cast<uint64_t>(warp) * 32 * kSelRounds;
+        uint64_t wv[kSelRounds];
+        uint32_t rt[kSelRounds], wt = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            uint64_t w = w0 + k;
+        for (int k = 0; k < kSelRounds; ++k) {
+            const uint64_t w = wbase + k * 32 + lane;
             uint64_t x = w < nwords ? bitmap[w] : 0;
             if (w == nwords - 1 && (rows & 63)) x &= (1ull << (rows & 63)) - 1;
             wv[k] = x;
-            c += __popcll(x);
+            rt[k] = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popcll(x)));
+            wt += rt[k];
         }
-        // block exclusive scan of c
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        unsigned int inc = c;
-        for (int d = 1; d < 32; d <<= 1) {
-            unsigned int y = __shfl_up_sync(0xffffffffu, inc, d);
-            if (lane >= d) inc += y;
-        }
-        if (lane == 31) s_warp[warp] = inc;
+        if (lane == 0) s_warp[warp] = wt;
         __syncthreads();
-        if (warp == 0) {
-            unsigned int v = lane < kSelThreads / 32 ? s_warp[lane] : 0;
-            unsigned int t = v;
-            for (int d = 1; d < 32; d <<= 1) {
-                unsigned int y = __shfl_up_sync(0xffffffffu, t, d);
-                if (lane >= d) t += y;
-            }
-            if (lane < kSelThreads / 32) s_warp[lane] = t - v;
-            if (lane == kSelThreads / 32 - 1) {
-                uint64_t agg = t;
-                s_base = lookback_exclusive(status, tile, agg, err);
-            }
-        }
-        __syncthreads();
-        uint64_t pos = s_base + s_warp[warp] + (inc - c);
+        if (warp == 0) {  // warp offsets, then the tile's offset from a warp-wide look-back
+            uint64_t run = 0, mine = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+            for (int w = 0; w < kSelThreads / 32; ++w) {
+                if (lane == w) mine = run;
+                run += s_warp[w];
+            }
+            __syncwarp();
+            if (lane < kSelThreads / 32) s_warp[lane] = mine;
+            const uint64_t e = lookback_exclusive_warp(status, tile, run, err);
+            if (lane == 0) s_base = e;
+        }
+        __syncthreads();
+        uint64_t pos = s_base + s_warp[warp];
+#pragma unroll
+        for (int k = 0; k < kSelRounds; ++k) {
+            if (rt[k] == 0) continue;  // uniform over the warp
             uint64_t x = wv[k];
-            uint64_t baseRow = (w0 + k) * 64;
+            const uint32_t c = __popcll(x);
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t q = incl - c;
+            const uint32_t row0 = static_cast<uint32_t>((wbase + k * 32 + lane) * 64);
             while (x) {
-                out[pos++] = static_cast<uint32_t>(baseRow + __ffsll(static_cast<long long>(x)) - 1);
+                stage[q++] = row0 + static_cast<uint32_t>(__ffsll(static_cast<long long>(x)) - 1);
                 x &= x - 1;
             }
+            __syncwarp();
+            for (uint32_t i = lane; i < rt[k]; i += 32) out[pos + i] = stage[i];
+            __syncwarp();
+            pos += rt[k];
         }
-        if (tile == ntiles - 1 && threadIdx.x == kSelThreads - 1) *count = pos;
+        if (tile == ntiles - 1 && threadIdx.x == kSelThreads - 1) *count = s_base + s_warp[warp] + wt;
         __syncthreads();
     }
 }
@@ -158,6 +195,7 @@ int launch_vfilter_t(const void* d, uint64_t n, int op, uint64_t a, uint64_t b, 
     std::memcpy(&ta, &a, sizeof(T));
     std::memcpy(&tb, &b, sizeof(T));
     uint64_t words = (n + 63) / 64;
+    constexpr int kWordsPerWarp = words_per_warp<T>();
     uint64_t warps_needed = (words + kWordsPerWarp - 1) / kWordsPerWarp;
     int sms = sm_count() > 0 ? sm_count() : 148;
     uint64_t blocks = (warps_needed * 32 + kFThreads - 1) / kFThreads;
@@ -289,8 +327,12 @@ int voxel_selection_from_bitmap_dev(const uint64_t* d_bitmap, size_t rows, uint3
     clear_error();
     if (int st = ensure_device()) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
-    DevBuf scratch(selection_scratch_bytes(rows));
-    if (!scratch.p) return kErrOutOfMemory;
+    static thread_local DevBuf scratch;  // look-back words, kept between calls
+    const size_t need = selection_scratch_bytes(rows);
+    if (scratch.n < need) {
+        scratch = DevBuf(need);
+        if (!scratch.p) return kErrOutOfMemory;
+    }
     int* err = t_err.get(s);
     int st = launch_selection(d_bitmap, rows, d_out, reinterpret_cast<unsigned long long*>(d_count), scratch.p, err, s);
     if (st) return st;
@@ -311,6 +353,23 @@ size_t voxel_selection_from_bitmap(const uint64_t* bitmap, size_t rows, uint32_t
     if (d2h(&cnt, c.p, 8, s) || sync(s)) return static_cast<size_t>(-1);
     if (cnt && (d2h(out, o.p, cnt * 4, s) || sync(s))) return static_cast<size_t>(-1);
     return cnt;
+}
+
+int voxel_bitmap_and_dev(const uint64_t* const* d_bitmaps, size_t nbm, size_t rows, uint64_t* d_out,
+                         uint64_t* d_count, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    static thread_local DevBuf table;  // the device copy of the pointer table
+    if (table.n < nbm * sizeof(void*) + 8) {
+        table = DevBuf(nbm * sizeof(void*) + 8);
+        if (!table.p) return kErrOutOfMemory;
+    }
+    if (nbm) {
+        if (int st = h2d(table.p, d_bitmaps, nbm * sizeof(void*), s)) return st;
+    }
+    return launch_bitmap_and(static_cast<const uint64_t* const*>(table.p), static_cast<int>(nbm), rows, d_out,
+                             reinterpret_cast<unsigned long long*>(d_count), s);
 }
 
 size_t voxel_bitmap_and(const uint64_t* const* bitmaps, size_t nbm, size_t rows, uint64_t* out) {
