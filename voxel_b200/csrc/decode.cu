@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(kDThreads) dict_gather_kernel(const T* __restr
 }
 
 // exclusive prefix of u32 run lengths -> u64 row starts (single pass)
-constexpr int kRunsPerTile = kDThreads * 8;
+constexpr int kRunsPer = 16;  // runs per thread
+constexpr int kRunsPerTile = kDThreads * kRunsPer;
 
 __global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* __restrict__ runs, uint64_t nruns,
                                                                uint64_t* __restrict__ starts,
@@ -123,14 +124,21 @@ __global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* _
         __syncthreads();
         uint64_t tile = s_tile;
         if (tile >= ntiles) break;
-        uint64_t r0 = tile * kRunsPerTile + threadIdx.x * 8;
-        uint64_t v[8];
+        uint64_t r0 = tile * kRunsPerTile + threadIdx.x * kRunsPer;
+        uint32_t v[kRunsPer];
         uint64_t c = 0;
+        if (r0 + kRunsPer <= nruns && (reinterpret_cast<uintptr_t>(runs + r0) & 15) == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            v[k] = r0 + k < nruns ? runs[r0 + k] : 0;
-            c += v[k];
+            for (int k = 0; k < kRunsPer; k += 4) {
+                const uint4 q = __ldcs(reinterpret_cast<const uint4*>(runs + r0 + k));
+                v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kRunsPer; ++k) v[k] = r0 + k < nruns ? runs[r0 + k] : 0;
         }
+#pragma unroll
+        for (int k = 0; k < kRunsPer; ++k) c += v[k];
         int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         uint64_t inc = c;
         for (int d = 1; d < 32; d <<= 1) {
@@ -146,26 +154,29 @@ __global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* _
                 if (lane >= d) t += y;
             }
             if (lane < kDThreads / 32) s_warp[lane] = t - x;
-            if (lane == kDThreads / 32 - 1) s_base = lookback_exclusive(status, tile, t, err);
+            const uint64_t tile_total = __shfl_sync(0xffffffffu, t, 31);
+            const uint64_t e = lookback_exclusive_warp(status, tile, tile_total, err);
+            if (lane == 0) s_base = e;
         }
         __syncthreads();
         uint64_t pos = s_base + s_warp[warp] + (inc - c);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < kRunsPer; ++k) {
             if (r0 + k < nruns) starts[r0 + k] = pos;
             pos += v[k];
         }
-        if (r0 < nruns && r0 + 8 >= nruns) starts[nruns] = pos;  // the thread holding the last run: total rows
+        if (r0 < nruns && r0 + kRunsPer >= nruns) starts[nruns] = pos;  // the thread holding the last run: total rows
         __syncthreads();
     }
 }
 
 // rows [offset, offset+count): block b expands rows [b*R, (b+1)*R) of the
 // output.  The block knows the run covering its first row, marks each later
-// run's first row in shared memory with its run index, takes an
-// inclusive max-scan over the R rows (each row's covering run is the last
-// run starting at or before it), and writes the rows' values coalesced.
-constexpr int kRleRows = 4096;
+// run's first row in shared memory with its run index (and stages the runs'
+// values there), takes an inclusive max-scan over the R rows (each row's
+// covering run is the last run starting at or before it), and writes the
+// rows' values coalesced.
+constexpr int kRleRows = 2048;
 constexpr int kRlePer = kRleRows / kDThreads;  // rows per thread in the scan
 __device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + (j >> 5); }  // bank-conflict padding
 
@@ -174,6 +185,7 @@ __global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restri
                                                                const uint64_t* __restrict__ starts, uint64_t nruns,
                                                                uint64_t offset, uint64_t count, T* __restrict__ out) {
     __shared__ uint32_t s_idx[kRleRows + kRleRows / 32];
+    __shared__ T s_val[kRleRows];  // values of runs k0 .. k0 + kRleRows - 1
     __shared__ uint32_t s_wmax[kDThreads / 32];
     __shared__ uint64_t s_k0;
     const uint64_t total = starts[nruns];
@@ -197,15 +209,19 @@ __global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restri
     for (uint64_t blk = tb; blk < te; ++blk) {
         const uint64_t row0 = offset + blk * kRleRows;
         const uint32_t nb = static_cast<uint32_t>(min(static_cast<uint64_t>(kRleRows), count - blk * kRleRows));
-        for (uint32_t j = threadIdx.x; j < kRleRows; j += kDThreads) s_idx[rle_pad(j)] = 0;
+#pragma unroll
+        for (int e = 0; e < kRlePer; ++e) s_idx[rle_pad(threadIdx.x + e * kDThreads)] = 0;
         __syncthreads();
         const uint64_t k0 = s_k0;
+        if (threadIdx.x == 0) s_val[0] = __ldg(values + k0);
         // runs after k0 start after row0 (starts are non-decreasing); each
         // thread stops at its first run past the tile
         for (uint64_t k = k0 + 1 + threadIdx.x; k < nruns; k += kDThreads) {
             const uint64_t st = __ldg(starts + k);
             if (st - row0 >= nb) break;
-            atomicMax(&s_idx[rle_pad(static_cast<uint32_t>(st - row0))], static_cast<uint32_t>(k - k0));
+            const uint32_t rel = static_cast<uint32_t>(k - k0);
+            atomicMax(&s_idx[rle_pad(static_cast<uint32_t>(st - row0))], rel);
+            if (rel < kRleRows) s_val[rel] = __ldg(values + k);
         }
         __syncthreads();
         // inclusive max-scan: each thread a segment of kRlePer rows, then warps, then the block
@@ -229,9 +245,15 @@ __global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restri
 #pragma unroll
         for (int e = 0; e < kRlePer; ++e) s_idx[rle_pad(threadIdx.x * kRlePer + e)] = max(pre, loc[e]);
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < nb; j += kDThreads) {
-            const uint64_t row = row0 + j;
-            out[blk * kRleRows + j] = row < total ? __ldg(values + k0 + s_idx[rle_pad(j)]) : T(0);
+#pragma unroll
+        for (int e = 0; e < kRlePer; ++e) {
+            const uint32_t j = threadIdx.x + e * kDThreads;
+            if (j < nb) {
+                const uint32_t rel = s_idx[rle_pad(j)];
+                // more than kRleRows runs start in the tile only with empty runs
+                const T x = rel < kRleRows ? s_val[rel] : __ldg(values + k0 + rel);
+                out[blk * kRleRows + j] = row0 + j < total ? x : T(0);
+            }
         }
         if (threadIdx.x == 0) {  // the next tile's first row: from the run covering this tile's last row
             uint64_t k = k0 + s_idx[rle_pad(nb - 1)];
