@@ -34,12 +34,13 @@ __global__ void __launch_bounds__(kDThreads) unpack_tile_kernel(const uint64_t* 
                                                                 uint32_t w, const int32_t* __restrict__ dict,
                                                                 uint32_t card, uint64_t offset, uint64_t count,
                                                                 uint32_t* __restrict__ out, int* err) {
-    __shared__ uint64_t s_w[kUnpackWords];
+    __shared__ uint64_t s_w[kUnpackWords + 1];  // + one word read (masked off) past the last value
     extern __shared__ __align__(16) int32_t s_dict[];
     const bool dict_smem = DICT && card <= 8192;
     if (dict_smem)
         for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) s_dict[i] = dict[i];
-    const uint64_t mask = w >= 64 ? ~0ull : ((1ull << w) - 1);
+    const uint32_t mask = w >= 32 ? ~0u : ((1u << w) - 1u);
+    const uint32_t* s_w32 = reinterpret_cast<const uint32_t*>(s_w);  // little-endian halves of s_w
     bool bad = false;
     for (uint64_t tile = blockIdx.x; tile * kUnpackRows < count; tile += gridDim.x) {
         const uint64_t r0 = offset + tile * kUnpackRows;
@@ -48,14 +49,22 @@ __global__ void __launch_bounds__(kDThreads) unpack_tile_kernel(const uint64_t* 
         uint64_t wi1 = ((r0 + nb) * w + 63) >> 6;  // past the last row's last bit: at most nb*w/64 + 2 words
         if (wi1 > nwords) wi1 = nwords;
         const uint32_t nwl = wi1 > wi0 ? static_cast<uint32_t>(wi1 - wi0) : 0;
-        for (uint32_t i = threadIdx.x; i < nwl; i += blockDim.x) s_w[i] = __ldg(words + wi0 + i);
+#pragma unroll
+        for (int e = 0; e < (kUnpackWords + kDThreads - 1) / kDThreads; ++e) {
+            const uint32_t i = threadIdx.x + e * kDThreads;
+            if (i < nwl) s_w[i] = __ldg(words + wi0 + i);
+        }
+        if (threadIdx.x == 0) s_w[nwl] = 0;  // words past nwords read as zero
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
-            const uint64_t bit = (r0 + j) * w - wi0 * 64;
-            const uint32_t li = static_cast<uint32_t>(bit >> 6), sh = static_cast<uint32_t>(bit & 63);
-            uint64_t v = li < nwl ? s_w[li] >> sh : 0;
-            if (sh + w > 64 && li + 1 < nwl) v |= s_w[li + 1] << (64 - sh);
-            const uint32_t k = static_cast<uint32_t>(v & mask);
+        const uint32_t b0 = static_cast<uint32_t>(r0 * w - wi0 * 64);  // the tile's first bit in s_w (< 64)
+#pragma unroll 4
+        for (int e = 0; e < kUnpackRows / kDThreads; ++e) {
+            const uint32_t j = threadIdx.x + e * kDThreads;
+            if (j >= nb) break;
+            const uint32_t bit = b0 + j * w;  // < 64 + 4096 * 32
+            // a value of <= 32 bits spans at most two 32-bit words
+            const uint32_t q = bit >> 5;
+            const uint32_t k = q < 2 * nwl ? __funnelshift_r(s_w32[q], s_w32[q + 1], bit & 31) & mask : 0u;
             uint32_t o = k;
             if constexpr (DICT) {
                 if (k >= card) {
