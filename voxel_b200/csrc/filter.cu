@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* 
         for (int k = 0; k < kSelRounds; ++k) {
             const uint64_t w = wbase + k * 32 + lane;
             uint64_t x = w < nwords ? bitmap[w] : 0;
-            if (w == nwords - 1 && (rows & 63)) x &= (1ull << (rows & 63)) - 1;
+            if (w == nwords - 1 && (rows & 63)) x &= (1ull << (rows & 63)) - 1;  // tail word: existing rows only
             wv[k] = x;
             rt[k] = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(__popcll(x)));
             wt += rt[k];
@@ -170,7 +170,8 @@ __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* 
         uint64_t pos = s_base + s_warp[warp];
 #pragma unroll
         for (int k = 0; k < kSelRounds; ++k) {
-            if (rt[k] == 0) continue;  // uniform over the warp
+            const uint32_t rk = rt[k];
+            if (rk == 0) continue;  // uniform over the warp
             uint64_t x = wv[k];
             const uint32_t c = __popcll(x);
             uint32_t incl = c;
@@ -186,9 +187,9 @@ __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* 
                 x &= x - 1;
             }
             __syncwarp();
-            for (uint32_t i = lane; i < rt[k]; i += 32) out[pos + i] = stage[i];
+            for (uint32_t i = lane; i < rk; i += 32) out[pos + i] = stage[i];
             __syncwarp();
-            pos += rt[k];
+            pos += rk;
         }
         if (tile == ntiles - 1 && threadIdx.x == kSelThreads - 1) *count = s_base + s_warp[warp] + wt;
         __syncthreads();
@@ -300,7 +301,14 @@ struct ErrWord {
 thread_local ErrWord t_err;
 
 int check_err(int* d_err, cudaStream_t s) {
-    int h = 0;
+    static thread_local int* h_err = nullptr;  // pinned: the read-back is one small DMA
+    if (!h_err && cudaHostAlloc(reinterpret_cast<void**>(&h_err), sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        h_err = nullptr;
+    }
+    int local = 0;
+    int& h = h_err ? *h_err : local;
+    h = 0;
     int st = d2h(&h, d_err, 4, s);
     if (st) return st;
     st = sync(s);
