@@ -765,6 +765,34 @@ def workload_ops(args, L, rank, world, local, dist, dev):
         "rle_decode_i64": (lambda: ok(L.voxel_rle_decode_i64_dev(rvals.data_ptr(), runs.data_ptr(), nruns, 0, rrows,
                                                                  outi.data_ptr(), sh)), nruns * 12 + rrows * 8),
     }
+    # the general scan kernel (two atoms: not the one-atom fast path), through
+    # the engine with a device segment; its device time is the engine's own
+    from voxel_b200 import estimator as Est
+    from voxel_b200 import templates as Tm
+
+    prog2 = Tm.build(Tm.F64, [Tm.Pred(5, 100.0), Tm.Pred(2, 900.0)], "SUM")
+    code2 = np.asarray(prog2.code, np.uint32)
+    regs2 = prog2.registers(n)
+    eng = L.voxel_engine_create_f64()
+    L.voxel_engine_add_segment_device(eng, f64.data_ptr(), n)
+
+    def run_scan2():
+        for r_, v_ in enumerate(regs2):
+            L.voxel_engine_set_scalar(eng, r_, v_)
+        L.voxel_engine_load_program(eng, code2.ctypes.data, code2.size)
+        ok(L.voxel_engine_run_status(eng))
+        return L.voxel_engine_last_device_ms(eng)
+
+    agg = L.voxel_agg_create()
+    L.voxel_agg_init(agg, card)
+    na = n // 2
+    akeys = idx[:na]
+    avals = f64[:na]
+    ops["engine_scan_2pred_sum_f64"] = (run_scan2, n * 8)
+    ops["agg_accumulate_u32_f64"] = (lambda: ok(L.voxel_agg_accumulate_dev(agg, akeys.data_ptr(), avals.data_ptr(), na,
+                                                                           sh)), na * 12)
+    ops["sketch_column_f64"] = (lambda: Est.sketch(0, f64.data_ptr(), n), n * 8)
+    timing = {"engine_scan_2pred_sum_f64": "engine device time", "sketch_column_f64": "wall clock (returns to host)"}
     launches = {"rle_decode_i64": 2}
     res = {}
     total_bytes, total_ms, nl = 0, 0.0, 0
@@ -779,6 +807,15 @@ def workload_ops(args, L, rank, world, local, dist, dev):
                 flush.zero_()  # on the current stream: evict the previous launch's lines from L2
                 torch.cuda.current_stream().synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                if timing.get(name, "").startswith("engine"):
+                    ms.append(fn())
+                    continue
+                if timing.get(name, "").startswith("wall"):
+                    w0_ = time.perf_counter()
+                    fn()
+                    torch.cuda.synchronize()
+                    ms.append((time.perf_counter() - w0_) * 1e3)
+                    continue
                 e0.record(stream)
                 fn()
                 e1.record(stream)
@@ -788,12 +825,14 @@ def workload_ops(args, L, rank, world, local, dist, dev):
                 nbytes = words * 8 + 4 * int(cnt[3].item())
             m = _max_over_ranks(dist, dev, statistics.mean(ms))
             gbs = nbytes / (m * 1e-3) / 1e9
+            rows_ = rrows if name == "rle_decode_i64" else na if name == "agg_accumulate_u32_f64" else n
             res[name] = {"ms": m, "GB/s": gbs, "frac": gbs / peak, "bytes": nbytes,
-                         "M_rows/s": (rrows if name == "rle_decode_i64" else n) / (m * 1e-3) / 1e6}
+                         "M_rows/s": rows_ / (m * 1e-3) / 1e6, "timing": timing.get(name, "CUDA events")}
             total_bytes += nbytes
             total_ms += m
             nl += args.steps * launches.get(name, 1)
     # spot checks against torch on the device
+    want_sum2 = float(f64[(f64 >= 100.0) & (f64 < 900.0)].sum().item())
     checks = {
         "vfilter_count": int(cnt[0].item()) == int((f64 > 900.0).sum().item()),
         "between_count": int(cnt[1].item()) == int(((i32 >= 100) & (i32 <= 499)).sum().item()),
@@ -802,7 +841,10 @@ def workload_ops(args, L, rank, world, local, dist, dev):
                                       torch.nonzero(f64 > 900.0).flatten())),
         "dict_decode": bool(torch.equal(outf, dictf[idx.long()])),
         "rle_decode": bool(torch.equal(outi, torch.repeat_interleave(rvals, runs.long()))),
+        "scan_2pred_sum": abs(L.voxel_engine_get_scalar_f64(eng, 0) - want_sum2) <= 1e-12 * abs(want_sum2),
     }
+    L.voxel_engine_destroy(eng)
+    L.voxel_agg_destroy(agg)
     # e2e: the host entry point of the f64 filter (pinned host column in, bitmap out)
     hcol = f64.cpu().pin_memory()
     hbm = np.empty(words, np.uint64)
@@ -840,12 +882,14 @@ def workload_ops(args, L, rank, world, local, dist, dev):
     top = max(res, key=lambda k: res[k]["ms"])
     value = world * total_bytes / (total_ms * 1e-3) / 1e9
     roof = _roofline("ops_kernels", total_bytes, total_ms)
-    roof["note"] = "aggregate of the eight kernels (sum of algorithmic bytes / sum of launch times); per kernel in config.ops"
+    roof["note"] = "aggregate of all kernels (sum of algorithmic bytes / sum of launch times); per kernel in config.ops"
     return _common_line(
         "filter/decode kernels GB/s (sum of bytes / sum of times)", UNIT, value, world, args, total_ms,
         {"workload": f"{n} rows per column: f64 U[0,1000) > 900, i32 U[0,1000) BETWEEN 100 AND 499, AND of the two "
                      f"bitmaps, selection vector of the f64 bitmap, 10-bit unpack, dictionary ({card}) decode of the "
-                     f"packed indices and of u32 indices into f64, RLE i64 ({nruns} runs of 1-15 rows)",
+                     f"packed indices and of u32 indices into f64, RLE i64 ({nruns} runs of 1-15 rows), a two-predicate "
+                     f"f64 SUM program through the engine, HashAggregator accumulate of {na} (u32 key, f64) rows over "
+                     f"{card} keys, the estimator's column sketch (min/max, histogram, HLL) of the f64 column",
          "ops": res, "checks": checks, "slowest": top, "l2": "256 MB written before every timed launch",
          "parallelism": f"replicas x{world}"},
         roof, cpu, e2e, clk.summary(), nl, "mixed")

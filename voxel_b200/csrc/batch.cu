@@ -26,6 +26,7 @@
 
 #include "batch.h"
 #include "engine.h"
+#include "rangeform.h"
 #include "scan_core.cuh"
 #include "voxel_c.h"
 #include "vx_runtime.h"
@@ -41,11 +42,6 @@ constexpr int kBW = 8;          // passes per item
 constexpr int kBNR = 4;         // reductions per batched program
 constexpr uint64_t kItemGroups = static_cast<uint64_t>(kBThreads) * kBU * kBW;
 constexpr int kRangeBlocks = 4;  // resident blocks per SM of the range-form kernels
-// The accumulator fold a range-form program uses for each reduction kind
-// (SUM: ADDF on floats, ADD on integers; COUNT: ADD; MIN / MAX: MIN / MAX).
-__host__ __device__ constexpr uint8_t range_acc(int rk, bool is_float) {
-    return rk == kRedSum ? (is_float ? kAccAddF : kAccAdd) : rk == kRedCount ? kAccAdd : rk == kRedMin ? kAccMin : kAccMax;
-}
 
 // shared memory of one block's current item (one copy for every element type)
 struct ItemShared {
@@ -636,114 +632,16 @@ int launch_class(int cls, const BatchProg* progs, const uint32_t* pids, uint32_t
 #undef VX_KIND
 }
 
-// Host: the range form of a program (BatchProg::fast), when it has one.  The
-// conjunction of ordered atoms (EQ LT LE GT GE) on column 0 is the interval
-// [lo, hi] in T's order (x < t is x <= the next value below t, and so on; an
-// empty set is lo > hi); NE atoms stay as up to two excluded values (an NE
-// against a NaN threshold holds for every x and is dropped).  A program
-// qualifies with one column, one reduction whose predicate is all atoms and
-// whose false value is a constant, and at least one ordered atom.
-template <typename T>
-T host_from_bits(uint64_t b) {
-    T v;
-    if constexpr (sizeof(T) == 8) {
-        std::memcpy(&v, &b, 8);
-    } else {
-        const uint32_t w = static_cast<uint32_t>(b);
-        std::memcpy(&v, &w, 4);
-    }
-    return v;
-}
-
-template <typename T>
-uint64_t host_to_bits(T v) {
-    if constexpr (sizeof(T) == 8) {
-        uint64_t b;
-        std::memcpy(&b, &v, 8);
-        return b;
-    } else {
-        uint32_t w;
-        std::memcpy(&w, &v, 4);
-        return w;
-    }
-}
-
-template <typename T>
-bool range_form(BatchProg& bp) {
-    const ScanParams& p = bp.p;
-    if (p.ncols != 1 || p.nred != 1 || p.natoms < 1 || p.natoms > kMaxAtoms) return false;
-    const uint32_t all = (1u << p.natoms) - 1u;
-    const Red& r = p.red[0];
-    if (r.pmask != all || bp.sel_mask != all || r.kind > kRedMax) return false;
-    constexpr bool kFloat = std::is_floating_point<T>::value;
-    if (r.acc != range_acc(r.kind, kFloat)) return false;
-    // COUNT counts a constant (the VCOUNT of M & one); the others reduce the column
-    if (r.kind == kRedCount ? (r.a.kind != kOpConst && r.a.kind != kOpZero) : (r.a.kind != kOpCol || r.a.col != 0))
-        return false;
-    if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
-    const T lowest = kFloat ? -std::numeric_limits<T>::infinity() : std::numeric_limits<T>::lowest();
-    const T highest = kFloat ? std::numeric_limits<T>::infinity() : std::numeric_limits<T>::max();
-    T lo = lowest, hi = highest, ne[2] = {T(0), T(0)};
-    int nne = 0;
-    bool ordered = false, empty = false;
-    for (int a = 0; a < p.natoms; ++a) {
-        const Atom& at = p.atom[a];
-        if (at.col != 0 || at.op > 5) return false;
-        const T t = host_from_bits<T>(at.thr);
-        const bool nan = t != t;
-        if (at.op == 1) {  // NE
-            if (nan) continue;
-            if (nne == 2) return false;
-            ne[nne++] = t;
-            continue;
-        }
-        ordered = true;
-        if (nan) {
-            empty = true;
-            continue;
-        }
-        T l = lowest, h = highest;
-        switch (at.op) {
-        case 0: l = h = t; break;  // EQ
-        case 2:                    // LT
-            if (t == lowest) empty = true;
-            else if constexpr (kFloat) h = std::nextafter(t, lowest);
-            else h = static_cast<T>(t - 1);
-            break;
-        case 3: h = t; break;  // LE
-        case 4:                // GT
-            if (t == highest) empty = true;
-            else if constexpr (kFloat) l = std::nextafter(t, highest);
-            else l = static_cast<T>(t + 1);
-            break;
-        default: l = t; break;  // GE
-        }
-        if (l > lo) lo = l;
-        if (h < hi) hi = h;
-    }
-    if (!ordered) return false;
-    if (empty || lo > hi) {
-        lo = highest;
-        hi = lowest;
-    }
-    if (nne == 1) ne[1] = ne[0];
-    bp.lo = host_to_bits(lo);
-    bp.hi = host_to_bits(hi);
-    bp.ne[0] = host_to_bits(ne[0]);
-    bp.ne[1] = host_to_bits(ne[1]);
-    bp.fast = 1u + 2u * r.kind + (nne ? 1u : 0u);
-    return true;
-}
-
 bool set_range_form(BatchProg& bp) {
-    switch (bp.p.dtype) {
-    case F64: return range_form<double>(bp);
-    case F32: return range_form<float>(bp);
-    case I64: return range_form<int64_t>(bp);
-    case I32: return range_form<int32_t>(bp);
-    case U64: return range_form<uint64_t>(bp);
-    default: return range_form<uint32_t>(bp);
-    }
+    RangeForm rf;
+    const uint32_t all = bp.p.natoms ? (1u << bp.p.natoms) - 1u : 0u;
+    if (bp.sel_mask != all || !range_form_of(bp.p, &rf)) return false;
+    bp.fast = rf.fast;
+    bp.lo = rf.lo;
+    bp.hi = rf.hi;
+    bp.ne[0] = rf.ne[0];
+    bp.ne[1] = rf.ne[1];
+    return true;
 }
 
 __global__ void clear_outs_kernel(BatchOut* outs, uint32_t n) {

@@ -127,6 +127,116 @@ __global__ void accumulate_kernel(Table t, const uint32_t* __restrict__ keys, co
     if (bad) atomicOr(err, 1);
 }
 
+// Phase 2 for tables of up to kSmemSlots slots: each block folds its rows into
+// a shared-memory copy of the per-slot state (native 32-bit atomics), then adds
+// it to the table once.  The sum is the same 192-bit integer (LSB 2^-96) the
+// global path accumulates, kept as six 32-bit words: a row adds
+// trunc(|x| * 2^96) (three words at word k0, or subtracts it for x < 0) and a
+// word's wrap, read from the atomic's returned old value, ripples upward, so
+// concurrent rows compose to the exact sum in any order.
+constexpr uint32_t kSmemSlots = 2048;
+constexpr int kAccWords = 6;
+
+struct Words96 {
+    uint32_t c0, c1, c2;
+    int k0;
+};
+
+// trunc(|x| * 2^96) as three words at word k0; false for NaN / inf / |x| >= 2^63
+__device__ __forceinline__ bool words96(double x, Words96* w) {
+    const uint64_t b = static_cast<uint64_t>(__double_as_longlong(x));
+    const int ex = static_cast<int>((b >> 52) & 0x7FF);
+    w->c0 = w->c1 = w->c2 = 0;
+    w->k0 = 0;
+    if (ex == 0x7FF) return false;
+    if (ex == 0) return true;  // zero or subnormal: below the window
+    uint64_t m = (b & ((1ull << 52) - 1)) | (1ull << 52);
+    int sh = ex - 1075 + 96;  // |x| * 2^96 = m * 2^sh
+    if (sh >= 107) return false;  // |x| >= 2^63
+    if (sh < 0) {
+        m = sh > -64 ? (m >> -sh) : 0;
+        sh = 0;
+    }
+    const uint32_t ml = static_cast<uint32_t>(m), mh = static_cast<uint32_t>(m >> 32);
+    const uint32_t r = static_cast<uint32_t>(sh) & 31;
+    w->k0 = sh >> 5;  // <= 3: words k0..k0+2 lie inside the 6 words
+    w->c0 = ml << r;
+    w->c1 = __funnelshift_l(ml, mh, r);
+    w->c2 = __funnelshift_l(mh, 0u, r);
+    return true;
+}
+
+__device__ __noinline__ void ripple96(uint32_t* acc, int j, bool borrow) {
+    for (; j < kAccWords; ++j) {
+        const uint32_t old = atomicAdd(&acc[j], borrow ? 0xFFFFFFFFu : 1u);
+        if (borrow ? (old != 0u) : (old != 0xFFFFFFFFu)) break;
+    }
+}
+
+__device__ __forceinline__ void add96(uint32_t* acc, const Words96& w, bool neg) {
+    const uint32_t d0 = neg ? 0u - w.c0 : w.c0, d1 = neg ? 0u - w.c1 : w.c1, d2 = neg ? 0u - w.c2 : w.c2;
+    uint32_t o0 = 0, o1 = 0, o2 = 0;
+    if (w.c0) o0 = atomicAdd(&acc[w.k0], d0);
+    if (w.c1) o1 = atomicAdd(&acc[w.k0 + 1], d1);
+    if (w.c2) o2 = atomicAdd(&acc[w.k0 + 2], d2);
+    const bool r0 = w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0);
+    const bool r1 = w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1);
+    const bool r2 = w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2);
+    if (r0) ripple96(acc, w.k0 + 1, neg);
+    if (r1) ripple96(acc, w.k0 + 2, neg);
+    if (r2) ripple96(acc, w.k0 + 3, neg);
+}
+
+__global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uint32_t* __restrict__ keys,
+                                                              const double* __restrict__ vals, uint64_t n, int* err) {
+    extern __shared__ __align__(16) unsigned long long a_sm[];
+    const uint32_t cap = static_cast<uint32_t>(t.mask + 1);
+    unsigned long long* s_mn = a_sm;
+    unsigned long long* s_mx = s_mn + cap;
+    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + cap);
+    uint32_t* s_cnt = s_w + kAccWords * cap;
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < kAccWords; ++k) s_w[kAccWords * i + k] = 0;
+        s_cnt[i] = 0;
+        s_mn[i] = ~0ull;
+        s_mx[i] = 0;
+    }
+    __syncthreads();
+    bool bad = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t sl = find_slot(t, __ldcs(keys + i));
+        if (sl == ~0ull) {
+            bad = true;
+            continue;
+        }
+        const double v = __ldcs(vals + i);
+        Words96 w;
+        if (words96(v, &w)) add96(s_w + kAccWords * sl, w, v < 0.0);
+        else bad = true;
+        atomicAdd(&s_cnt[sl], 1u);
+        const uint64_t ok = f64_order_key(v);
+        if (ok < s_mn[sl]) atomicMin(&s_mn[sl], static_cast<unsigned long long>(ok));
+        if (ok > s_mx[sl]) atomicMax(&s_mx[sl], static_cast<unsigned long long>(ok));
+    }
+    if (bad) atomicOr(err, 1);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) {
+        const uint32_t c = s_cnt[i];
+        if (!c) continue;
+        const uint32_t* w = s_w + kAccWords * i;
+        const Fix3 f{w[0] | (static_cast<uint64_t>(w[1]) << 32), w[2] | (static_cast<uint64_t>(w[3]) << 32),
+                     w[4] | (static_cast<uint64_t>(w[5]) << 32)};
+        fix_atomic_add(&t.sum[3 * i], f);
+        atomicAdd(&t.cnt[i], static_cast<unsigned long long>(c));
+        atomicMin(&t.mn[i], s_mn[i]);
+        atomicMax(&t.mx[i], s_mx[i]);
+    }
+}
+
+size_t smem_table_bytes(uint64_t cap) { return cap * (2 * 8 + kAccWords * 4 + 4); }
+
 // move every occupied slot of `from` into `to` (a grow)
 __global__ void rehash_kernel(Table from, Table to) {
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= from.mask;
@@ -479,7 +589,24 @@ public:
             if (!ovf) break;
             if (int st = grow(s)) return st;
         }
-        accumulate_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, dv, n, oerr(s));
+        if (cap <= kSmemSlots) {  // per-block shared-memory state, one flush per block
+            const size_t smem = smem_table_bytes(cap);
+            static bool attr_set = false;
+            if (!attr_set) {
+                VX_CUDA(cudaFuncSetAttribute(accumulate_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem_table_bytes(kSmemSlots))));
+                attr_set = true;
+            }
+            int per_sm = 0;
+            VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, accumulate_smem_kernel, 512, smem));
+            if (per_sm < 1) per_sm = 1;
+            const int sms = sm_count() > 0 ? sm_count() : 148;
+            uint64_t blocks = (n + 511) / 512;
+            if (blocks > static_cast<uint64_t>(sms) * per_sm) blocks = static_cast<uint64_t>(sms) * per_sm;
+            accumulate_smem_kernel<<<static_cast<unsigned>(blocks), 512, smem, s>>>(t, dk, dv, n, oerr(s));
+        } else {
+            accumulate_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, dv, n, oerr(s));
+        }
         VX_CUDA(cudaGetLastError());
         return ocheck(s, "group-by");
     }

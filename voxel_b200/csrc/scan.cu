@@ -8,6 +8,7 @@
 // grid.
 #include <cstdio>
 
+#include "rangeform.h"
 #include "scan.h"
 #include "scan_core.cuh"
 #include "vx_runtime.h"
@@ -196,6 +197,115 @@ int fsum_grid(uint64_t ndata) {
     return g < 1 ? 1 : static_cast<int>(g);
 }
 
+// Range form (rangeform.h) of a one-column, one-reduction program: the atoms'
+// conjunction as lo <= x <= hi (and x != ne[0], x != ne[1] when NE) with the
+// reduction kind RK and its canonical fold fixed per instance.  Per group the
+// lane values, the group result, the fold, the block partials and the
+// finalisation are the generic kernel's, so results are the same bits.
+template <typename T, int RK, bool NE>
+__global__ void __launch_bounds__(kThreads, 6) range_scan_kernel(const __grid_constant__ ScanParams p,
+                                                                const RangeForm rf, int vec, ScanPartial* part,
+                                                                unsigned int* done, ScanResult* out) {
+    constexpr int KL = 32 / sizeof(T);
+    constexpr uint8_t accop = range_acc(RK, Traits<T>::kFloat);
+    const T lo = from_bits<T>(rf.lo), hi = from_bits<T>(rf.hi);
+    const T n0 = from_bits<T>(rf.ne[0]), n1 = from_bits<T>(rf.ne[1]);
+    const T ac = p.red[0].a.kind == kOpConst ? from_bits<T>(p.red[0].a.bits) : T(0);
+    const T bc = p.red[0].b.kind == kOpConst ? from_bits<T>(p.red[0].b.bits) : T(0);
+    // COUNT of the constants: passing lanes count when ac is nonzero (and not
+    // NaN), the others when bc is
+    const uint32_t cnt_pass = (!t_isnan<T>(ac) && ac != T(0)) ? 1u : 0u;
+    const uint32_t cnt_fail = (!t_isnan<T>(bc) && bc != T(0)) ? 1u : 0u;
+    Acc acc[1];
+    acc[0].u = acc_identity(accop);
+    acc[0].k = {0.0, 0.0};
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t lastj = p.ngroups - 1;
+    for (uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j0 < p.ndata;
+         j0 += stride * kFsUnroll) {
+        T v[kFsUnroll][1][KL];
+#pragma unroll
+        for (int u = 0; u < kFsUnroll; ++u) {
+            const uint64_t j = j0 + u * stride;
+            if (j < p.ndata) load_group<T, 1>(p, j, vec != 0, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kFsUnroll; ++u) {
+            const uint64_t j = j0 + u * stride;
+            if (j >= p.ndata) continue;
+            uint32_t pm = 0;
+            T x[KL];
+#pragma unroll
+            for (int l = 0; l < KL; ++l) {
+                const T y = v[u][0][l];
+                bool pass = y >= lo && y <= hi;
+                if constexpr (NE) pass = pass && y != n0 && y != n1;
+                pm |= pass ? 1u << l : 0u;
+                if constexpr (RK != kRedCount) x[l] = pass ? y : bc;
+            }
+            uint64_t r;
+            if constexpr (RK == kRedCount) {
+                const uint32_t np = __popc(pm);
+                r = cnt_pass * np + cnt_fail * (KL - np);
+            } else {
+                r = reduce_group<T>(RK, x);
+            }
+            acc_fold<T>(acc[0], accop, r);
+            if (j == lastj) out->last[0] = r;
+        }
+    }
+    __shared__ Acc blk[1];
+    block_reduce<T, 1, kThreads>(p, acc, blk);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x].u[0] = blk[0].u;
+        part[blockIdx.x].s[0] = blk[0].k.s;
+        part[blockIdx.x].c[0] = blk[0].k.c;
+    }
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    acc[0].u = acc_identity(accop);
+    acc[0].k = {0.0, 0.0};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        Acc o;
+        o.u = __ldcg(&part[b].u[0]);
+        o.k.s = __ldcg(&part[b].s[0]);
+        o.k.c = __ldcg(&part[b].c[0]);
+        acc_merge<T>(acc[0], accop, o);
+    }
+    block_reduce<T, 1, kThreads>(p, acc, blk);
+    if (threadIdx.x == 0) {
+        *done = 0;
+        finalize_scan<T, 1, 1>(p, blk, out);
+    }
+}
+
+template <typename T>
+int launch_range(const ScanParams& p, const RangeForm& rf, ScanResult* d_out, void* scratch, cudaStream_t s) {
+    ScanPartial* part = static_cast<ScanPartial*>(scratch);
+    unsigned int* done = reinterpret_cast<unsigned int*>(static_cast<char*>(scratch) + kMaxBlocks * sizeof(ScanPartial));
+    const int vec = (reinterpret_cast<uintptr_t>(p.col[0]) + p.off0 * sizeof(T)) % 16 == 0 ? 1 : 0;
+    const int grid = fsum_grid(p.ndata);
+#define VX_RS(RK, NE) range_scan_kernel<T, RK, NE><<<grid, kThreads, 0, s>>>(p, rf, vec, part, done, d_out)
+    switch (rf.fast) {
+    case 1: VX_RS(kRedSum, false); break;
+    case 2: VX_RS(kRedSum, true); break;
+    case 3: VX_RS(kRedCount, false); break;
+    case 4: VX_RS(kRedCount, true); break;
+    case 5: VX_RS(kRedMin, false); break;
+    case 6: VX_RS(kRedMin, true); break;
+    case 7: VX_RS(kRedMax, false); break;
+    default: VX_RS(kRedMax, true); break;
+    }
+#undef VX_RS
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
 template <typename T>
 int launch_fsum(const ScanParams& p, ScanResult* d_out, void* scratch, cudaStream_t s) {
     ScanPartial* part = static_cast<ScanPartial*>(scratch);
@@ -231,6 +341,8 @@ int launch_t(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cu
 template <typename T>
 int dispatch(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
     if (fsum_shape(p)) return launch_fsum<T>(p, d_out, scratch, s);
+    RangeForm rf;
+    if (range_form_of(p, &rf)) return launch_range<T>(p, rf, d_out, scratch, s);
     if (p.ncols <= 1 && p.nred <= 2) return launch_t<T, 1, 2, 4>(p, grid, d_out, scratch, s);
     if (p.ncols <= 1) return launch_t<T, 1, kMaxRed, 2>(p, grid, d_out, scratch, s);
     return launch_t<T, kMaxCols, kMaxRed, 1>(p, grid, d_out, scratch, s);

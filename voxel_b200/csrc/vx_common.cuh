@@ -80,7 +80,9 @@ __device__ __forceinline__ void ksum_add(KSum& k, double x) {
     double t = __dadd_rn(k.s, x);
     double e = fabs(k.s) >= fabs(x) ? __dadd_rn(__dsub_rn(k.s, t), x) : __dadd_rn(__dsub_rn(x, t), k.s);
     k.s = t;
-    k.c = __dadd_rn(k.c, e);
+    // an infinite (or NaN) running sum has no rounding error to carry: its
+    // error term would be inf - inf = NaN and turn an overflowed sum into NaN
+    if (isfinite(t)) k.c = __dadd_rn(k.c, e);
 }
 
 __device__ __forceinline__ KSum ksum_merge(KSum a, KSum b) {
