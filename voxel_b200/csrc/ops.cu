@@ -97,6 +97,51 @@ __global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, u
     }
 }
 
+// Phase 1 for small tables: each block first looks a key up in a shared copy
+// of the slot words taken at its start; only keys missing there (new keys, or
+// keys another block inserted after the copy) take the global CAS path above.
+__global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const uint32_t* __restrict__ keys,
+                                                               uint64_t n, unsigned long long* groups, uint64_t limit,
+                                                               int* overflow) {
+    extern __shared__ __align__(16) unsigned long long i_slot[];
+    const uint32_t cap = static_cast<uint32_t>(t.mask + 1), mask = cap - 1;
+    for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) i_slot[i] = __ldcg(t.slot + i);
+    __syncthreads();
+    unsigned int added = 0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t k = __ldcs(keys + i);
+        const unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
+        uint32_t h = hash32(k) & mask;
+        uint32_t probes = 0;
+        unsigned long long cur;
+        while ((cur = i_slot[h]) != want && cur != 0 && probes++ < mask) h = (h + 1) & mask;
+        if (cur == want) continue;
+        uint64_t g = hash32(k) & t.mask;
+        for (uint64_t p = 0;; ++p) {
+            const unsigned long long c = __ldcg(t.slot + g);
+            if (c == want) break;
+            if (c == 0) {
+                const unsigned long long old = atomicCAS(&t.slot[g], 0ull, want);
+                if (old == 0) {
+                    ++added;
+                    break;
+                }
+                if (old == want) break;
+            }
+            g = (g + 1) & t.mask;
+            if (p > t.mask) {
+                atomicOr(overflow, 1);
+                break;
+            }
+        }
+    }
+    if (added) {
+        const unsigned long long gsum = atomicAdd(groups, static_cast<unsigned long long>(added)) + added;
+        if (gsum > limit) atomicOr(overflow, 1);
+    }
+}
+
 __device__ __forceinline__ uint64_t find_slot(const Table& t, uint32_t k) {
     unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
     uint64_t h = hash32(k) & t.mask;
@@ -191,11 +236,13 @@ __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uin
                                                               const double* __restrict__ vals, uint64_t n, int* err) {
     extern __shared__ __align__(16) unsigned long long a_sm[];
     const uint32_t cap = static_cast<uint32_t>(t.mask + 1);
-    unsigned long long* s_mn = a_sm;
+    unsigned long long* s_slot = a_sm;  // the table's slot words (read at L2: written by the insert kernel)
+    unsigned long long* s_mn = s_slot + cap;
     unsigned long long* s_mx = s_mn + cap;
     uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + cap);
     uint32_t* s_cnt = s_w + kAccWords * cap;
     for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) {
+        s_slot[i] = __ldcg(t.slot + i);
 #pragma unroll
         for (int k = 0; k < kAccWords; ++k) s_w[kAccWords * i + k] = 0;
         s_cnt[i] = 0;
@@ -203,11 +250,18 @@ __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uin
         s_mx[i] = 0;
     }
     __syncthreads();
+    const uint32_t mask = cap - 1;
     bool bad = false;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t sl = find_slot(t, __ldcs(keys + i));
-        if (sl == ~0ull) {
+        // the key's slot: linear probing in the shared copy
+        const uint32_t key = __ldcs(keys + i);
+        const unsigned long long want = (static_cast<unsigned long long>(key) << 32) | 1ull;
+        uint32_t sl = hash32(key) & mask;
+        uint32_t probes = 0;
+        unsigned long long cur;
+        while ((cur = s_slot[sl]) != want && cur != 0 && probes++ < mask) sl = (sl + 1) & mask;
+        if (cur != want) {
             bad = true;
             continue;
         }
@@ -235,7 +289,7 @@ __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uin
     }
 }
 
-size_t smem_table_bytes(uint64_t cap) { return cap * (2 * 8 + kAccWords * 4 + 4); }
+size_t smem_table_bytes(uint64_t cap) { return cap * (3 * 8 + kAccWords * 4 + 4); }
 
 // move every occupied slot of `from` into `to` (a grow)
 __global__ void rehash_kernel(Table from, Table to) {
@@ -577,8 +631,16 @@ public:
         for (int attempt = 0; attempt < 40; ++attempt) {
             VX_CUDA(cudaMemsetAsync(flag_d.p, 0, 4, s));
             uint64_t limit = cap * 3 / 4;
-            insert_keys_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, n, groups_d.as<unsigned long long>(), limit,
-                                                              flag_d.as<int>());
+            if (cap <= kSmemSlots) {
+                const int sms = sm_count() > 0 ? sm_count() : 148;
+                uint64_t blocks = (n + 511) / 512;
+                if (blocks > static_cast<uint64_t>(sms) * 4) blocks = static_cast<uint64_t>(sms) * 4;
+                insert_keys_smem_kernel<<<static_cast<unsigned>(blocks), 512, cap * 8, s>>>(
+                    t, dk, n, groups_d.as<unsigned long long>(), limit, flag_d.as<int>());
+            } else {
+                insert_keys_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, n, groups_d.as<unsigned long long>(), limit,
+                                                                  flag_d.as<int>());
+            }
             VX_CUDA(cudaGetLastError());
             int ovf = 0;
             uint64_t g = 0;
