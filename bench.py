@@ -561,12 +561,15 @@ def workload_batch(args, L, rank, world, local, dist, dev):
         raise RuntimeError("batch fetch failed")
     launch_ms = _max_over_ranks(dist, dev, statistics.mean(launch_ev))
     written = int(sum(min(r.count, c) for r, c in zip(res, lb.caps)))
-    # kernels per step: the output clear + one per non-empty program class,
-    # and the same for the exact re-run of overflowed programs
+    # kernels per step: the output clear + one per non-empty program class, one
+    # gather of the spilled rows when a program overflowed, and the clear +
+    # class kernels of an exact re-run when the spill arena was full
     forms = [L.voxel_batch_form(lb.b, i) for i in range(len(progs))]
     cls_of = [(p_.dtype, f) for p_, f in zip(progs, forms)]
-    redo = [i for i, r in enumerate(res) if r.overflowed]
-    launches_per_step = 1 + len(set(cls_of)) + ((1 + len({cls_of[i] for i in redo})) if redo else 0)
+    lt = lb.last_timing
+    launches_per_step = 1 + len(set(cls_of)) + (1 if lt["overflowed"] > lt["reruns"] else 0)
+    if lt["reruns"]:
+        launches_per_step += 1 + len(set(cls_of))  # an upper bound on the re-run's classes
     plain, p_ev, p_wall = timed(lambda: B.plain_two_pass(progs, cols, stream))
     p_wall = _max_over_ranks(dist, dev, p_wall)
     # the batch must reproduce the plain kernels exactly

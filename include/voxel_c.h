@@ -373,7 +373,10 @@ int       voxel_batch_add(void* batch, int dtype, const uint32_t* code, size_t l
 int       voxel_batch_set_capacity(void* batch, size_t prog, size_t capacity, uint32_t* d_sel);
 int       voxel_batch_launch(void* batch, int use_graph, void* stream);
 int       voxel_batch_fetch(void* batch, void* stream);
-/* after fetch: the program's 64 registers, exact selected-row count, overflow flag */
+/* after fetch: the program's 64 registers, exact selected-row count, overflow
+ * flag (0: the selection fit; 1: rows past the capacity went to the spill
+ * arena, voxel_batch_gather_overflow assembles them; 2: some did not fit the
+ * arena either, re-run the program) */
 int       voxel_batch_result(const void* batch, size_t prog, uint64_t* regs64, uint64_t* sel_count,
                              int* overflow);
 /* after fetch: every program at once (regs64: 64 per program; any pointer may be NULL) */
@@ -383,6 +386,15 @@ int       voxel_batch_results_all(const void* batch, uint64_t* regs64, uint64_t*
  * 1 + 2 * reduction kind SUM/COUNT/MIN/MAX + excluded values present);
  * -1 for an invalid index */
 int       voxel_batch_form(const void* batch, size_t prog);
+/* rows past a program's selection capacity go to a spill arena of `rows`
+ * entries (default 2^24); takes effect at the next launch */
+int       voxel_batch_set_spill_capacity(void* batch, size_t rows);
+/* after fetch: the whole selection of each overflowed program progs[k] (its
+ * exact count of rows) into d_pool at offset count[progs[0]] + ... +
+ * count[progs[k-1]], from its buffer and its spilled rows; VOXEL_ECAPACITY if
+ * a listed program's rows did not all fit the spill arena (re-run those) */
+int       voxel_batch_gather_overflow(void* batch, size_t n, const size_t* progs, uint32_t* d_pool,
+                                      void* stream);
 /* after fetch: re-run programs progs[0..n) (e.g. those that overflowed) with
  * selection capacities capacities[k], writing program k's row ids at
  * d_pool + capacities[0] + ... + capacities[k-1]; one launch from the

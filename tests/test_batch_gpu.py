@@ -117,6 +117,11 @@ def test_batch_overflow_is_flagged_with_exact_count():
     assert ovf == 1 and cnt == want and regs[0] == want
     sel = keep[1][: want // 3].cpu().numpy().astype(np.int64)
     assert (sel == np.flatnonzero(col < 500)[: want // 3]).all()
+    # the rows past the buffer are in the spill arena: the exact selection
+    pool = torch.zeros(want, dtype=torch.int32, device=torch.device("cuda", 0))
+    progs = np.zeros(1, np.uint64)
+    assert L.voxel_batch_gather_overflow(b, 1, progs.ctypes.data, pool.data_ptr(), None) == 0, capi.last_error()
+    assert (pool.cpu().numpy().astype(np.int64) == np.flatnonzero(col < 500)).all()
     L.voxel_batch_destroy(b)
 
 
@@ -224,12 +229,14 @@ def test_batch_range_form_edge_cases():
     L.voxel_batch_destroy(b)
 
 
-@pytest.mark.parametrize("margin,slack", [(4.0, 1024), (0.0, 0)])
-def test_learned_batch_run_matches_plain_two_pass(margin, slack):
-    """LearnedBatch.run (graph launch, bulk results, exact re-run of programs
-    whose estimated buffer was too small) equals one exact two-pass launch per
-    program: registers, counts and selection vectors.  With no margin every
-    program with a selected row is re-run."""
+@pytest.mark.parametrize("margin,slack,spill", [(4.0, 1024, None), (0.0, 0, None), (0.0, 0, 1000)])
+def test_learned_batch_run_matches_plain_two_pass(margin, slack, spill):
+    """LearnedBatch.run (graph launch, bulk results; a program whose estimated
+    buffer was too small gets its rows past the buffer from the spill arena,
+    or is re-run exactly when the arena is full) equals one exact two-pass
+    launch per program: registers, counts and selection vectors.  With no
+    margin every program with a selected row overflows; with a 1000-row arena
+    most of those are re-run."""
     from voxel_b200 import batch as B
 
     rng = np.random.default_rng(45)
@@ -241,7 +248,7 @@ def test_learned_batch_run_matches_plain_two_pass(margin, slack):
         progs.append(T.random_program(dt, rng))
         cols.append(torch.from_numpy(T.make_column(dt, n, rng)).to(dev))
     stream = torch.cuda.Stream(dev)
-    lb = B.LearnedBatch(None, margin=margin, slack=slack)
+    lb = B.LearnedBatch(None, margin=margin, slack=slack, spill_rows=spill)
     for p, c in zip(progs, cols):
         lb.add(p, c)
     lb.prepare(stream)
@@ -250,7 +257,11 @@ def test_learned_batch_run_matches_plain_two_pass(margin, slack):
         res = lb.run()
         assert len(res) == len(progs)
         if margin == 0.0:
-            assert lb.last_timing["reruns"] == sum(r.count > 0 for r in plain)
+            assert lb.last_timing["overflowed"] == sum(r.count > 0 for r in plain)
+            if spill is None:
+                assert lb.last_timing["reruns"] == 0
+            else:
+                assert lb.last_timing["reruns"] > 0
         for a, b in zip(res, plain):
             assert np.array_equal(np.asarray(a.registers, np.uint64), np.asarray(b.registers, np.uint64))
             assert a.count == b.count and torch.equal(a.selection, b.selection)

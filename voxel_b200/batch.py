@@ -102,6 +102,7 @@ class LearnedBatch:
     model: "E.Model | None"
     margin: float = 4.0
     slack: int = 1024
+    spill_rows: int | None = None  # spill arena rows (None: the library default)
     programs: list = field(default_factory=list)
     columns: list = field(default_factory=list)  # (dtype, device tensor) per program
     sketches: dict = field(default_factory=dict)
@@ -142,6 +143,8 @@ class LearnedBatch:
         self.pool = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=dev)
         self.offs = offs
         self.b = L.voxel_batch_create()
+        if self.spill_rows is not None:
+            L.voxel_batch_set_spill_capacity(self.b, int(self.spill_rows))
         base = self.pool.data_ptr()
         for i, (prog, dcol) in enumerate(zip(self.programs, self.columns)):
             _batch_add(L, self.b, prog, dcol, dcol.numel(), 1, caps[i], base + 4 * int(offs[i]))
@@ -150,9 +153,10 @@ class LearnedBatch:
 
     # -- execution ------------------------------------------------------------
     def run(self):
-        """One graph launch of every program; programs whose selection did not
-        fit are re-run once with exactly sized buffers.  Returns a
-        BatchResults (a sequence of ProgramResult)."""
+        """One graph launch of every program.  A program whose selection outgrew
+        its buffer has the rest in the batch's spill arena and gets an exactly
+        sized buffer assembled on the device; only if the arena was full is it
+        re-run exactly.  Returns a BatchResults (a sequence of ProgramResult)."""
         import torch  # noqa: PLC0415
 
         import time  # noqa: PLC0415
@@ -172,26 +176,40 @@ class LearnedBatch:
         redo = np.flatnonzero(ovfs)
         t2 = time.perf_counter()
         extra = {}
-        if redo.size:  # exact write pass for the programs whose estimate was low
-            sizes = cnts[redo]
-            offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-            pool2 = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=self.pool.device)
-            idx = redo.astype(np.uint64)
-            caps = sizes.astype(np.uint64)
-            if L.voxel_batch_rerun(self.b, redo.size, idx.ctypes.data, caps.ctypes.data, pool2.data_ptr(), sh):
-                raise RuntimeError(capi.last_error())
-            regs2 = np.zeros((n, 64), np.uint64)
-            cnt2 = np.zeros(n, np.uint64)
-            ovf2 = np.zeros(n, np.int32)
-            if L.voxel_batch_results_all(self.b, regs2.ctypes.data, cnt2.ctypes.data, ovf2.ctypes.data):
-                raise RuntimeError(capi.last_error())
-            if ovf2[redo].any() or (cnt2[redo] != sizes).any() or (regs2[redo] != regs[redo]).any():
-                raise RuntimeError("exact re-run disagrees with the batch")
-            for k, i in enumerate(redo.tolist()):
-                extra[i] = pool2[int(offs[k]):int(offs[k + 1])]
+        if redo.size:
+            # programs whose rows past the estimate-sized buffer all went to the
+            # spill arena: assemble buffer + spilled fragments into exact
+            # buffers; the rest (arena full) are re-run exactly
+            gather = redo[ovfs[redo] == 1]
+            rerun = redo[ovfs[redo] != 1]
+            for ids, how in ((gather, "gather"), (rerun, "rerun")):
+                if not ids.size:
+                    continue
+                sizes = cnts[ids]
+                offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+                pool2 = torch.empty(int(offs[-1]) + 1, dtype=torch.int32, device=self.pool.device)
+                idx = ids.astype(np.uint64)
+                if how == "gather":
+                    st = L.voxel_batch_gather_overflow(self.b, ids.size, idx.ctypes.data, pool2.data_ptr(), sh)
+                else:
+                    caps = sizes.astype(np.uint64)
+                    st = L.voxel_batch_rerun(self.b, ids.size, idx.ctypes.data, caps.ctypes.data, pool2.data_ptr(), sh)
+                if st:
+                    raise RuntimeError(capi.last_error())
+                if how == "rerun":
+                    regs2 = np.zeros((n, 64), np.uint64)
+                    cnt2 = np.zeros(n, np.uint64)
+                    ovf2 = np.zeros(n, np.int32)
+                    if L.voxel_batch_results_all(self.b, regs2.ctypes.data, cnt2.ctypes.data, ovf2.ctypes.data):
+                        raise RuntimeError(capi.last_error())
+                    if ovf2[ids].any() or (cnt2[ids] != sizes).any() or (regs2[ids] != regs[ids]).any():
+                        raise RuntimeError("exact re-run disagrees with the batch")
+                for k, i in enumerate(ids.tolist()):
+                    extra[i] = pool2[int(offs[k]):int(offs[k + 1])]
         out = BatchResults(regs, cnts, self.est, ovfs, self.pool, self.offs, extra)
         self.last_timing = {"launch_fetch_ms": (t1 - t0) * 1e3, "results_ms": (t2 - t1) * 1e3,
-                            "rerun_ms": (time.perf_counter() - t2) * 1e3, "reruns": int(redo.size)}
+                            "overflow_ms": (time.perf_counter() - t2) * 1e3, "overflowed": int(redo.size),
+                            "reruns": int((ovfs[redo] != 1).sum()) if redo.size else 0}
         return out
 
     def close(self):

@@ -159,6 +159,8 @@ _SIGS = {
     "voxel_batch_results_all": (C.c_int, [vp, vp, vp, vp]),
     "voxel_batch_form": (C.c_int, [vp, sz]),
     "voxel_batch_rerun": (C.c_int, [vp, sz, vp, vp, vp, vp]),
+    "voxel_batch_gather_overflow": (C.c_int, [vp, sz, vp, vp, vp]),
+    "voxel_batch_set_spill_capacity": (C.c_int, [vp, sz]),
     "voxel_server_create": (vp, [sz, u32]),
     "voxel_server_destroy": (None, [vp]),
     "voxel_server_submit_program": (u64, [vp, C.c_int, vp, sz, vp, vp, sz, C.c_int, sz, vp]),

@@ -51,6 +51,8 @@ struct ItemShared {
     Acc wacc[kBThreads / 32][kBNR];  // per-warp reduction partials
     uint32_t stage[kBThreads / 32][32 * 8 * kBU];  // one warp's row ids of one pass (8 lanes per group at most)
     uint64_t item_base;
+    uint64_t spill_a0, spill_p0;  // this item's arena range starts at output position p0 (rows past capacity)
+    int spill_ok;
 };
 
 struct ItemPartial {
@@ -122,7 +124,7 @@ __device__ __forceinline__ void prefetch_item(const ScanParams& p, uint64_t g0) 
 template <typename T, int NR>
 __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, Acc (&acc)[NR], ItemPartial* part_item,
                                               BatchOut* out, unsigned long long* status_prog, int* err,
-                                              ItemShared& sh) {
+                                              ItemShared& sh, const SpillArgs& sp, uint32_t pid) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
     uint32_t (*s_mask)[kBThreads] = sh.mask;
@@ -201,6 +203,23 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
         if (lane == 0) {
             sh.item_base = e;
             if (t == bp.nitems - 1) out->sel_count = e + total_item;
+            // rows past the capacity: one arena range for the item, recorded as a fragment
+            uint64_t a0 = 0, p0 = 0;
+            int ok = 1;
+            if (bp.sel_mask && bp.want_sel && e + total_item > bp.sel_cap) {
+                p0 = e > bp.sel_cap ? e : bp.sel_cap;
+                const uint64_t nov = e + total_item - p0;
+                a0 = atomicAdd(sp.cursor, static_cast<unsigned long long>(nov));
+                if (a0 + nov <= sp.cap) {
+                    const unsigned int f = atomicAdd(sp.nfrags, 1u);  // < items: one per item at most
+                    sp.frags[f] = SpillFrag{pid, static_cast<uint32_t>(nov), p0, a0};
+                } else {
+                    ok = 0;
+                }
+            }
+            sh.spill_a0 = a0;
+            sh.spill_p0 = p0;
+            sh.spill_ok = ok;
         }
     }
     __syncthreads();
@@ -239,14 +258,19 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
         if (gpos + wtot <= sel_cap) {
             for (uint32_t i = lane; i < wtot; i += 32) sel_out[gpos + i] = stage[i];
         } else {
+            ovf = true;
             for (uint32_t i = lane; i < wtot; i += 32) {
-                if (gpos + i < sel_cap) sel_out[gpos + i] = stage[i];
-                else ovf = true;
+                const uint64_t pos = gpos + i;
+                if (pos < sel_cap) sel_out[pos] = stage[i];
+                else if (sh.spill_ok) sp.rows[sh.spill_a0 + (pos - sh.spill_p0)] = stage[i];
             }
         }
         __syncwarp();
     }
-    if (ovf) out->overflow = 1;
+    if (ovf && lane == 0) {
+        out->overflow = 1;
+        if (!sh.spill_ok) out->spill_lost = 1;
+    }
 }
 
 // Range form (BatchProg::fast != 0): one column, one reduction whose predicate
@@ -256,7 +280,8 @@ __device__ __forceinline__ void item_epilogue(const BatchProg& bp, uint64_t t, A
 // order, and NaN fails every interval test as it fails every ordered atom.
 template <typename T, int RK, bool NE>
 __device__ __forceinline__ void process_range(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
-                                           unsigned long long* status_prog, int* err, ItemShared& sh) {
+                                           unsigned long long* status_prog, int* err, ItemShared& sh,
+                                           const SpillArgs& sp, uint32_t pid) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
     constexpr uint8_t accop = range_acc(RK, Traits<T>::kFloat);
@@ -339,7 +364,7 @@ __device__ __forceinline__ void process_range(const BatchProg& bp, uint64_t t, I
         sh.mask[w][threadIdx.x] = mask;
     }
     if (has_last) out->res.last[0] = last_res;
-    item_epilogue<T, 1>(bp, t, acc, part_item, out, status_prog, err, sh);
+    item_epilogue<T, 1>(bp, t, acc, part_item, out, status_prog, err, sh, sp, pid);
 }
 
 // NA = 0: the generic evaluator (scan_core.cuh) for any program shape;
@@ -347,7 +372,8 @@ __device__ __forceinline__ void process_range(const BatchProg& bp, uint64_t t, I
 // program's fields held in registers for the whole item.
 template <typename T, int NR, int NA>
 __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, ItemPartial* part_item, BatchOut* out,
-                                          unsigned long long* status_prog, int* err, ItemShared& sh) {
+                                          unsigned long long* status_prog, int* err, ItemShared& sh,
+                                          const SpillArgs& sp, uint32_t pid) {
     constexpr int KL = 32 / sizeof(T);
     const ScanParams& p = bp.p;
     uint32_t (*s_mask)[kBThreads] = sh.mask;
@@ -451,7 +477,7 @@ __device__ __forceinline__ void process_item(const BatchProg& bp, uint64_t t, It
         }
         s_mask[w][threadIdx.x] = mask;
     }
-    item_epilogue<T, NR>(bp, t, acc, part_item, out, status_prog, err, sh);
+    item_epilogue<T, NR>(bp, t, acc, part_item, out, status_prog, err, sh, sp, pid);
 }
 
 template <typename T, int NR>
@@ -490,7 +516,7 @@ __global__ void __launch_bounds__(kBThreads, FAST ? kRangeBlocks : 2) batch_kern
                                                           const uint64_t* __restrict__ cstart, uint64_t citems,
                                                           ItemPartial* parts, unsigned long long* status,
                                                           unsigned int* pdone, unsigned int* item_ctr,
-                                                          BatchOut* outs, int* err) {
+                                                          BatchOut* outs, int* err, const SpillArgs sp) {
     __shared__ uint64_t s_item, s_kbeg, s_kend;
     __shared__ uint32_t s_k;
     __shared__ __align__(16) BatchProg s_bp;
@@ -539,17 +565,17 @@ __global__ void __launch_bounds__(kBThreads, FAST ? kRangeBlocks : 2) batch_kern
         const uint64_t it = s_bp.item0 + t;  // global item index
         if constexpr (FAST) {
             process_range<T, (FAST - 1) / 2, ((FAST - 1) & 1) != 0>(s_bp, t, parts + it, outs + pid,
-                                                                   status + s_bp.item0, err, sh);
+                                                                   status + s_bp.item0, err, sh, sp, pid);
         } else if constexpr (NR == 1) {
             switch (s_bp.p.ncols == 1 ? s_bp.p.natoms : 0) {
-            case 1: process_item<T, 1, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-            case 2: process_item<T, 1, 2>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-            case 3: process_item<T, 1, 3>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-            case 4: process_item<T, 1, 4>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
-            default: process_item<T, 1, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh); break;
+            case 1: process_item<T, 1, 1>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid); break;
+            case 2: process_item<T, 1, 2>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid); break;
+            case 3: process_item<T, 1, 3>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid); break;
+            case 4: process_item<T, 1, 4>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid); break;
+            default: process_item<T, 1, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid); break;
             }
         } else {
-            process_item<T, NR, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh);
+            process_item<T, NR, 0>(s_bp, t, parts + it, outs + pid, status + s_bp.item0, err, sh, sp, pid);
         }
         // the item's partial and row ids are written: count it done, and take
         // the next item in the same step
@@ -583,7 +609,7 @@ int class_of(const BatchProg& bp) {
 template <typename T, int NR, int FAST>
 int launch_class_t(const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
                    uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
-                   unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
+                   unsigned int* ctr, BatchOut* outs, int* err, const SpillArgs& sp, cudaStream_t s) {
     static int per_sm = 0;
     if (!per_sm) {
         VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, NR, FAST>, kBThreads, 0));
@@ -592,7 +618,7 @@ int launch_class_t(const BatchProg* progs, const uint32_t* pids, uint32_t npc, c
     uint64_t grid = static_cast<uint64_t>(sm_count() > 0 ? sm_count() : 148) * per_sm;
     if (grid > citems) grid = citems;
     batch_kernel<T, NR, FAST><<<static_cast<unsigned>(grid), kBThreads, 0, s>>>(progs, pids, npc, cstart, citems,
-                                                                              parts, status, pdone, ctr, outs, err);
+                                                                              parts, status, pdone, ctr, outs, err, sp);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -600,8 +626,8 @@ int launch_class_t(const BatchProg* progs, const uint32_t* pids, uint32_t npc, c
 template <typename T>
 int launch_kind(int kind, const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
                 uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
-                unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
-#define VX_K(NR, F) launch_class_t<T, NR, F>(progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
+                unsigned int* ctr, BatchOut* outs, int* err, const SpillArgs& sp, cudaStream_t s) {
+#define VX_K(NR, F) launch_class_t<T, NR, F>(progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, sp, s)
     switch (kind) {
     case 0: return VX_K(1, 1);
     case 1: return VX_K(1, 2);
@@ -619,8 +645,9 @@ int launch_kind(int kind, const BatchProg* progs, const uint32_t* pids, uint32_t
 
 int launch_class(int cls, const BatchProg* progs, const uint32_t* pids, uint32_t npc, const uint64_t* cstart,
                  uint64_t citems, ItemPartial* parts, unsigned long long* status, unsigned int* pdone,
-                 unsigned int* ctr, BatchOut* outs, int* err, cudaStream_t s) {
-#define VX_KIND(TT) launch_kind<TT>(cls % kKinds, progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, s)
+                 unsigned int* ctr, BatchOut* outs, int* err, const SpillArgs& sp, cudaStream_t s) {
+#define VX_KIND(TT) \
+    launch_kind<TT>(cls % kKinds, progs, pids, npc, cstart, citems, parts, status, pdone, ctr, outs, err, sp, s)
     switch (cls / kKinds) {
     case F64: return VX_KIND(double);
     case F32: return VX_KIND(float);
@@ -644,9 +671,37 @@ bool set_range_form(BatchProg& bp) {
     return true;
 }
 
+// Exact selections of overflowed programs: blocks [0, nlist) copy program k's
+// rows that fit its buffer to d_pool + off[k]; the other blocks copy the
+// spilled fragments of listed programs (offmap[pid] = its pool offset, or ~0).
+struct GatherItem {
+    const uint32_t* sel;
+    uint64_t cap;  // rows in the buffer (min of capacity and count)
+    uint64_t off;
+};
+
+__global__ void gather_overflow_kernel(const GatherItem* __restrict__ list, uint32_t nlist,
+                                       const uint64_t* __restrict__ offmap, const SpillFrag* __restrict__ frags,
+                                       const unsigned int* nfrags, const uint32_t* __restrict__ spill,
+                                       uint32_t* __restrict__ pool) {
+    if (blockIdx.x < nlist) {
+        const GatherItem g = list[blockIdx.x];
+        for (uint64_t r = threadIdx.x; r < g.cap; r += blockDim.x) pool[g.off + r] = __ldg(g.sel + r);
+        return;
+    }
+    const unsigned int nf = *nfrags;
+    for (unsigned int f = blockIdx.x - nlist; f < nf; f += gridDim.x - nlist) {
+        const SpillFrag fr = frags[f];
+        const uint64_t off = offmap[fr.pid];
+        if (off == ~0ull) continue;
+        for (uint32_t r = threadIdx.x; r < fr.n; r += blockDim.x) pool[off + fr.dst + r] = __ldg(spill + fr.src + r);
+    }
+}
+
 __global__ void clear_outs_kernel(BatchOut* outs, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         outs[i].overflow = 0;
+        outs[i].spill_lost = 0;
         outs[i].sel_count = 0;
     }
 }
@@ -748,8 +803,11 @@ int Batch::upload(cudaStream_t s) {
         d_err_ = DevBuf(16);
         if (d_err_.p) VX_CUDA(cudaMemsetAsync(d_err_.p, 0, 16, s));
     }
+    if (d_spill_.n < spill_cap_ * 4 + 16) d_spill_ = DevBuf(spill_cap_ * 4 + 16);
+    if (d_frags_.n < items * sizeof(SpillFrag) + 16) d_frags_ = DevBuf(items * sizeof(SpillFrag) + 16);
+    if (!d_spill_ctr_.p) d_spill_ctr_ = DevBuf(16);
     if (!d_progs_.p || !d_start_.p || !d_pids_.p || !d_outs_.p || !d_parts_.p || !d_status_.p || !d_pdone_.p ||
-        !d_err_.p)
+        !d_err_.p || !d_spill_.p || !d_frags_.p || !d_spill_ctr_.p)
         return kErrOutOfMemory;
     if (int st = h2d(d_progs_.p, host_.data(), np * sizeof(BatchProg), s)) return st;
     if (int st = h2d(d_start_.p, cstart.data(), cstart.size() * 8, s)) return st;
@@ -772,6 +830,9 @@ int Batch::enqueue(cudaStream_t s, bool branches) {
     VX_CUDA(cudaMemsetAsync(d_status_.p, 0, nitems_ * 8 + 8 * kClasses, s));
     clear_outs_kernel<<<(np + 255) / 256, 256, 0, s>>>(d_outs_.as<BatchOut>(), np);
     VX_CUDA(cudaGetLastError());
+    VX_CUDA(cudaMemsetAsync(d_spill_ctr_.p, 0, 16, s));
+    const SpillArgs sp{d_spill_.as<uint32_t>(), d_spill_.n / 4, d_spill_ctr_.as<unsigned long long>(),
+                       d_frags_.as<SpillFrag>(), reinterpret_cast<unsigned int*>(d_spill_ctr_.as<unsigned long long>() + 1)};
     // The class kernels are independent: when recording, spread them over
     // parallel branches (largest class first, each to the least-loaded
     // branch), so one kernel's tail overlaps the next one's start.
@@ -796,7 +857,7 @@ int Batch::enqueue(cudaStream_t s, bool branches) {
         st = launch_class(c, d_progs_.as<BatchProg>(), d_pids_.as<uint32_t>() + cls_[c].pid_off, cls_[c].np,
                           d_start_.as<uint64_t>() + cls_[c].cs_off, cls_[c].items, d_parts_.as<ItemPartial>(),
                           d_status_.as<unsigned long long>(), d_pdone_.as<unsigned int>(), ctr + c,
-                          d_outs_.as<BatchOut>(), d_err_.as<int>(), branches ? branch_[b] : s);
+                          d_outs_.as<BatchOut>(), d_err_.as<int>(), sp, branches ? branch_[b] : s);
         if (st) break;
     }
     if (branches) {  // join every branch, also after a failed launch, so the recording can end
@@ -852,13 +913,57 @@ int Batch::fetch(cudaStream_t s) {
     return kOk;
 }
 
+int Batch::gather_overflow(size_t n, const size_t* idx, uint32_t* d_pool, cudaStream_t s) {
+    if (outs_.size() != host_.size()) {
+        set_error(kErrInvalidArg, "batch gather before fetch");
+        return kErrInvalidArg;
+    }
+    if (!n) return kOk;
+    const size_t np = host_.size();
+    std::vector<uint64_t> offmap(np, ~0ull);
+    std::vector<GatherItem> list(n);
+    uint64_t off = 0;
+    bool lost = false;
+    for (size_t k = 0; k < n; ++k) {
+        if (idx[k] >= np) {
+            set_error(kErrInvalidArg, "batch gather: program %zu out of range", idx[k]);
+            return kErrInvalidArg;
+        }
+        const BatchOut& o = outs_[idx[k]];
+        if (o.spill_lost) lost = true;
+        const uint64_t cnt = o.sel_count;
+        list[k] = GatherItem{host_[idx[k]].sel_out, cnt < host_[idx[k]].sel_cap ? cnt : host_[idx[k]].sel_cap, off};
+        offmap[idx[k]] = off;
+        off += cnt;
+    }
+    if (lost) {
+        set_error(kErrCapacity, "batch gather: a listed program's overflow did not fit the spill arena; re-run it");
+        return kErrCapacity;
+    }
+    if (d_offmap_.n < np * 8) d_offmap_ = DevBuf(np * 8 + 8);
+    if (d_glist_.n < n * sizeof(GatherItem)) d_glist_ = DevBuf(n * sizeof(GatherItem) + 16);
+    if (!d_offmap_.p || !d_glist_.p) return kErrOutOfMemory;
+    if (int st = h2d(d_offmap_.p, offmap.data(), np * 8, s)) return st;
+    if (int st = h2d(d_glist_.p, list.data(), n * sizeof(GatherItem), s)) return st;
+    const unsigned grid = static_cast<unsigned>(n) + 4u * static_cast<unsigned>(sm_count() > 0 ? sm_count() : 148);
+    gather_overflow_kernel<<<grid, 256, 0, s>>>(d_glist_.as<GatherItem>(), static_cast<uint32_t>(n),
+                                               d_offmap_.as<uint64_t>(), d_frags_.as<SpillFrag>(),
+                                               reinterpret_cast<unsigned int*>(d_spill_ctr_.as<unsigned long long>() + 1),
+                                               d_spill_.as<uint32_t>(), d_pool);
+    VX_CUDA(cudaGetLastError());
+    return sync(s);
+}
+
 int Batch::rerun(size_t n, const size_t* idx, const size_t* caps, uint32_t* d_pool, cudaStream_t s) {
     if (outs_.size() != host_.size()) {
         set_error(kErrInvalidArg, "batch re-run before fetch");
         return kErrInvalidArg;
     }
     if (!n) return kOk;
-    if (!sub_) sub_.reset(new Batch());
+    if (!sub_) {
+        sub_.reset(new Batch());
+        sub_->spill_cap_ = 1024;  // exact capacities: nothing spills
+    }
     Batch& b = *sub_;
     b.host_.clear();
     b.writes_.clear();
@@ -938,8 +1043,18 @@ int voxel_batch_results_all(const void* b, uint64_t* regs64, uint64_t* sel_count
     for (size_t i = 0; i < B->size(); ++i) {
         if (regs64) B->registers(i, regs64 + 64 * i);
         if (sel_counts) sel_counts[i] = B->out(i).sel_count;
-        if (overflows) overflows[i] = B->out(i).overflow;
+        if (overflows) overflows[i] = B->out(i).overflow + B->out(i).spill_lost;
     }
+    return kOk;
+}
+
+int voxel_batch_gather_overflow(void* b, size_t n, const size_t* progs, uint32_t* d_pool, void* stream) {
+    clear_error();
+    return static_cast<Batch*>(b)->gather_overflow(n, progs, d_pool, static_cast<cudaStream_t>(stream));
+}
+
+int voxel_batch_set_spill_capacity(void* b, size_t rows) {
+    static_cast<Batch*>(b)->set_spill_capacity(rows);
     return kOk;
 }
 
@@ -960,7 +1075,7 @@ int voxel_batch_result(const void* b, size_t prog, uint64_t* regs64, uint64_t* s
     if (prog >= B->size() || prog >= B->fetched()) return kErrInvalidArg;
     if (regs64) B->registers(prog, regs64);
     if (sel_count) *sel_count = B->out(prog).sel_count;
-    if (overflow) *overflow = B->out(prog).overflow;
+    if (overflow) *overflow = B->out(prog).overflow + B->out(prog).spill_lost;
     return kOk;
 }
 

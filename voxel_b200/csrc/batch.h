@@ -33,8 +33,25 @@ struct __align__(16) BatchProg {
 struct BatchOut {
     ScanResult res;
     unsigned long long sel_count;  // exact count of selected rows
-    int overflow;                  // the selection did not fit sel_cap
-    int pad;
+    int overflow;                  // the selection did not fit sel_cap (rows past it went to the spill arena)
+    int spill_lost;                // ... and some of them did not fit the spill arena either
+};
+
+// Rows past a program's capacity: each item claims one contiguous range of the
+// spill arena and records it as a fragment (at most one per item).
+struct SpillFrag {
+    uint32_t pid;       // program
+    uint32_t n;         // rows
+    uint64_t dst;       // output position of the fragment's first row
+    uint64_t src;       // arena offset
+};
+
+struct SpillArgs {
+    uint32_t* rows;                // the arena
+    uint64_t cap;                  // arena capacity in rows
+    unsigned long long* cursor;    // rows claimed
+    SpillFrag* frags;
+    unsigned int* nfrags;
 };
 
 class Batch {
@@ -53,6 +70,15 @@ public:
     const BatchOut& out(size_t i) const { return outs_[i]; }
     const BatchProg& prog(size_t i) const { return host_[i]; }
     void registers(size_t i, uint64_t* regs) const;
+    // After fetch: program idx[k]'s whole selection (its count rows) into d_pool
+    // at caps... offsets (the counts of idx[0..k)), assembled from its buffer
+    // and its spilled fragments; kErrCapacity if a listed program lost rows
+    // (its spill did not fit the arena), which then needs rerun().
+    int gather_overflow(size_t n, const size_t* idx, uint32_t* d_pool, cudaStream_t s);
+    void set_spill_capacity(uint64_t rows) {
+        spill_cap_ = rows;
+        dirty_ = true;
+    }
     // After fetch: re-runs programs idx[0..n) with selection capacities caps[k]
     // into d_pool (program k's rows at d_pool + caps[0] + ... + caps[k-1]),
     // from their already-lowered descriptors, one launch, and takes their
@@ -69,6 +95,8 @@ private:
     std::vector<std::vector<uint64_t>> regs_;
     std::vector<BatchOut> outs_;
     DevBuf d_progs_, d_start_, d_pids_, d_outs_, d_parts_, d_status_, d_pdone_, d_err_;
+    DevBuf d_spill_, d_frags_, d_spill_ctr_, d_offmap_, d_glist_;
+    uint64_t spill_cap_ = 1ull << 24;  // rows
     uint64_t nitems_ = 0;
     // per class: its programs
     // (d_pids_ + pid_off), item starts (d_start_ + cs_off) and item count
