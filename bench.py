@@ -686,7 +686,17 @@ def workload_serve(args, L, rank, world, local, dist, dev):
                     "completed_per_s": nreq / wall, "served_gbs": served / wall / 1e9, "p50_ms": st["p50_ms"],
                     "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
 
-        one_rate(1000, 200, 1)  # warm-up
+        # warm-up: every group-by and join input several times (each of the
+        # operator workers sizes its scratch on first use) and a run of programs
+        wids = []
+        for _ in range(4):
+            for keys, vals, ng in gbs_in:
+                wids.append(srv.submit_groupby(keys, vals, ng, capacity=ng))
+            for b, pay, pk, (lo, ro) in joins:
+                wids.append(srv.submit_join(b, pay, pk, lo, ro, pk.numel()))
+        for rid in wids:
+            srv.result(rid)
+        one_rate(1000, 1000, 1)
         with ClockSampler(local) as clk:
             for i, rate in enumerate(rates):
                 table.append(one_rate(rate, args.requests, 100 + i))
