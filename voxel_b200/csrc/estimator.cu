@@ -61,17 +61,28 @@ __global__ void minmax_hll_kernel(const T* __restrict__ col, uint64_t n, unsigne
     for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     double lo = INFINITY, hi = -INFINITY;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        T v = col[i];
-        double d = as_double(v);
-        lo = d < lo ? d : lo;
-        hi = d > hi ? d : hi;
-        uint64_t h = splitmix(to_bits<T>(v));
-        uint32_t reg = static_cast<uint32_t>(h >> (64 - kHllP));
-        uint64_t rest = h << kHllP;
-        uint32_t rank = rest ? static_cast<uint32_t>(__clzll(static_cast<long long>(rest))) + 1 : 64 - kHllP + 1;
-        if (rank > sh[reg]) atomicMax(&sh[reg], rank);
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    // four elements in flight per thread: loads first, then the updates
+    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        T vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t i = i0 + u * stride;
+            vv[u] = i < n ? __ldcs(col + i) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) break;
+            const T v = vv[u];
+            double d = as_double(v);
+            lo = d < lo ? d : lo;
+            hi = d > hi ? d : hi;
+            uint64_t h = splitmix(to_bits<T>(v));
+            uint32_t reg = static_cast<uint32_t>(h >> (64 - kHllP));
+            uint64_t rest = h << kHllP;
+            uint32_t rank = rest ? static_cast<uint32_t>(__clzll(static_cast<long long>(rest))) + 1 : 64 - kHllP + 1;
+            if (rank > sh[reg]) atomicMax(&sh[reg], rank);
+        }
     }
     auto okey = [](double x) {
         uint64_t b = static_cast<uint64_t>(__double_as_longlong(x));
@@ -97,12 +108,22 @@ __global__ void histogram64_kernel(const T* __restrict__ col, uint64_t n, double
     if (threadIdx.x < kHistBins) sh[threadIdx.x] = 0;
     __syncthreads();
     double w = hi > lo ? (hi - lo) / kHistBins : 1.0;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        double d = as_double(col[i]);
-        int b = static_cast<int>((d - lo) / w);
-        b = b < 0 ? 0 : (b >= kHistBins ? kHistBins - 1 : b);
-        atomicAdd(&sh[b], 1u);
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        T vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t i = i0 + u * stride;
+            vv[u] = i < n ? __ldcs(col + i) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) break;
+            double d = as_double(vv[u]);
+            int b = static_cast<int>((d - lo) / w);
+            b = b < 0 ? 0 : (b >= kHistBins ? kHistBins - 1 : b);
+            atomicAdd(&sh[b], 1u);
+        }
     }
     __syncthreads();
     if (threadIdx.x < kHistBins && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
@@ -386,7 +407,7 @@ int sketch_t(const T* d, uint64_t n, ColumnSketch* out, cudaStream_t s) {
     VX_CUDA(cudaMemsetAsync(hll, 0, kHllRegs * 4 + kHistBins * 8, s));
     out->n = n;
     if (n) {
-        minmax_hll_kernel<T><<<sgrid(n), 256, 0, s>>>(d, n, mm, mm + 1, hll);
+        minmax_hll_kernel<T><<<sgrid(n, 8), 256, 0, s>>>(d, n, mm, mm + 1, hll);
         VX_CUDA(cudaGetLastError());
         unsigned long long h[2];
         if (int st = d2h(h, mm, 16, s)) return st;
@@ -399,7 +420,7 @@ int sketch_t(const T* d, uint64_t n, ColumnSketch* out, cudaStream_t s) {
         };
         out->min = dec(h[0]);
         out->max = dec(h[1]);
-        histogram64_kernel<T><<<sgrid(n), 256, 0, s>>>(d, n, out->min, out->max, hist);
+        histogram64_kernel<T><<<sgrid(n, 8), 256, 0, s>>>(d, n, out->min, out->max, hist);
         VX_CUDA(cudaGetLastError());
     } else {
         out->min = out->max = 0.0;
