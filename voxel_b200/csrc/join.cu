@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(kJThreads) probe_kernel(
                 if (lane >= d) t += y;
             }
             if (lane < kJThreads / 32) s_warp[lane] = t - x;
-            if (lane == kJThreads / 32 - 1) s_base = lookback_exclusive(status, tile, t, err);
+            const uint64_t tile_total = __shfl_sync(0xffffffffu, t, kJThreads / 32 - 1);
+            const uint64_t e = lookback_exclusive_warp(status, tile, tile_total, err);
+            if (lane == 0) s_base = e;
         }
         __syncthreads();
         uint64_t pos = s_base + s_warp[warp] + (inc - c);
