@@ -73,7 +73,7 @@ __global__ void insert_runs_kernel(const int64_t* __restrict__ skeys, const uint
 }
 
 constexpr int kJThreads = 256;
-constexpr int kJItems = 8;
+constexpr int kJItems = 4;  // probes per thread (8 blocks per SM; measured best)
 constexpr int kJTile = kJThreads * kJItems;
 
 __device__ __forceinline__ Slot lookup(const Slot* __restrict__ table, uint64_t mask, int64_t k) {
@@ -95,7 +95,7 @@ __device__ __forceinline__ Slot lookup(const Slot* __restrict__ table, uint64_t 
     return miss;
 }
 
-__global__ void __launch_bounds__(kJThreads) probe_kernel(
+__global__ void __launch_bounds__(kJThreads, 8) probe_kernel(
     const Slot* __restrict__ table, uint64_t mask, const uint32_t* __restrict__ srows,
     const uint64_t* __restrict__ payload, const int64_t* __restrict__ probe, uint64_t np, int all, uint64_t cap,
     uint32_t* __restrict__ left, uint32_t* __restrict__ right, unsigned long long* count_sum,
