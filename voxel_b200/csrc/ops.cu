@@ -108,31 +108,38 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
     for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) i_slot[i] = __ldcg(t.slot + i);
     __syncthreads();
     unsigned int added = 0;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t k = __ldcs(keys + i);
-        const unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
-        uint32_t h = hash32(k) & mask;
-        uint32_t probes = 0;
-        unsigned long long cur;
-        while ((cur = i_slot[h]) != want && cur != 0 && probes++ < mask) h = (h + 1) & mask;
-        if (cur == want) continue;
-        uint64_t g = hash32(k) & t.mask;
-        for (uint64_t p = 0;; ++p) {
-            const unsigned long long c = __ldcg(t.slot + g);
-            if (c == want) break;
-            if (c == 0) {
-                const unsigned long long old = atomicCAS(&t.slot[g], 0ull, want);
-                if (old == 0) {
-                    ++added;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        uint32_t kk[4];  // four keys in flight per thread
+#pragma unroll
+        for (int u = 0; u < 4; ++u) kk[u] = i0 + u * stride < n ? __ldcs(keys + i0 + u * stride) : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) break;
+            const uint32_t k = kk[u];
+            const unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
+            uint32_t h = hash32(k) & mask;
+            uint32_t probes = 0;
+            unsigned long long cur;
+            while ((cur = i_slot[h]) != want && cur != 0 && probes++ < mask) h = (h + 1) & mask;
+            if (cur == want) continue;
+            uint64_t g = hash32(k) & t.mask;
+            for (uint64_t p = 0;; ++p) {
+                const unsigned long long c = __ldcg(t.slot + g);
+                if (c == want) break;
+                if (c == 0) {
+                    const unsigned long long old = atomicCAS(&t.slot[g], 0ull, want);
+                    if (old == 0) {
+                        ++added;
+                        break;
+                    }
+                    if (old == want) break;
+                }
+                g = (g + 1) & t.mask;
+                if (p > t.mask) {
+                    atomicOr(overflow, 1);
                     break;
                 }
-                if (old == want) break;
-            }
-            g = (g + 1) & t.mask;
-            if (p > t.mask) {
-                atomicOr(overflow, 1);
-                break;
             }
         }
     }
@@ -252,27 +259,39 @@ __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uin
     __syncthreads();
     const uint32_t mask = cap - 1;
     bool bad = false;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        // the key's slot: linear probing in the shared copy
-        const uint32_t key = __ldcs(keys + i);
-        const unsigned long long want = (static_cast<unsigned long long>(key) << 32) | 1ull;
-        uint32_t sl = hash32(key) & mask;
-        uint32_t probes = 0;
-        unsigned long long cur;
-        while ((cur = s_slot[sl]) != want && cur != 0 && probes++ < mask) sl = (sl + 1) & mask;
-        if (cur != want) {
-            bad = true;
-            continue;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        // four rows in flight per thread: loads first
+        uint32_t kk[4];
+        double vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t i = i0 + u * stride;
+            kk[u] = i < n ? __ldcs(keys + i) : 0u;
+            vv[u] = i < n ? __ldcs(vals + i) : 0.0;
         }
-        const double v = __ldcs(vals + i);
-        Words96 w;
-        if (words96(v, &w)) add96(s_w + kAccWords * sl, w, v < 0.0);
-        else bad = true;
-        atomicAdd(&s_cnt[sl], 1u);
-        const uint64_t ok = f64_order_key(v);
-        if (ok < s_mn[sl]) atomicMin(&s_mn[sl], static_cast<unsigned long long>(ok));
-        if (ok > s_mx[sl]) atomicMax(&s_mx[sl], static_cast<unsigned long long>(ok));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) break;
+            // the key's slot: linear probing in the shared copy
+            const unsigned long long want = (static_cast<unsigned long long>(kk[u]) << 32) | 1ull;
+            uint32_t sl = hash32(kk[u]) & mask;
+            uint32_t probes = 0;
+            unsigned long long cur;
+            while ((cur = s_slot[sl]) != want && cur != 0 && probes++ < mask) sl = (sl + 1) & mask;
+            if (cur != want) {
+                bad = true;
+                continue;
+            }
+            const double v = vv[u];
+            Words96 w;
+            if (words96(v, &w)) add96(s_w + kAccWords * sl, w, v < 0.0);
+            else bad = true;
+            atomicAdd(&s_cnt[sl], 1u);
+            const uint64_t ok = f64_order_key(v);
+            if (ok < s_mn[sl]) atomicMin(&s_mn[sl], static_cast<unsigned long long>(ok));
+            if (ok > s_mx[sl]) atomicMax(&s_mx[sl], static_cast<unsigned long long>(ok));
+        }
     }
     if (bad) atomicOr(err, 1);
     __syncthreads();
