@@ -72,9 +72,9 @@ class BatchResults(Sequence):
             return [self[k] for k in range(*i.indices(len(self)))]
         r = self._cache[i]
         if r is None:
-            sel = self._extra.get(i)
-            r = ProgramResult(self.registers[i], int(self.counts[i]), sel, float(self._est[i]), bool(self._ovf[i]),
-                              None if sel is not None else self._pool, int(self._offs[i]))
+            pool, off = self._extra.get(i, (self._pool, int(self._offs[i])))
+            r = ProgramResult(self.registers[i], int(self.counts[i]), None, float(self._est[i]), bool(self._ovf[i]),
+                              pool, off)
             self._cache[i] = r
         return r
 
@@ -205,7 +205,7 @@ class LearnedBatch:
                     if ovf2[ids].any() or (cnt2[ids] != sizes).any() or (regs2[ids] != regs[ids]).any():
                         raise RuntimeError("exact re-run disagrees with the batch")
                 for k, i in enumerate(ids.tolist()):
-                    extra[i] = pool2[int(offs[k]):int(offs[k + 1])]
+                    extra[i] = (pool2, int(offs[k]))  # a view is made on first access
         out = BatchResults(regs, cnts, self.est, ovfs, self.pool, self.offs, extra)
         self.last_timing = {"launch_fetch_ms": (t1 - t0) * 1e3, "results_ms": (t2 - t1) * 1e3,
                             "overflow_ms": (time.perf_counter() - t2) * 1e3, "overflowed": int(redo.size),
