@@ -224,3 +224,22 @@ def test_device_entry_points_equal_host_ones():
     bad[777] = d["dict"].size  # one index past the dictionary
     st = L.voxel_dict_decode_dev(T.I32, dd.data_ptr(), d["dict"].size, bad.data_ptr(), d["n"], o2.data_ptr(), None)
     assert st == 1  # VOXEL_EINVAL
+
+
+def test_rle_decode_zero_length_runs_and_windows():
+    """RLE decode with empty runs mixed in (a run of 0 rows covers nothing) and
+    windows that start and end inside runs, across the expand kernel's tiles
+    (and past the last row, which decodes to 0), against numpy's repeat."""
+    L = capi.lib()
+    rng = np.random.default_rng(61)
+    nruns = 50_000
+    runs = rng.integers(0, 6, nruns).astype(np.uint32)  # about 1 in 6 runs is empty
+    vals = rng.integers(-(1 << 40), 1 << 40, nruns).astype(np.int64)
+    full = np.repeat(vals, runs.astype(np.int64))
+    for off, cnt in ((0, full.size), (1, 5000), (2047, 4099), (12345, 60000), (full.size - 10, 30), (5, full.size)):
+        out = np.full(cnt, 7, np.int64)
+        assert L.voxel_rle_decode_i64(vals.ctypes.data, runs.ctypes.data, nruns, off, cnt, out.ctypes.data) == 0
+        want = np.zeros(cnt, np.int64)
+        part = full[off:off + cnt]
+        want[:part.size] = part
+        assert (out == want).all(), (off, cnt)
