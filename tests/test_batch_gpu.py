@@ -266,3 +266,80 @@ def test_learned_batch_run_matches_plain_two_pass(margin, slack, spill):
             assert np.array_equal(np.asarray(a.registers, np.uint64), np.asarray(b.registers, np.uint64))
             assert a.count == b.count and torch.equal(a.selection, b.selection)
     lb.close()
+
+
+def _sum_count_program(dt, p0, p1):
+    """Two reductions in one loop over the conjunction of two atoms: SUM into
+    r0, COUNT into r3 (the interpreted several-reduction class)."""
+    from voxel_b200 import bytecode as bc
+
+    kl = T.K_LANES[dt]
+    code = [bc.vsplat(8, 8), bc.vsplat(9, 9), bc.vsplat(12, 12)]
+    head = len(code)
+    code += [bc.vload(0, 1, 0), bc.vcmp(p0.op, 4, 0, 8), bc.vcmp(p1.op, 5, 0, 9), bc.vand(4, 4, 5),
+             bc.vand(6, 4, 0), bc.vsum(5, 6), bc.addf(0, 0, 5) if dt in (T.F64, T.F32) else bc.add(0, 0, 5),
+             bc.vand(7, 4, 12), bc.vcount(10, 7), bc.add(3, 3, 10), bc.add(1, 1, 4), bc.cmp(1, 2)]
+    code.append(bc.jnz(head - len(code)))
+    code.append(bc.halt())
+    regs = {0: 0, 1: 0, 3: 0, 4: kl, 8: T.reg_image(dt, p0.value), 9: T.reg_image(dt, p1.value),
+            12: T.reg_image(dt, 1)}
+    return T.Program(dt, [p0, p1], "SUM", code, regs, 0)
+
+
+def test_batch_interpreted_classes_with_spill():
+    """Programs without a range form (two reductions in one loop, NE-only
+    predicates, three NE atoms) run on the interpreted class kernels: counts,
+    selection vectors (through buffers a third of the size, the rest from the
+    spill arena) and registers equal numpy and the reference interpreter."""
+    L = capi.lib()
+    rng = np.random.default_rng(46)
+    progs, cols, masks = [], [], []
+    for i in range(36):
+        dt = i % 6
+        n = int(T.K_LANES[dt] * rng.integers(200, 30000))
+        col = T.make_column(dt, n, rng)
+        a, b, c = (float(x) for x in rng.uniform(0, 1000, 3))
+        if dt not in (T.F64, T.F32):
+            a, b, c = (float(int(x)) for x in (a, b, c))
+        kind = i // 6 % 3
+        if kind == 0:
+            prog = _sum_count_program(dt, T.Pred(5, min(a, b)), T.Pred(2, max(a, b)))
+        elif kind == 1:
+            prog = T.build(dt, [T.Pred(1, a), T.Pred(1, b)], T.AGGS[i % 4])
+        else:
+            prog = T.build(dt, [T.Pred(4, min(a, b)), T.Pred(1, a), T.Pred(1, b), T.Pred(1, c)], T.AGGS[i % 4])
+        m = np.ones(n, bool)
+        for p in prog.preds:
+            v = np.float32(p.value) if dt == T.F32 else T.NP[dt](p.value)
+            m &= [np.equal, np.not_equal, np.less, np.less_equal, np.greater, np.greater_equal][p.op](col, v)
+        progs.append(prog)
+        cols.append(col)
+        masks.append(m)
+    caps = [int(m.sum()) // 3 for m in masks]
+    b, keep = make_batch(progs, cols, caps)
+    forms = [L.voxel_batch_form(b, i) for i in range(len(progs))]
+    assert all(f == 0 for f in forms)  # none has a range form
+    assert L.voxel_batch_launch(b, 1, None) == 0 and L.voxel_batch_fetch(b, None) == 0, capi.last_error()
+    over = []
+    for i, (prog, col, m) in enumerate(zip(progs, cols, masks)):
+        regs, cnt, ovf = results(b, i)
+        assert cnt == int(m.sum()), i
+        if cnt > caps[i]:
+            assert ovf == 1, i
+            over.append(i)
+        if prog.dtype == T.F32:
+            st_, want, _ = oracle.engine_run_port(prog.dtype, prog.code, [col], prog.registers(col.size))
+            assert st_ == 0
+        else:
+            want = oracle.engine_run_ref(prog.dtype, prog.code, [col], prog.registers(col.size))
+        check_regs(prog.dtype, prog.code, regs, want)
+    sizes = [int(masks[i].sum()) for i in over]
+    pool = torch.zeros(max(sum(sizes), 1), dtype=torch.int32, device=torch.device("cuda", 0))
+    ids = np.asarray(over, np.uint64)
+    assert L.voxel_batch_gather_overflow(b, len(over), ids.ctypes.data, pool.data_ptr(), None) == 0, capi.last_error()
+    got = pool.cpu().numpy().astype(np.int64)
+    off = 0
+    for i, sz in zip(over, sizes):
+        assert (got[off:off + sz] == np.flatnonzero(masks[i])).all(), i
+        off += sz
+    L.voxel_batch_destroy(b)
