@@ -256,7 +256,9 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
 /* kernel variant of the calling thread's fused scan:
- *   -1 = default (1);
+ *   -1 = default: the autotuner times variants 1, 2, 3 and 5 on the first
+ *        call of each (dictionary size, row count) of 65,536 rows or more and
+ *        keeps the fastest (1 for smaller scans and when tuning is off);
  *    1 / 2 = 32-bit-word group table fed by a per-warp row queue, 4 / 8 rows
  *        per thread (1 is the default);
  *    3 / 5 = 32-bit-word group table, rows added where read, 4 / 8 rows per thread;
@@ -267,6 +269,16 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  * with queue, 3 word table direct. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
+/* Autotuner (no reference counterpart): kernel families with several
+ * equivalent configurations (the fused scan's variants, the radix sort's
+ * keys per thread) time them on the first call of each (GPU, element type,
+ * log2 size) and cache the fastest in a JSON file: $VOXEL_TUNE_CACHE, else
+ * tune_cache.json beside this library.  VOXEL_TUNE=0 (or enable(0)) uses
+ * each family's default.  lookup returns the cached choice or -1. */
+void      voxel_tune_enable(int on);
+void      voxel_tune_set_cache_path(const char* path);
+void      voxel_tune_clear(void);
+int       voxel_tune_lookup(const char* family, int dtype, size_t n);
 int       voxel_scan_groupby_dev(const uint64_t* d_packed_key, size_t nwords, uint32_t width,
                                  const int32_t* d_dict, size_t card, const double* d_price,
                                  const int32_t* d_qty, size_t n, double price_gt, int32_t qty_lo,

@@ -135,3 +135,32 @@ def test_reference_c_example_builds_against_this_library(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", src, "-I", os.path.join(root, "include"), "-L", lib, "-lvoxel_c",
                         f"-Wl,-rpath,{lib}", "-o", str(out)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_tune_cache_file_round_trip(lib, tmp_path):
+    """The autotuner's cache is a JSON object of "<gpu>|<family>|<dtype>|<log2
+    n>": choice entries; lookups read it, a malformed file reads as empty, and
+    clear() writes an empty object.  Without a GPU the device name is
+    "unknown"."""
+    import json
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("keys carry the device name when a GPU is present")
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"unknown|radix_onesweep|2|20": 1, "unknown|scan_groupby_card10|9|25": 3}))
+    try:
+        lib.voxel_tune_set_cache_path(str(path).encode())
+        assert lib.voxel_tune_lookup(b"radix_onesweep", 2, 1 << 20) == 1
+        assert lib.voxel_tune_lookup(b"radix_onesweep", 2, (1 << 21) - 1) == 1  # same log2 bucket
+        assert lib.voxel_tune_lookup(b"radix_onesweep", 2, 1 << 21) == -1
+        assert lib.voxel_tune_lookup(b"radix_onesweep", 3, 1 << 20) == -1
+        assert lib.voxel_tune_lookup(b"scan_groupby_card10", 9, 1 << 25) == 3
+        path.write_text('{"unknown|radix_onesweep|2|20": , garbage')
+        lib.voxel_tune_set_cache_path(str(path).encode())
+        assert lib.voxel_tune_lookup(b"radix_onesweep", 2, 1 << 20) == -1
+        lib.voxel_tune_clear()
+        assert json.loads(path.read_text()) == {}
+    finally:
+        lib.voxel_tune_set_cache_path(None)

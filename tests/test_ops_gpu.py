@@ -147,6 +147,57 @@ def test_radix_sort_golden_and_properties(golden):
         assert (idx == order).all() and (k == k0[order]).all()
 
 
+def test_autotuner_times_and_caches_radix_and_scan(tmp_path):
+    """First calls of a shape time the candidate configurations, cache the
+    fastest per (GPU, family, element type, log2 size) and still return the
+    exact result; later calls read the cache."""
+    import json
+
+    L = capi.lib()
+    path = tmp_path / "tune.json"
+    L.voxel_tune_set_cache_path(str(path).encode())
+    try:
+        L.voxel_tune_enable(1)
+        L.voxel_tune_clear()
+        n = (1 << 20) + 7
+        k0 = inputs.sort_keys(T.U64, n, 77)
+        for _ in range(2):
+            k = k0.copy()
+            idx = np.arange(n, dtype=np.uint32)
+            assert L.voxel_radix_sort(T.U64, k.ctypes.data, idx.ctypes.data, n) == 0, capi.last_error()
+            order = np.argsort(k0, kind="stable")
+            assert (idx == order).all() and (k == k0[order]).all()
+        assert L.voxel_tune_lookup(b"radix_onesweep", T.U64, n) in (0, 1)
+        assert L.voxel_tune_lookup(b"radix_onesweep", T.U32, n) == -1
+        d = inputs.config2(1 << 20, 78)
+        card = d["dict"].size
+        w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], 20.0, 10, 50)
+        assert L.voxel_scan_groupby_tune(-1) == 0
+        for _ in range(2):
+            ok = np.zeros(card, np.int32)
+            s, mn, mx = (np.zeros(card) for _ in range(3))
+            c = np.zeros(card, np.uint64)
+            g = L.voxel_scan_groupby(d["packed"].ctypes.data, d["packed"].size, d["width"], d["dict"].ctypes.data,
+                                     card, d["price"].ctypes.data, d["qty"].ctypes.data, d["price"].size, 20.0, 10,
+                                     50, ok.ctypes.data, s.ctypes.data, mn.ctypes.data, mx.ctypes.data, c.ctypes.data)
+            assert g == w[0].size, capi.last_error()
+            assert (ok[:g] == w[0]).all() and (c[:g] == w[4]).all() and (mn[:g] == w[2]).all()
+            np.testing.assert_allclose(s[:g], w[1], rtol=1e-12, atol=0)
+        fam = "scan_groupby_card%d" % (card.bit_length() - 1)
+        assert L.voxel_tune_lookup(fam.encode(), T.F64, d["price"].size) in (0, 1, 2, 3)
+        entries = json.loads(path.read_text())
+        assert {e.split("|")[1] for e in entries} == {"radix_onesweep", fam}
+        # tuning off: nothing new is timed or cached
+        L.voxel_tune_enable(0)
+        k = inputs.sort_keys(T.U32, n, 79)
+        idx = np.arange(n, dtype=np.uint32)
+        assert L.voxel_radix_sort(T.U32, k.ctypes.data, idx.ctypes.data, n) == 0
+        assert L.voxel_tune_lookup(b"radix_onesweep", T.U32, n) == -1
+    finally:
+        L.voxel_tune_enable(1)
+        L.voxel_tune_set_cache_path(None)
+
+
 def test_hashjoin_golden_and_properties(golden):
     L = capi.lib()
     for case in golden["ops"]["hashjoin"]:

@@ -47,6 +47,7 @@ CORE_SOURCES = [
     "estimator.cu",
     "batch.cu",
     "serve.cpp",
+    "tune.cpp",
     "capi.cpp",
 ]
 

@@ -158,6 +158,10 @@ _SIGS = {
     "voxel_batch_result": (C.c_int, [vp, sz, vp, vp, vp]),
     "voxel_batch_results_all": (C.c_int, [vp, vp, vp, vp]),
     "voxel_batch_form": (C.c_int, [vp, sz]),
+    "voxel_tune_enable": (None, [C.c_int]),
+    "voxel_tune_set_cache_path": (None, [C.c_char_p]),
+    "voxel_tune_clear": (None, []),
+    "voxel_tune_lookup": (C.c_int, [C.c_char_p, C.c_int, sz]),
     "voxel_batch_rerun": (C.c_int, [vp, sz, vp, vp, vp, vp]),
     "voxel_batch_gather_overflow": (C.c_int, [vp, sz, vp, vp, vp]),
     "voxel_batch_set_spill_capacity": (C.c_int, [vp, sz]),

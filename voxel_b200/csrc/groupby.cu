@@ -25,6 +25,7 @@
 
 #include "fixedpoint.cuh"
 #include "groupby.h"
+#include "tune.h"
 #include "tma.cuh"
 #include "voxel_c.h"
 #include "vx_common.cuh"
@@ -869,6 +870,25 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
 #define VX_LAUNCH_RPT(R, M)                                                                                    \
     launch_rpt<R, M>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum, out_min, \
                      out_max, out_count, out_ngroups, s)
+    if (autotune && !use_tma && n >= (1u << 16)) {  // smaller scans take the default
+        // the word-table variants give identical bits: time them on this call's
+        // data once per (dictionary size, rows) and keep the fastest
+        auto variant = [&](int c) -> int {
+            switch (c) {
+            case 1: return VX_LAUNCH_RPT(8, 1);
+            case 2: return VX_LAUNCH_RPT(4, 2);
+            case 3: return VX_LAUNCH_RPT(8, 2);
+            default: return VX_LAUNCH_RPT(4, 1);
+            }
+        };
+        int cl = 0;
+        while (cl < 31 && (2u << cl) <= card) ++cl;
+        const std::string family = "scan_groupby_card" + std::to_string(cl);
+        const std::string key = tune_key(family.c_str(), F64, n);
+        int c = 0;
+        if (!tune_lookup(key, &c)) c = tune_pick(key, 4, 0, s, variant);
+        return variant(c);
+    }
     if (mode == 1) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 1) : VX_LAUNCH_RPT(4, 1);
     if (mode == 2) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 2) : VX_LAUNCH_RPT(4, 2);
     switch (rows_per_thread) {
@@ -978,6 +998,7 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
 
 int voxel_scan_groupby_tune(int variant) {
     ScanGroupBy& S = scan_groupby_state();
+    S.autotune = variant == -1;  // -1: the autotuner's choice per shape (word table + queue, 4 rows, untuned)
     if (variant == -1) variant = 1;
     if (variant == 0) {
         S.use_tma = true;

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "radix.h"
+#include "tune.h"
 #include "voxel_c.h"
 #include "vx_common.cuh"
 #include "vx_runtime.h"
@@ -28,8 +29,11 @@ constexpr int kRBits = 8;
 constexpr int kRadix = 1 << kRBits;
 constexpr int kRThreads = 512;
 constexpr int kRWarps = kRThreads / 32;
-constexpr int kRItems = 16;
-constexpr int kRTile = kRThreads * kRItems;  // 8192 keys
+// keys per thread in the onesweep pass: 16 (8192-key tiles, one block per SM)
+// or 8 (4096-key tiles, two blocks per SM), chosen per shape by the autotuner
+constexpr int kRItemsMax = 16;
+constexpr int kRItemsMin = 8;
+constexpr int kRTileMin = kRThreads * kRItemsMin;  // the smallest tile sizes the scratch
 
 constexpr uint32_t kStAgg = 1u << 30;
 constexpr uint32_t kStInc = 2u << 30;
@@ -74,22 +78,22 @@ __global__ void hist_scan_kernel(const unsigned int* hist, unsigned int* offs) {
     offs[p * kRadix + d] = s[d] - hist[p * kRadix + d];
 }
 
-template <typename K>
-__global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
+template <typename K, int ITEMS>
+__global__ void __launch_bounds__(kRThreads, ITEMS >= 16 ? 1 : 2) onesweep_kernel(
     const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __restrict__ vin, uint32_t* __restrict__ vout,
     uint64_t n, int shift, K flip_in, K flip_out, const unsigned int* __restrict__ digit_offs,
     unsigned int* status, unsigned int* tile_ctr, int* err) {
     extern __shared__ __align__(16) unsigned char smem[];
     K* s_keys = reinterpret_cast<K*>(smem);
-    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + kRTile);
-    unsigned int* s_cnt = s_vals + kRTile;                // [kRWarps][kRadix]
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + (kRThreads * ITEMS));
+    unsigned int* s_cnt = s_vals + (kRThreads * ITEMS);                // [kRWarps][kRadix]
     unsigned int* s_tstart = s_cnt + kRWarps * kRadix;     // [kRadix]
     unsigned int* s_gstart = s_tstart + kRadix;            // [kRadix] (low 32 bits)
     unsigned int* s_gstart_hi = s_gstart + kRadix;
     __shared__ uint64_t s_tile;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t ntiles = (n + kRTile - 1) / kRTile;
+    const uint64_t ntiles = (n + (kRThreads * ITEMS) - 1) / (kRThreads * ITEMS);
     const unsigned lanemask_lt = (1u << lane) - 1;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
@@ -97,13 +101,13 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
         __syncthreads();
         const uint64_t tile = s_tile;
         if (tile >= ntiles) break;
-        const uint64_t base = tile * kRTile;
-        const uint64_t wbase = base + static_cast<uint64_t>(warp) * 32 * kRItems;
-        K key[kRItems];
-        uint32_t val[kRItems];
-        uint32_t rank[kRItems];
+        const uint64_t base = tile * (kRThreads * ITEMS);
+        const uint64_t wbase = base + static_cast<uint64_t>(warp) * 32 * ITEMS;
+        K key[ITEMS];
+        uint32_t val[ITEMS];
+        uint32_t rank[ITEMS];
 #pragma unroll
-        for (int i = 0; i < kRItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             uint64_t pos = wbase + i * 32 + lane;
             if (pos < n) {
                 key[i] = __ldcs(kin + pos) ^ flip_in;
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
         }
         unsigned int* wc = s_cnt + warp * kRadix;
 #pragma unroll
-        for (int i = 0; i < kRItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             uint64_t pos = wbase + i * 32 + lane;
             bool valid = pos < n;
             uint32_t d = valid ? digit_of(key[i], shift) : 0u;
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
         __syncthreads();
         // scatter into shared memory in (digit, stable rank) order
 #pragma unroll
-        for (int i = 0; i < kRItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             uint64_t pos = wbase + i * 32 + lane;
             if (pos < n) {
                 uint32_t d = digit_of(key[i], shift);
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
             }
         }
         __syncthreads();
-        const uint32_t tn = static_cast<uint32_t>(n - base < static_cast<uint64_t>(kRTile) ? n - base : kRTile);
+        const uint32_t tn = static_cast<uint32_t>(n - base < static_cast<uint64_t>((kRThreads * ITEMS)) ? n - base : (kRThreads * ITEMS));
         for (uint32_t j = threadIdx.x; j < tn; j += kRThreads) {
             K k = s_keys[j];
             uint32_t d = digit_of(k, shift);
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(kRThreads, 1) onesweep_kernel(
 
 template <typename K>
 size_t tmp_bytes_t(uint64_t n) {
-    uint64_t ntiles = (n + kRTile - 1) / kRTile;
+    uint64_t ntiles = (n + kRTileMin - 1) / kRTileMin;
     size_t b = n * sizeof(K) + n * 4;                    // ping-pong buffers
     b = (b + 255) / 256 * 256;
     b += ntiles * kRadix * 4 + 256;                       // look-back status
@@ -233,30 +237,23 @@ size_t tmp_bytes_t(uint64_t n) {
     return b;
 }
 
-size_t smem_bytes_t(size_t ksize) {
-    return kRTile * (ksize + 4) + (kRWarps * kRadix + 3 * kRadix) * 4;
+size_t smem_bytes_t(size_t ksize, int items) {
+    return static_cast<size_t>(kRThreads) * items * (ksize + 4) + (kRWarps * kRadix + 3 * kRadix) * 4;
 }
 
-template <typename K>
-int sort_t(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, size_t tmp_bytes, int* err,
-           cudaStream_t s, int* passes_out) {
-    if (n <= 1) return kOk;  // sort.hpp:84
-    if (n >= (1ull << 30)) {
-        set_error(kErrInvalidArg, "radix sort supports fewer than 2^30 keys per call");
-        return kErrInvalidArg;
-    }
-    if (tmp_bytes < tmp_bytes_t<K>(n)) {
-        set_error(kErrInvalidArg, "radix sort scratch too small (%zu < %zu)", tmp_bytes, tmp_bytes_t<K>(n));
-        return kErrInvalidArg;
-    }
+// the passes with ITEMS keys per thread (scratch laid out as tmp_bytes_t)
+template <typename K, int ITEMS>
+int sort_run(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, int* err, cudaStream_t s) {
+    constexpr uint64_t kTile = static_cast<uint64_t>(kRThreads) * ITEMS;
     const int passes = static_cast<int>(sizeof(K) * 8 / kRBits);
-    const uint64_t ntiles = (n + kRTile - 1) / kRTile;
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    const uint64_t status_words = ((n + kRTileMin - 1) / kRTileMin) * kRadix;  // sized for the smallest tile
     char* b = static_cast<char*>(tmp);
     K* ktmp = reinterpret_cast<K*>(b);
     uint32_t* vtmp = reinterpret_cast<uint32_t*>(b + n * sizeof(K));
     size_t off = (n * sizeof(K) + n * 4 + 255) / 256 * 256;
     unsigned int* status = reinterpret_cast<unsigned int*>(b + off);
-    off += ntiles * kRadix * 4 + 256;
+    off += status_words * 4 + 256;
     unsigned int* hist = reinterpret_cast<unsigned int*>(b + off);
     unsigned int* offs = hist + 8 * kRadix;
     off += 8 * kRadix * 4 * 2 + 256;
@@ -272,10 +269,12 @@ int sort_t(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, size_t
     VX_CUDA(cudaGetLastError());
     hist_scan_kernel<<<passes, kRadix, 0, s>>>(hist, offs);
     VX_CUDA(cudaGetLastError());
-    size_t smem = smem_bytes_t(sizeof(K));
-    VX_CUDA(cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = smem_bytes_t(sizeof(K), ITEMS);
+    VX_CUDA(cudaFuncSetAttribute(onesweep_kernel<K, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
-    uint64_t grid = ntiles < static_cast<uint64_t>(sms) ? ntiles : static_cast<uint64_t>(sms);
+    const uint64_t per_sm = ITEMS >= 16 ? 1 : 2;  // resident blocks per SM (shared memory)
+    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+    if (grid > ntiles) grid = ntiles;
     const K* kin = keys;
     const uint32_t* vin = idx;
     K* kout = ktmp;
@@ -285,7 +284,7 @@ int sort_t(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, size_t
         VX_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
         K fin = p == 0 ? flip : 0;
         K fout = p == passes - 1 ? flip : 0;
-        onesweep_kernel<K><<<static_cast<unsigned>(grid), kRThreads, smem, s>>>(
+        onesweep_kernel<K, ITEMS><<<static_cast<unsigned>(grid), kRThreads, smem, s>>>(
             kin, kout, vin, vout, n, p * kRBits, fin, fout, offs + p * kRadix, status, ctr, err);
         VX_CUDA(cudaGetLastError());
         // ping-pong; an even pass count leaves the result in the caller's buffers
@@ -296,8 +295,58 @@ int sort_t(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, size_t
         kin = nk;
         vin = nv;
     }
-    if (passes_out) *passes_out = passes;
     return kOk;
+}
+
+template <typename K>
+__global__ void tune_sample_kernel(K* keys, uint32_t* idx, uint64_t n, uint64_t seed) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t z = (i + 1) * 0x9e3779b97f4a7c15ull + seed;  // splitmix64 of the row
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        keys[i] = static_cast<K>(z ^ (z >> 31));
+        idx[i] = static_cast<uint32_t>(i);
+    }
+}
+
+constexpr uint64_t kTuneMinKeys = 1ull << 16;     // smaller sorts take the default
+constexpr uint64_t kTuneSampleKeys = 1ull << 24;  // tuning sorts at most this many random keys
+
+template <typename K>
+int sort_t(int dtype, K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, size_t tmp_bytes, int* err,
+           cudaStream_t s, int* passes_out) {
+    if (n <= 1) return kOk;  // sort.hpp:84
+    if (n >= (1ull << 30)) {
+        set_error(kErrInvalidArg, "radix sort supports fewer than 2^30 keys per call");
+        return kErrInvalidArg;
+    }
+    if (tmp_bytes < tmp_bytes_t<K>(n)) {
+        set_error(kErrInvalidArg, "radix sort scratch too small (%zu < %zu)", tmp_bytes, tmp_bytes_t<K>(n));
+        return kErrInvalidArg;
+    }
+    // keys per thread: the autotuner's choice for this (type, size), timed on
+    // random keys of the same type (the caller's keys are sorted only once)
+    int choice = 0;  // 0: 16 keys per thread, 1: 8
+    if (n >= kTuneMinKeys) {
+        const std::string key = tune_key("radix_onesweep", dtype, n);
+        if (!tune_lookup(key, &choice) && tune_may_time(s)) {
+            const uint64_t m = n < kTuneSampleKeys ? n : kTuneSampleKeys;
+            DevBuf sk(m * sizeof(K)), si(m * 4), st(tmp_bytes_t<K>(m));
+            if (sk.p && si.p && st.p) {
+                choice = tune_pick(key, 2, 0, s, [&](int c) -> int {
+                    tune_sample_kernel<K><<<static_cast<unsigned>(sm_count() > 0 ? sm_count() * 4 : 592), 256, 0, s>>>(
+                        sk.as<K>(), si.as<uint32_t>(), m, 0x5eedull);
+                    return c == 0 ? sort_run<K, kRItemsMax>(sk.as<K>(), si.as<uint32_t>(), m, is_signed, st.p, err, s)
+                                  : sort_run<K, kRItemsMin>(sk.as<K>(), si.as<uint32_t>(), m, is_signed, st.p, err, s);
+                });
+            }
+        }
+    }
+    const int r = choice == 1 ? sort_run<K, kRItemsMin>(keys, idx, n, is_signed, tmp, err, s)
+                              : sort_run<K, kRItemsMax>(keys, idx, n, is_signed, tmp, err, s);
+    if (passes_out) *passes_out = static_cast<int>(sizeof(K) * 8 / kRBits);
+    return r;
 }
 
 }  // namespace
@@ -309,10 +358,10 @@ size_t radix_tmp_bytes(int dtype, uint64_t n) {
 int launch_radix_sort(int dtype, void* keys, uint32_t* idx, uint64_t n, void* tmp, size_t tmp_bytes, int* err,
                       cudaStream_t s, int* passes) {
     switch (dtype) {
-    case U64: return sort_t<uint64_t>(static_cast<uint64_t*>(keys), idx, n, false, tmp, tmp_bytes, err, s, passes);
-    case I64: return sort_t<uint64_t>(static_cast<uint64_t*>(keys), idx, n, true, tmp, tmp_bytes, err, s, passes);
-    case U32: return sort_t<uint32_t>(static_cast<uint32_t*>(keys), idx, n, false, tmp, tmp_bytes, err, s, passes);
-    case I32: return sort_t<uint32_t>(static_cast<uint32_t*>(keys), idx, n, true, tmp, tmp_bytes, err, s, passes);
+    case U64: return sort_t<uint64_t>(dtype, static_cast<uint64_t*>(keys), idx, n, false, tmp, tmp_bytes, err, s, passes);
+    case I64: return sort_t<uint64_t>(dtype, static_cast<uint64_t*>(keys), idx, n, true, tmp, tmp_bytes, err, s, passes);
+    case U32: return sort_t<uint32_t>(dtype, static_cast<uint32_t*>(keys), idx, n, false, tmp, tmp_bytes, err, s, passes);
+    case I32: return sort_t<uint32_t>(dtype, static_cast<uint32_t*>(keys), idx, n, true, tmp, tmp_bytes, err, s, passes);
     default:
         set_error(kErrInvalidArg, "radix sort key type %d must be an integer type (2..5)", dtype);
         return kErrInvalidArg;
