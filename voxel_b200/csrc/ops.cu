@@ -40,12 +40,13 @@ int ogrid(uint64_t n, int per_sm = 8) {
     return b < 1 ? 1 : static_cast<int>(b);
 }
 
-__device__ __forceinline__ uint32_t hash32(uint32_t k) {
-    // murmur3 fmix64 on the widened key, the mixer HashValue<u32> uses (ops/hash.hpp:334-339)
-    uint64_t x = k;
-    x = (x ^ (x >> 33)) * 0xff51afd7ed558ccdull;
-    x = (x ^ (x >> 33)) * 0xc4ceb9fe1a85ec53ull;
-    return static_cast<uint32_t>(x ^ (x >> 33));
+// Home slot of a key: Fibonacci (multiplicative) hashing, the top log2(cap)
+// bits of k * 2^32/phi (two instructions).  The slot layout is internal: every
+// result leaves the table sorted by key, so it need not follow the reference's
+// murmur3 mixer (ops/hash.hpp:334-339), whose two 64-bit multiplies and
+// shifts per row made both table kernels ALU-bound.
+__device__ __forceinline__ uint32_t home_slot(uint32_t k, uint32_t shift) {
+    return (k * 0x9E3779B1u) >> shift;
 }
 
 struct Table {
@@ -55,6 +56,7 @@ struct Table {
     unsigned long long* mn;
     unsigned long long* mx;
     uint64_t mask;
+    uint32_t shift;  // 32 - log2(mask + 1)
 };
 
 __global__ void table_init_kernel(Table t) {
@@ -78,7 +80,7 @@ __global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, u
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         uint32_t k = keys[i];
         unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
-        uint64_t h = hash32(k) & t.mask;
+        uint64_t h = home_slot(k, t.shift);
         for (uint64_t p = 0;; ++p) {
             unsigned long long cur = t.slot[h];
             if (cur == want) break;
@@ -118,12 +120,12 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
             if (i0 + u * stride >= n) break;
             const uint32_t k = kk[u];
             const unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
-            uint32_t h = hash32(k) & mask;
+            uint32_t h = home_slot(k, t.shift);
             uint32_t probes = 0;
             unsigned long long cur;
             while ((cur = i_slot[h]) != want && cur != 0 && probes++ < mask) h = (h + 1) & mask;
             if (cur == want) continue;
-            uint64_t g = hash32(k) & t.mask;
+            uint64_t g = home_slot(k, t.shift);
             for (uint64_t p = 0;; ++p) {
                 const unsigned long long c = __ldcg(t.slot + g);
                 if (c == want) break;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
 
 __device__ __forceinline__ uint64_t find_slot(const Table& t, uint32_t k) {
     unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
-    uint64_t h = hash32(k) & t.mask;
+    uint64_t h = home_slot(k, t.shift);
     for (uint64_t p = 0; p <= t.mask; ++p) {
         unsigned long long cur = __ldg(t.slot + h);
         if (cur == want) return h;
@@ -275,7 +277,7 @@ __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uin
             if (i0 + u * stride >= n) break;
             // the key's slot: linear probing in the shared copy
             const unsigned long long want = (static_cast<unsigned long long>(kk[u]) << 32) | 1ull;
-            uint32_t sl = hash32(kk[u]) & mask;
+            uint32_t sl = home_slot(kk[u], t.shift);
             uint32_t probes = 0;
             unsigned long long cur;
             while ((cur = s_slot[sl]) != want && cur != 0 && probes++ < mask) sl = (sl + 1) & mask;
@@ -317,7 +319,7 @@ __global__ void rehash_kernel(Table from, Table to) {
         unsigned long long w = from.slot[i];
         if (!w) continue;
         uint32_t k = static_cast<uint32_t>(w >> 32);
-        uint64_t h = hash32(k) & to.mask;
+        uint64_t h = home_slot(k, to.shift);
         for (;;) {
             if (atomicCAS(&to.slot[h], 0ull, w) == 0ull) break;
             h = (h + 1) & to.mask;
@@ -604,6 +606,10 @@ public:
     DevBuf groups_d, flag_d;
 
     int alloc_table(uint64_t c, Table& out, DevBuf& m, cudaStream_t s) {
+        if (c > (1ull << 32)) {  // more slots than 32-bit keys could need
+            set_error(kErrInvalidArg, "hash table of %llu slots exceeds 2^32", static_cast<unsigned long long>(c));
+            return kErrInvalidArg;
+        }
         size_t bytes = c * (8 + 24 + 8 + 8 + 8);
         m = DevBuf(bytes);
         if (!m.p) return kErrOutOfMemory;
@@ -614,6 +620,9 @@ public:
         out.mn = out.cnt + c;
         out.mx = out.mn + c;
         out.mask = c - 1;
+        int lg = 0;
+        while ((2ull << lg) <= c) ++lg;
+        out.shift = static_cast<uint32_t>(32 - lg);
         table_init_kernel<<<ogrid(c), kOThreads, 0, s>>>(out);
         VX_CUDA(cudaGetLastError());
         return kOk;
