@@ -141,19 +141,12 @@ __device__ __forceinline__ bool row_words(double x, RowWords* w) {
     return true;
 }
 
-// Propagates a carry (+1) or borrow (-1) into word j and upwards of a 5-word
-// two's-complement accumulator (exact modulo 2^160; no true sum needs more).
-__device__ __noinline__ void word_ripple(uint32_t* acc, int j, bool borrow) {
-    for (; j < kWords; ++j) {
-        const uint32_t old = atomicAdd(&acc[j], borrow ? 0xFFFFFFFFu : 1u);
-        if (borrow ? (old != 0u) : (old != 0xFFFFFFFFu)) break;
-    }
-}
-
 // Adds (neg: subtracts) a row's words to a group accumulator: the three
 // atomics are issued back to back, then each one's own wrap (read from its
-// returned old value) ripples into the next word.  Every wrap is accounted
-// exactly once, so concurrent updates compose to the exact sum.
+// returned old value) ripples into the next word, and further up while that
+// word wraps too.  Every wrap is accounted exactly once, so concurrent updates
+// compose to the exact sum (modulo 2^160; no true sum needs more).  The
+// pending wraps are walked in one inline loop (a call per wrap cost more).
 __device__ __forceinline__ void words_add(uint32_t* acc, const RowWords& w, bool neg) {
     const uint32_t d0 = neg ? 0u - w.c0 : w.c0, d1 = neg ? 0u - w.c1 : w.c1, d2 = neg ? 0u - w.c2 : w.c2;
     uint32_t o0 = 0, o1 = 0, o2 = 0;
@@ -161,12 +154,15 @@ __device__ __forceinline__ void words_add(uint32_t* acc, const RowWords& w, bool
     if (w.c1) o1 = atomicAdd(&acc[w.k0 + 1], d1);
     if (w.c2) o2 = atomicAdd(&acc[w.k0 + 2], d2);
     // add: carry when old + c wraps; subtract: borrow when old < c
-    const bool r0 = w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0);
-    const bool r1 = w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1);
-    const bool r2 = w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2);
-    if (r0) word_ripple(acc, w.k0 + 1, neg);
-    if (r1) word_ripple(acc, w.k0 + 2, neg);
-    if (r2) word_ripple(acc, w.k0 + 3, neg);
+    uint32_t pend = (w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0)) ? 2u : 0u;
+    pend |= (w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1)) ? 4u : 0u;
+    pend |= (w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2)) ? 8u : 0u;
+    const uint32_t step = neg ? 0xFFFFFFFFu : 1u, wrap = neg ? 0u : 0xFFFFFFFFu;
+    while (pend) {
+        int j = w.k0 + __ffs(pend) - 1;
+        pend &= pend - 1;
+        while (j < kWords && atomicAdd(&acc[j], step) == wrap) ++j;
+    }
 }
 
 // 160-bit two's complement (5 words) -> 192-bit.
