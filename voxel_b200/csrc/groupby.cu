@@ -257,7 +257,12 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     const int lane = threadIdx.x & 31;
     const unsigned lanemask_lt = (1u << lane) - 1;
     WarpQueue& Q = s_queue[threadIdx.x >> 5];
-    int qn = 0;  // warp-uniform fill of Q
+    int qn = 0;  // warp-uniform fill of Q (a ring of kQueue entries from qh)
+    int qh = 0;
+    // qty in [qlo, qhi] as one unsigned compare; an empty range passes nothing
+    // (p > +inf never holds), and rows past n read NaN prices (never pass)
+    const uint32_t qspan = qlo <= qhi ? static_cast<uint32_t>(qhi) - static_cast<uint32_t>(qlo) : 0u;
+    const double pcut = qlo <= qhi ? pthr : __longlong_as_double(0x7FF0000000000000ll);
     // lanes < cnt fold queue entry `lane` into the block table, converged.
     // Entries of the same group are first combined by the lowest such lane
     // (match + shuffles), so a hot group costs one set of atomics per round
@@ -282,10 +287,11 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
         uint32_t gi = 0;
         double p = 0.0, v = 0.0;
         if (valid) {
-            p = Q.price[lane];
-            gi = key_bits(packed, Q.row[lane], width, mask);
+            const int e = (qh + lane) & (kQueue - 1);
+            p = Q.price[e];
+            gi = key_bits(packed, Q.row[e], width, mask);
             // one rounded multiply, as the reference materialises price*qty
-            v = __dmul_rn(p, static_cast<double>(Q.qty[lane]));
+            v = __dmul_rn(p, static_cast<double>(Q.qty[e]));
         }
         if (WORDS) {
             if (valid) add_row(gi, v, p);
@@ -356,7 +362,7 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
 #pragma unroll
             for (int k = 0; k < RPT; ++k) {
                 bool in = r0 + k < n;
-                pv[k] = in ? price[r0 + k] : 0.0;
+                pv[k] = in ? price[r0 + k] : __longlong_as_double(0x7FF8000000000000ll);
                 qv[k] = in ? qty[r0 + k] : 0;
             }
         }
@@ -365,14 +371,14 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
             const uint64_t r = r0 + k;
             const double p = pv[k];
             const int32_t q = qv[k];
-            const bool pass = r < n && p > pthr && q >= qlo && q <= qhi;
+            const bool pass = p > pcut && static_cast<uint32_t>(q) - static_cast<uint32_t>(qlo) <= qspan;
             if (MODE == 2) {  // no queue: passing lanes add their rows directly
                 if (pass) add_row(key_bits(packed, r, width, mask), __dmul_rn(p, static_cast<double>(q)), p);
                 continue;
             }
             unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
-                int pos = qn + __popc(m & lanemask_lt);
+                const int pos = (qh + qn + __popc(m & lanemask_lt)) & (kQueue - 1);
                 Q.row[pos] = r;
                 Q.price[pos] = p;
                 Q.qty[pos] = q;
@@ -381,13 +387,8 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
             if (qn >= 32) {
                 __syncwarp();
                 consume(32);
-                __syncwarp();
-                if (lane < qn - 32) {
-                    Q.row[lane] = Q.row[32 + lane];
-                    Q.price[lane] = Q.price[32 + lane];
-                    Q.qty[lane] = Q.qty[32 + lane];
-                }
-                __syncwarp();
+                __syncwarp();  // the consumed entries are free for the next pushes
+                qh = (qh + 32) & (kQueue - 1);
                 qn -= 32;
             }
         }
