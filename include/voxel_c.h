@@ -262,11 +262,15 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  *    1 / 2 = 32-bit-word group table fed by a per-warp row queue, 4 / 8 rows
  *        per thread (1 is the default);
  *    3 / 5 = 32-bit-word group table, rows added where read, 4 / 8 rows per thread;
+ *    6 = 32-bit-word group table fed by bulk copies into shared-memory stages
+ *        (a producer warp keeps them in flight while 16 warps aggregate); needs
+ *        16-byte-aligned packed keys, at least 2048 rows, at most 2^19 rows per
+ *        SM and a table that fits beside two stages, else runs variant 1;
  *    4 / 8 / 16 = warp-merged rows, 192-bit shared atomics, that many rows per thread;
  *    0 = TMA-fed private warp tables (dictionaries up to 1024 entries).
  * All but 0 give bit-identical results.  voxel_scan_groupby_last_variant
  * reports the kernel the last call ran: 0 warp-merged, 1 TMA-fed, 2 word table
- * with queue, 3 word table direct. */
+ * with queue, 3 word table direct, 4 word table fed by bulk copies. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
 /* Autotuner (no reference counterpart): kernel families with several

@@ -81,14 +81,15 @@ def test_every_variant_gives_identical_bits():
     same integers, so every output bit agrees; the TMA-fed variant (compensated
     f64 per warp) and all of them match the oracle."""
     L = capi.lib()
-    cases = [inputs.config2(1 << 20, 31), inputs.config2(333_333, 32, card=4096), inputs.config2(5000, 33, card=3)]
+    cases = [inputs.config2(1 << 20, 31), inputs.config2(333_333, 32, card=4096), inputs.config2(5000, 33, card=3),
+             inputs.config2(1_000_003, 35, card=700)]
     preds = ((20.0, 10, 50), (-1.0, 0, 1000), (20.0, 50, 10))
     try:
         for d in cases:
             for pthr, qlo, qhi in preds:
                 w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], pthr, qlo, qhi)
                 base = None
-                for v in (4, 8, 16, 1, 2, 3, 5, 0):
+                for v in (4, 8, 16, 1, 2, 3, 5, 6, 0):
                     assert L.voxel_scan_groupby_tune(v) == 0
                     got = gpu_scan_groupby(d, pthr, qlo, qhi)
                     k, s, mn, mx, c = got
@@ -100,6 +101,25 @@ def test_every_variant_gives_identical_bits():
                         base = got
                     for a, b in zip(got, base):
                         assert a.size == b.size and (a.view(np.uint8) == b.view(np.uint8)).all(), (v, pthr)
+    finally:
+        L.voxel_scan_groupby_tune(-1)
+
+
+def test_bulk_copy_fed_word_table_runs_where_the_shape_allows():
+    """Variant 6 (bulk copies into shared-memory stages, word table) runs for
+    shapes with at least one full 2048-row stage and a table that fits beside
+    two stages, with a ragged tail; other shapes fall back to variant 1.  Both
+    give the oracle's results."""
+    L = capi.lib()
+    try:
+        assert L.voxel_scan_groupby_tune(6) == 0
+        for n, card, want_kernel in ((2048 * 300 + 1, 1000, 4), (4096, 5, 4), (2047, 50, 2), (300_000, 4096, 2)):
+            d = inputs.config2(n, 40 + card, card=card)
+            w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], 20.0, 10, 50)
+            k, s, mn, mx, c = gpu_scan_groupby(d)
+            assert L.voxel_scan_groupby_last_variant() == want_kernel, (n, card)
+            assert (k == w[0]).all() and (c == w[4]).all() and (mn == w[2]).all() and (mx == w[3]).all()
+            np.testing.assert_allclose(s, w[1], rtol=1e-12, atol=0)
     finally:
         L.voxel_scan_groupby_tune(-1)
 
@@ -120,7 +140,7 @@ def test_negative_and_mixed_sign_values_are_exact():
     exact = np.array([math.fsum(prod[d["idx"] == i]) for i in range(d["dict"].size)])
     exact = exact[np.bincount(d["idx"], minlength=d["dict"].size) > 0]
     try:
-        for v in (4, 1, 3):
+        for v in (4, 1, 3, 6):
             assert L.voxel_scan_groupby_tune(v) == 0
             k, s, mn, mx, c = gpu_scan_groupby(d, -np.inf, -1000, 1000)
             assert (k == w[0]).all() and (c == w[4]).all() and (mn == w[2]).all() and (mx == w[3]).all()
