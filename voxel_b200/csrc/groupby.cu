@@ -141,28 +141,38 @@ __device__ __forceinline__ bool row_words(double x, RowWords* w) {
     return true;
 }
 
+// Carry (+1) or borrow (-1) into word j and upwards while words wrap: rare
+// (the first level is handled inline below).
+__device__ __noinline__ void words_ripple(uint32_t* acc, int j, uint32_t step, uint32_t wrap) {
+    while (j < kWords && atomicAdd(&acc[j], step) == wrap) ++j;
+}
+
 // Adds (neg: subtracts) a row's words to a group accumulator: the three
-// atomics are issued back to back, then each one's own wrap (read from its
-// returned old value) ripples into the next word, and further up while that
-// word wraps too.  Every wrap is accounted exactly once, so concurrent updates
-// compose to the exact sum (modulo 2^160; no true sum needs more).  The
-// pending wraps are walked in one inline loop (a call per wrap cost more).
+// atomics are issued back to back, each one's own wrap (read from its
+// returned old value) goes into the next word, and a wrap of that word
+// ripples further up.  Every wrap is accounted exactly once, so concurrent
+// updates compose to the exact sum (modulo 2^160; no true sum needs more).
+// MAYNEG = false: the caller knows every value of the warp is >= 0.
+template <bool MAYNEG = true>
 __device__ __forceinline__ void words_add(uint32_t* acc, const RowWords& w, bool neg) {
+    if (!MAYNEG) neg = false;
     const uint32_t d0 = neg ? 0u - w.c0 : w.c0, d1 = neg ? 0u - w.c1 : w.c1, d2 = neg ? 0u - w.c2 : w.c2;
     uint32_t o0 = 0, o1 = 0, o2 = 0;
     if (w.c0) o0 = atomicAdd(&acc[w.k0], d0);
     if (w.c1) o1 = atomicAdd(&acc[w.k0 + 1], d1);
     if (w.c2) o2 = atomicAdd(&acc[w.k0 + 2], d2);
     // add: carry when old + c wraps; subtract: borrow when old < c
-    uint32_t pend = (w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0)) ? 2u : 0u;
-    pend |= (w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1)) ? 4u : 0u;
-    pend |= (w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2)) ? 8u : 0u;
+    const bool r0 = w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0);
+    const bool r1 = w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1);
+    const bool r2 = w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2) && w.k0 + 3 < kWords;
     const uint32_t step = neg ? 0xFFFFFFFFu : 1u, wrap = neg ? 0u : 0xFFFFFFFFu;
-    while (pend) {
-        int j = w.k0 + __ffs(pend) - 1;
-        pend &= pend - 1;
-        while (j < kWords && atomicAdd(&acc[j], step) == wrap) ++j;
-    }
+    bool x0 = false, x1 = false, x2 = false;
+    if (r0) x0 = atomicAdd(&acc[w.k0 + 1], step) == wrap;
+    if (r1) x1 = atomicAdd(&acc[w.k0 + 2], step) == wrap;
+    if (r2) x2 = atomicAdd(&acc[w.k0 + 3], step) == wrap;
+    if (x0) words_ripple(acc, w.k0 + 2, step, wrap);
+    if (x1) words_ripple(acc, w.k0 + 3, step, wrap);
+    if (x2) words_ripple(acc, w.k0 + 4, step, wrap);
 }
 
 // 160-bit two's complement (5 words) -> 192-bit.
@@ -269,14 +279,15 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
     // instead of one per row, and no two lanes of an atomic hit one address.
     // MODE 1, 2: a row is added by its own lane; same-address lanes are handled
     // by the shared-memory atomic unit (32-bit atomics stay fast under conflicts)
-    auto add_row = [&](uint32_t gi, double v, double p) {
+    auto add_row = [&](uint32_t gi, double v, double p, bool mayneg) {
         if (gi >= card) {
             bad_key = true;
             return;
         }
         RowWords w;
-        if (row_words(v, &w)) words_add(s_w + kWords * gi, w, v < 0.0);
-        else bad_value = true;
+        if (!row_words(v, &w)) bad_value = true;
+        else if (mayneg) words_add<true>(s_w + kWords * gi, w, v < 0.0);
+        else words_add<false>(s_w + kWords * gi, w, false);
         atomicAdd(&s_cnt[gi], 1u);
         const uint64_t k = f64_order_key(p);
         if (k < s_mn[gi]) atomicMin(&s_mn[gi], static_cast<unsigned long long>(k));
@@ -294,7 +305,9 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
             v = __dmul_rn(p, static_cast<double>(Q.qty[e]));
         }
         if (WORDS) {
-            if (valid) add_row(gi, v, p);
+            // one warp-uniform test picks the add-only path for the whole warp
+            const bool mayneg = __any_sync(0xffffffffu, valid && v < 0.0);
+            if (valid) add_row(gi, v, p, mayneg);
             return;
         }
         if (valid && gi >= card) {
@@ -373,7 +386,7 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
             const int32_t q = qv[k];
             const bool pass = p > pcut && static_cast<uint32_t>(q) - static_cast<uint32_t>(qlo) <= qspan;
             if (MODE == 2) {  // no queue: passing lanes add their rows directly
-                if (pass) add_row(key_bits(packed, r, width, mask), __dmul_rn(p, static_cast<double>(q)), p);
+                if (pass) add_row(key_bits(packed, r, width, mask), __dmul_rn(p, static_cast<double>(q)), p, true);
                 continue;
             }
             unsigned m = __ballot_sync(0xffffffffu, pass);

@@ -220,23 +220,32 @@ __device__ __forceinline__ bool words96(double x, Words96* w) {
     return true;
 }
 
-// Adds (neg: subtracts) the row's words, then walks each wrap upward in one
-// inline loop (exact under any interleaving of concurrent rows).
+// Carry (+1) or borrow (-1) into word j and upwards while words wrap: rare
+// (the first level is handled inline below).
+__device__ __noinline__ void ripple96(uint32_t* acc, int j, uint32_t step, uint32_t wrap) {
+    while (j < kAccWords && atomicAdd(&acc[j], step) == wrap) ++j;
+}
+
+// Adds (neg: subtracts) the row's words; each word's wrap goes into the next
+// word inline and ripples further only when that word wraps too (exact under
+// any interleaving of concurrent rows).
 __device__ __forceinline__ void add96(uint32_t* acc, const Words96& w, bool neg) {
     const uint32_t d0 = neg ? 0u - w.c0 : w.c0, d1 = neg ? 0u - w.c1 : w.c1, d2 = neg ? 0u - w.c2 : w.c2;
     uint32_t o0 = 0, o1 = 0, o2 = 0;
     if (w.c0) o0 = atomicAdd(&acc[w.k0], d0);
     if (w.c1) o1 = atomicAdd(&acc[w.k0 + 1], d1);
     if (w.c2) o2 = atomicAdd(&acc[w.k0 + 2], d2);
-    uint32_t pend = (w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0)) ? 2u : 0u;
-    pend |= (w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1)) ? 4u : 0u;
-    pend |= (w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2)) ? 8u : 0u;
+    const bool r0 = w.c0 && (neg ? o0 < w.c0 : o0 + w.c0 < o0);
+    const bool r1 = w.c1 && (neg ? o1 < w.c1 : o1 + w.c1 < o1);
+    const bool r2 = w.c2 && (neg ? o2 < w.c2 : o2 + w.c2 < o2) && w.k0 + 3 < kAccWords;
     const uint32_t step = neg ? 0xFFFFFFFFu : 1u, wrap = neg ? 0u : 0xFFFFFFFFu;
-    while (pend) {
-        int j = w.k0 + __ffs(pend) - 1;
-        pend &= pend - 1;
-        while (j < kAccWords && atomicAdd(&acc[j], step) == wrap) ++j;
-    }
+    bool x0 = false, x1 = false, x2 = false;
+    if (r0) x0 = atomicAdd(&acc[w.k0 + 1], step) == wrap;
+    if (r1) x1 = atomicAdd(&acc[w.k0 + 2], step) == wrap;
+    if (r2) x2 = atomicAdd(&acc[w.k0 + 3], step) == wrap;
+    if (x0) ripple96(acc, w.k0 + 2, step, wrap);
+    if (x1) ripple96(acc, w.k0 + 3, step, wrap);
+    if (x2) ripple96(acc, w.k0 + 4, step, wrap);
 }
 
 __global__ void __launch_bounds__(512) accumulate_smem_kernel(Table t, const uint32_t* __restrict__ keys,
