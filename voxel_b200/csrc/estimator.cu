@@ -101,12 +101,23 @@ __global__ void minmax_hll_kernel(const T* __restrict__ col, uint64_t n, unsigne
         if (sh[i]) atomicMax(&hll[i], sh[i]);
 }
 
+// order key (minmax_hll_kernel's okey) -> the double
+__host__ __device__ __forceinline__ double from_order_key(unsigned long long k) {
+    const uint64_t b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    double x;
+    memcpy(&x, &b, 8);
+    return x;
+}
+
+// bins [lo, hi] (read from the min / max order keys the first pass left in
+// device memory, so no host round trip sits between the passes) in 64 equal widths
 template <typename T>
-__global__ void histogram64_kernel(const T* __restrict__ col, uint64_t n, double lo, double hi,
-                                   unsigned long long* hist) {
+__global__ void histogram64_kernel(const T* __restrict__ col, uint64_t n, const unsigned long long* mnk,
+                                   const unsigned long long* mxk, unsigned long long* hist) {
     __shared__ unsigned int sh[kHistBins];
     if (threadIdx.x < kHistBins) sh[threadIdx.x] = 0;
     __syncthreads();
+    const double lo = from_order_key(*mnk), hi = from_order_key(*mxk);
     double w = hi > lo ? (hi - lo) / kHistBins : 1.0;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
@@ -397,39 +408,41 @@ int sgrid(uint64_t n, int per_sm = 4) {
 
 template <typename T>
 int sketch_t(const T* d, uint64_t n, ColumnSketch* out, cudaStream_t s) {
-    DevBuf buf(16 + kHllRegs * 4 + kHistBins * 8);
+    // [min key, max key][HLL registers][histogram], kept between calls; one
+    // read-back at the end
+    constexpr size_t kBytes = 16 + kHllRegs * 4 + kHistBins * 8;
+    static thread_local DevBuf buf;
+    if (!buf.p) buf = DevBuf(kBytes);
     if (!buf.p) return kErrOutOfMemory;
     unsigned long long* mm = buf.as<unsigned long long>();
     unsigned int* hll = reinterpret_cast<unsigned int*>(mm + 2);
     unsigned long long* hist = reinterpret_cast<unsigned long long*>(hll + kHllRegs);
-    unsigned long long init[2] = {~0ull, 0ull};
-    if (int st = h2d(mm, init, 16, s)) return st;
-    VX_CUDA(cudaMemsetAsync(hll, 0, kHllRegs * 4 + kHistBins * 8, s));
+    VX_CUDA(cudaMemsetAsync(mm, 0xFF, 8, s));
+    VX_CUDA(cudaMemsetAsync(mm + 1, 0, kBytes - 8, s));
     out->n = n;
     if (n) {
         minmax_hll_kernel<T><<<sgrid(n, 8), 256, 0, s>>>(d, n, mm, mm + 1, hll);
         VX_CUDA(cudaGetLastError());
-        unsigned long long h[2];
-        if (int st = d2h(h, mm, 16, s)) return st;
-        if (int st = sync(s)) return st;
-        auto dec = [](unsigned long long k) {
-            uint64_t b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
-            double x;
-            std::memcpy(&x, &b, 8);
-            return x;
-        };
-        out->min = dec(h[0]);
-        out->max = dec(h[1]);
-        histogram64_kernel<T><<<sgrid(n, 8), 256, 0, s>>>(d, n, out->min, out->max, hist);
+        histogram64_kernel<T><<<sgrid(n, 8), 256, 0, s>>>(d, n, mm, mm + 1, hist);
         VX_CUDA(cudaGetLastError());
+    }
+    std::vector<unsigned char> h(kBytes);
+    if (int st = d2h(h.data(), buf.p, kBytes, s)) return st;
+    if (int st = sync(s)) return st;
+    if (n) {
+        unsigned long long k[2];
+        std::memcpy(k, h.data(), 16);
+        out->min = from_order_key(k[0]);
+        out->max = from_order_key(k[1]);
     } else {
         out->min = out->max = 0.0;
     }
-    std::vector<unsigned int> regs(kHllRegs);
-    if (int st = d2h(regs.data(), hll, kHllRegs * 4, s)) return st;
-    if (int st = d2h(out->hist, hist, kHistBins * 8, s)) return st;
-    if (int st = sync(s)) return st;
-    for (int i = 0; i < kHllRegs; ++i) out->hll[i] = static_cast<uint8_t>(regs[i]);
+    std::memcpy(out->hist, h.data() + 16 + kHllRegs * 4, kHistBins * 8);
+    for (int i = 0; i < kHllRegs; ++i) {
+        unsigned int r;
+        std::memcpy(&r, h.data() + 16 + i * 4, 4);
+        out->hll[i] = static_cast<uint8_t>(r);
+    }
     return kOk;
 }
 
