@@ -2,6 +2,7 @@
 #include "tune.h"
 
 #include <dlfcn.h>
+#include <unistd.h>
 
 #include <cmath>
 #include <cstdio>
@@ -63,7 +64,9 @@ void load_locked() {
 
 void save_locked() {
     if (g_path.empty()) g_path = default_path();
-    const std::string tmp = g_path + ".tmp";
+    // a temporary name of this process's own, so processes saving at once
+    // never write into one file; the rename then replaces the cache whole
+    const std::string tmp = g_path + "." + std::to_string(static_cast<long>(getpid())) + ".tmp";
     FILE* f = std::fopen(tmp.c_str(), "w");
     if (!f) return;  // an unwritable cache only costs re-tuning in the next process
     std::fputs("{\n", f);
