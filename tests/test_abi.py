@@ -164,3 +164,16 @@ def test_tune_cache_file_round_trip(lib, tmp_path):
         assert json.loads(path.read_text()) == {}
     finally:
         lib.voxel_tune_set_cache_path(None)
+
+
+def test_scan_groupby_variant_selection(lib):
+    """The fused scan's variant switch accepts exactly the documented ids
+    (-1 autotuned, 0 TMA-fed, 1/2 and 3/5 word table, 6 bulk-copy-fed word
+    table, 4/8/16 warp-merged) and rejects others; no device work is involved."""
+    try:
+        for v in (-1, 0, 1, 2, 3, 4, 5, 6, 8, 16):
+            assert lib.voxel_scan_groupby_tune(v) == 0, v
+        for v in (-2, 7, 9, 12, 32):
+            assert lib.voxel_scan_groupby_tune(v) != 0, v
+    finally:
+        lib.voxel_scan_groupby_tune(-1)
