@@ -31,7 +31,7 @@ def _outputs(card):
                 ngroups=torch.zeros(1, dtype=torch.int64, device=DEV))
 
 
-def _call(noalloc, d, t, pthr=20.0, qlo=10, qhi=50, card=None):
+def _call(noalloc, d, t, pthr=20.0, qlo=10, qhi=50, card=None, want_status=0):
     L = capi.lib()
     card = d["dict"].size if card is None else card
     o = _outputs(max(card, 1))
@@ -48,7 +48,7 @@ def _call(noalloc, d, t, pthr=20.0, qlo=10, qhi=50, card=None):
         return st, None
     torch.cuda.synchronize()
     if noalloc:
-        assert int(status[0]) == 0
+        assert int(status[0]) == want_status
     g = int(o["ngroups"][0])
     return 0, {k: v[:g].cpu().numpy() for k, v in o.items() if k != "ngroups"}
 
@@ -90,4 +90,31 @@ def test_noalloc_rejects_dictionary_beyond_its_scratch():
     st, want = _call(False, d, t)
     st2, got = _call(True, d, t)
     assert st == 0 and st2 == 0
+    _same(got, want)
+
+
+def test_noalloc_table_recovers_after_flagged_calls():
+    """A call that flags a key outside the dictionary (status bit 2) or a
+    product that is not finite (bit 1) still leaves the shared table at rest:
+    the next valid call is bit-identical to the allocating entry point."""
+    L = capi.lib()
+    d, t = _device_case(200_000, 16, 300)
+    st, want = _call(False, d, t)
+    assert st == 0, capi.last_error()
+    # a dictionary shorter than the packed indices need
+    st, _ = _call(True, d, t, card=150, want_status=2)
+    assert st == 0
+    assert L.voxel_scan_groupby_status_code(2) == 1 and "dictionary" in capi.last_error()
+    st, got = _call(True, d, t)
+    assert st == 0, capi.last_error()
+    _same(got, want)
+    # an infinite price passes "price > 20" and makes a non-finite product
+    bad = t["price"].clone()
+    bad[1234] = float("inf")
+    tb = dict(t, price=bad)
+    st, _ = _call(True, d, tb, want_status=1)
+    assert st == 0
+    assert L.voxel_scan_groupby_status_code(1) == 7
+    st, got = _call(True, d, t)
+    assert st == 0, capi.last_error()
     _same(got, want)

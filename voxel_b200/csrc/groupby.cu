@@ -1183,20 +1183,37 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
 #undef VX_LAUNCH_RPT
 }
 
+// Status word bits the fused scan kernels OR in: 4 a bounded bulk-copy wait ran
+// out (the group rows are partial), 2 a key index outside the dictionary, 1 a
+// product that is not finite or beyond 2^63.  The most serious bit wins.
+int groupby_status_error(int h) {
+    if (!h) return kOk;
+    if (h & 4) {
+        set_error(kErrDeviceTimeout, "a bulk-copy wait in the fused scan ran out of its budget; the group rows are partial");
+        return kErrDeviceTimeout;
+    }
+    if (h & 2) {
+        set_error(kErrInvalidArg, "a packed key index is outside the dictionary");
+        return kErrInvalidArg;
+    }
+    if (h & 1) {
+        set_error(kErrOverflow, "a price*qty product is not finite or exceeds 2^63 in magnitude");
+        return kErrOverflow;
+    }
+    set_error(kErrInvalidArg, "unknown fused-scan status bits 0x%x", static_cast<unsigned>(h));
+    return kErrInvalidArg;
+}
+
 int ScanGroupBy::check_status(cudaStream_t s) {
+    if (!status.p) return kOk;  // nothing launched on this thread yet
     int h = 0;
     int st = d2h(&h, status.p, sizeof(int), s);
     if (st) return st;
     st = sync(s);
     if (st) return st;
     if (h) {
-        cudaMemsetAsync(status.p, 0, 16, s);
-        if (h & 2) {
-            set_error(kErrInvalidArg, "a packed key index is outside the dictionary");
-            return kErrInvalidArg;
-        }
-        set_error(kErrOverflow, "a price*qty product is not finite or exceeds 2^63 in magnitude");
-        return kErrOverflow;
+        VX_CUDA(cudaMemsetAsync(status.p, 0, 16, s));
+        return groupby_status_error(h);
     }
     return kOk;
 }
@@ -1281,6 +1298,13 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
 }
 
 int voxel_scan_groupby_tune(int variant) {
+    clear_error();
+    // validate before touching the state: a rejected id leaves the previous choice in place
+    const bool known = variant == -1 || (variant >= 0 && variant <= 6) || variant == 8 || variant == 16;
+    if (!known) {
+        set_error(kErrInvalidArg, "unknown fused-scan variant %d", variant);
+        return kErrInvalidArg;
+    }
     ScanGroupBy& S = scan_groupby_state();
     S.autotune = variant == -1;  // -1: the autotuner's choice per shape (word table + queue, 4 rows, untuned)
     if (variant == -1) variant = 1;
@@ -1308,11 +1332,30 @@ int voxel_scan_groupby_tune(int variant) {
         S.rows_per_thread = variant == 3 ? 4 : 8;
         return kOk;
     }
-    if (variant != 4 && variant != 8 && variant != 16) return kErrInvalidArg;
-    S.use_tma = false;
+    S.use_tma = false;  // 4, 8, 16: warp-merged rows
     S.mode = 0;
     S.rows_per_thread = variant;
     return kOk;
+}
+
+int voxel_scan_groupby_tune_state(void) {
+    const ScanGroupBy& S = scan_groupby_state();
+    if (S.autotune) return -1;
+    if (S.use_tma) return 0;
+    if (S.use_tw) return 6;
+    if (S.mode == 1) return S.rows_per_thread == 8 ? 2 : 1;
+    if (S.mode == 2) return S.rows_per_thread == 8 ? 5 : 3;
+    return S.rows_per_thread;
+}
+
+int voxel_scan_groupby_status_code(int status_word) {
+    clear_error();
+    return groupby_status_error(status_word);
+}
+
+int voxel_scan_groupby_check(void* stream) {
+    clear_error();
+    return scan_groupby_state().check_status(static_cast<cudaStream_t>(stream));
 }
 
 int voxel_scan_groupby_last_variant(void) { return scan_groupby_state().last_kernel; }

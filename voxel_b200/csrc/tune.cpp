@@ -74,14 +74,19 @@ void save_locked() {
     for (const auto& e : g_cache)
         std::fprintf(f, "  \"%s\": %d%s\n", e.first.c_str(), e.second, ++k < g_cache.size() ? "," : "");
     std::fputs("}\n", f);
-    std::fclose(f);
+    // a short write (full disk) must not replace a good cache with a truncated one
+    const bool write_failed = std::ferror(f) != 0;
+    const bool close_failed = std::fclose(f) != 0;
+    if (write_failed || close_failed) {
+        std::remove(tmp.c_str());
+        return;
+    }
     std::rename(tmp.c_str(), g_path.c_str());
 }
 
-std::string gpu_name() {
-    int dev = 0;
+std::string gpu_name(int dev) {
     cudaDeviceProp p{};
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
         cudaGetLastError();
         return "unknown";
     }
@@ -96,7 +101,21 @@ std::string gpu_name() {
 std::string tune_key(const char* family, int dtype, uint64_t n) {
     int lg = 0;
     while (lg < 63 && (1ull << (lg + 1)) <= n) ++lg;  // floor(log2 n)
-    static const std::string gpu = gpu_name();
+    // the GPU part of the key belongs to the calling thread's current device
+    constexpr int kDevs = 64;
+    static std::string names[kDevs];
+    static std::mutex names_mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = -1;
+    }
+    std::string gpu = "unknown";
+    if (dev >= 0 && dev < kDevs) {
+        std::lock_guard<std::mutex> lk(names_mu);
+        if (names[dev].empty()) names[dev] = gpu_name(dev);
+        gpu = names[dev];
+    }
     return gpu + "|" + family + "|" + std::to_string(dtype) + "|" + std::to_string(lg);
 }
 

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <atomic>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -92,7 +93,23 @@ int ensure_device() {
 
 int sm_count() {
     if (ensure_device() != kOk) return 0;
-    return g_sms;
+    // per device ordinal: grid sizing follows the calling thread's current device
+    constexpr int kDevs = 64;
+    static std::atomic<int> per_dev[kDevs];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) {
+        cudaGetLastError();
+        return g_sms;
+    }
+    int v = per_dev[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+            cudaGetLastError();
+            return g_sms;
+        }
+        per_dev[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
 }
 
 void* dev_alloc(size_t bytes) {
