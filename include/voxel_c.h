@@ -236,6 +236,35 @@ int       voxel_rle_decode_i64_dev(const int64_t* d_values, const uint32_t* d_ru
                                    size_t offset, size_t count, int64_t* d_out, void* stream);
 /* device variants of the dictionary decoders; they return after the kernel
  * (an index outside the dictionary is reported as VOXEL_EINVAL) */
+/* ================================================================
+ * Additive: delta and frame-of-reference codecs.
+ * DeltaEncoding<T> (reference data/encoding.hpp:281-354), T an integer type
+ * (dtype 2 i64, 3 i32, 4 u64, 5 u32; base_bits = BaseValue's bits):
+ *   decode: out[i] = base + deltas[0] + ... + deltas[offset + i], wrapping in
+ *   T, for i < count and offset + i < n (DecodeBatch, 317-330); outputs past n
+ *   are not written.  encode: deltas[i] = data[i] - data[i-1], data[-1] = 0
+ *   (Build, 292-306; BaseValue 0).
+ * FrameOfReferenceEncoding (encoding.hpp:456-521), f64 values as i32 codes:
+ *   decode: out[i] = base + (double)code[offset + i] * scale, one rounding per
+ *   operation, for offset + i < n (DecodeBatch, 489-500).  encode: base = min,
+ *   scale = (max - min) / INT32_MAX (1 when max == min), code =
+ *   (int32)llround((x - base) / scale) (Build, 461-482); NaN-free columns.
+ * Return 0 or a VOXEL_E* code.
+ * ================================================================ */
+int       voxel_delta_decode(int dtype, const void* deltas, size_t n, uint64_t base_bits, size_t offset,
+                             size_t count, void* out);
+int       voxel_delta_decode_dev(int dtype, const void* d_deltas, size_t n, uint64_t base_bits, size_t offset,
+                                 size_t count, void* d_out, void* stream);
+int       voxel_delta_encode(int dtype, const void* data, size_t n, void* deltas);
+int       voxel_delta_encode_dev(int dtype, const void* d_data, size_t n, void* d_deltas, void* stream);
+int       voxel_for_decode_f64(const int32_t* code, size_t n, double base, double scale, size_t offset,
+                               size_t count, double* out);
+int       voxel_for_decode_f64_dev(const int32_t* d_code, size_t n, double base, double scale, size_t offset,
+                                   size_t count, double* d_out, void* stream);
+int       voxel_for_encode_f64(const double* data, size_t n, int32_t* code, double* base, double* scale);
+/* base / scale are host outputs; the call synchronises `stream` once (min / max) */
+int       voxel_for_encode_f64_dev(const double* d_data, size_t n, int32_t* d_code, double* base, double* scale,
+                                   void* stream);
 int       voxel_dict_bitpack_decode_i32_dev(const uint64_t* d_words, size_t nwords, uint32_t width,
                                             const int32_t* d_dict, size_t card, size_t value_count,
                                             size_t offset, size_t count, int32_t* d_out, void* stream);
@@ -273,6 +302,20 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  * with queue, 3 word table direct, 4 word table fed by bulk copies. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
+/* the calling thread's current variant id (as passed to voxel_scan_groupby_tune) */
+int       voxel_scan_groupby_tune_state(void);
+/* Errors of the device-pointer fused scan.  The kernels OR bits into a device
+ * status word: 1 = a price*qty product not finite or beyond 2^63, 2 = a packed
+ * key index outside the dictionary, 4 = a bounded bulk-copy wait ran out
+ * (variants 0 and 6 only; the group rows are then partial).
+ * voxel_scan_groupby_check synchronises `stream`, reads and clears the calling
+ * thread's status word of voxel_scan_groupby_dev and returns VOXEL_OK, or
+ * VOXEL_ETIMEOUT (bit 4), VOXEL_EINVAL (bit 2), VOXEL_EOVERFLOW (bit 1), with
+ * voxel_last_error() set.  voxel_scan_groupby_status_code maps a status word
+ * the caller read itself (the *d_status of voxel_scan_groupby_noalloc_dev) the
+ * same way. */
+int       voxel_scan_groupby_check(void* stream);
+int       voxel_scan_groupby_status_code(int status_word);
 /* Autotuner (no reference counterpart): kernel families with several
  * equivalent configurations (the fused scan's variants, the radix sort's
  * keys per thread) time them on the first call of each (GPU, element type,

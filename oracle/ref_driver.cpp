@@ -163,6 +163,21 @@ void group_chunk(GroupPipe& p, const encoding::BitPackedEncoding& keyPack,
 
 }  // namespace
 
+// encoding.hpp:281-354 (DeltaEncoding<T>::Build, DecodeBatch); returns BaseValue's bits
+template <typename T>
+uint64_t delta_build_t(const T* data, size_t n, T* deltas) {
+    encoding::DeltaEncoding<T> e;
+    e.Build(data, n);
+    if (!e.Deltas.empty()) std::memcpy(deltas, e.Deltas.data(), e.Deltas.size() * sizeof(T));
+    return static_cast<uint64_t>(e.BaseValue);
+}
+template <typename T>
+void delta_decode_t(const T* deltas, size_t n, uint64_t base, size_t offset, size_t count, T* out) {
+    encoding::DeltaEncoding<T> e;
+    e.BaseValue = static_cast<T>(base);
+    e.Deltas.assign(deltas, deltas + n);
+    e.DecodeBatch(out, offset, count);
+}
 extern "C" {
 
 int vref_engine_run(int dtype, const uint32_t* code, size_t len, const void* const* segs,
@@ -244,6 +259,37 @@ double vref_time_filter_sum_f64(int mode, const uint32_t* code, size_t len,
             res = std::bit_cast<f64>(rf.Scalar(0));
         }
         compiler->Release(func);
+    } else if (mode == 3) {
+        // Engine<f64>::Run on `threads` row chunks at once (each a multiple of
+        // kLanes, R2 = its own row count), for programs outside the fast path
+        // where RunParallel would loop every worker over all rows; the
+        // accumulator R0 is the sum of the chunks' R0.
+        const sz kl = Engine<f64>::kLanes;
+        const sz per = ((n / threads) / kl) * kl;
+        for (int i = 0; i < warmup + runs; ++i) {
+            std::vector<Engine<f64>> w(threads);
+            std::vector<std::thread> th;
+            double t0 = now_us();
+            for (u32 k = 0; k < threads; ++k) {
+                th.emplace_back([&, k] {
+                    const sz start = k * per;
+                    const sz cnt = k + 1 == threads ? ((n - start) / kl) * kl : per;
+                    Engine<f64>& e = w[k];
+                    e.AddSegment(const_cast<double*>(data) + start, cnt);
+                    e.ScalarReg(0) = 0; e.ScalarReg(1) = 0; e.ScalarReg(2) = cnt;
+                    e.ScalarReg(3) = std::bit_cast<u64>(threshold);
+                    e.ScalarReg(4) = kl;
+                    for (sz r = 5; r < 16; ++r) e.ScalarReg(r) = 0;
+                    e.LoadProgram(v);
+                    e.Run();
+                });
+            }
+            for (auto& x : th) x.join();
+            double t1 = now_us();
+            if (i >= warmup) t.push_back(t1 - t0);
+            res = 0;
+            for (u32 k = 0; k < threads; ++k) res += std::bit_cast<f64>(w[k].ScalarReg(0));
+        }
     } else {
         Engine<f64> e;
         e.AddSegment(const_cast<double*>(data), n);
@@ -270,6 +316,41 @@ size_t vref_vfilter_i64(int op, const int64_t* d, size_t n, int64_t a, int64_t b
 size_t vref_vfilter_i32(int op, const int32_t* d, size_t n, int32_t a, int32_t b, uint64_t* bm) { return vfilter_t<i32>(op, d, n, a, b, bm); }
 size_t vref_vfilter_u64(int op, const uint64_t* d, size_t n, uint64_t a, uint64_t b, uint64_t* bm) { return vfilter_t<u64>(op, d, n, a, b, bm); }
 size_t vref_vfilter_u32(int op, const uint32_t* d, size_t n, uint32_t a, uint32_t b, uint64_t* bm) { return vfilter_t<u32>(op, d, n, a, b, bm); }
+
+// simd/scalar.hpp:214-227 (scalar_filter_gt_f32): values > threshold, compacted in row order
+size_t vref_scalar_filter_gt_f32(float* dst, const float* src, float threshold, size_t n) {
+    return simd::scalar::scalar_filter_gt_f32(dst, src, threshold, n);
+}
+
+// simd/scalar.hpp:229-238 (scalar_sum_f32): 8 f32 lane accumulators, then the tail
+float vref_scalar_sum_f32(const float* src, size_t n) { return simd::scalar::scalar_sum_f32(src, n); }
+
+// encoding.hpp:281-354 (DeltaEncoding<T>): the helpers sit before the extern "C" block
+uint64_t vref_delta_build_i64(const int64_t* d, size_t n, int64_t* o) { return delta_build_t<i64>(d, n, o); }
+uint64_t vref_delta_build_i32(const int32_t* d, size_t n, int32_t* o) { return delta_build_t<i32>(d, n, o); }
+uint64_t vref_delta_build_u64(const uint64_t* d, size_t n, uint64_t* o) { return delta_build_t<u64>(d, n, o); }
+uint64_t vref_delta_build_u32(const uint32_t* d, size_t n, uint32_t* o) { return delta_build_t<u32>(d, n, o); }
+void vref_delta_decode_i64(const int64_t* d, size_t n, uint64_t b, size_t off, size_t c, int64_t* o) { delta_decode_t<i64>(d, n, b, off, c, o); }
+void vref_delta_decode_i32(const int32_t* d, size_t n, uint64_t b, size_t off, size_t c, int32_t* o) { delta_decode_t<i32>(d, n, b, off, c, o); }
+void vref_delta_decode_u64(const uint64_t* d, size_t n, uint64_t b, size_t off, size_t c, uint64_t* o) { delta_decode_t<u64>(d, n, b, off, c, o); }
+void vref_delta_decode_u32(const uint32_t* d, size_t n, uint64_t b, size_t off, size_t c, uint32_t* o) { delta_decode_t<u32>(d, n, b, off, c, o); }
+
+// encoding.hpp:456-521 (FrameOfReferenceEncoding::Build, DecodeBatch)
+void vref_for_build_f64(const double* d, size_t n, int32_t* codes, double* base, double* scale) {
+    encoding::FrameOfReferenceEncoding e;
+    e.Build(d, n);
+    if (!e.EncodedValues.empty()) std::memcpy(codes, e.EncodedValues.data(), e.EncodedValues.size() * 4);
+    *base = e.BaseValue;
+    *scale = e.Scale;
+}
+void vref_for_decode_f64(const int32_t* codes, size_t n, double base, double scale, size_t offset, size_t count,
+                         double* out) {
+    encoding::FrameOfReferenceEncoding e;
+    e.BaseValue = base;
+    e.Scale = scale;
+    e.EncodedValues.assign(codes, codes + n);
+    e.DecodeBatch(out, offset, count);
+}
 
 // filter.hpp:378-399 (SelectionVector::BuildFromBitmap)
 size_t vref_selection_from_bitmap(const uint64_t* bm, size_t rows, uint32_t* out) {

@@ -89,6 +89,23 @@ def test_plan_count_loop():
     st, s = plan(0, bc.filter_sum_count_program(), [x], [0, 0, 1000, T.reg_image(0, 500.0), 4, 0, 0])
     assert st == 0 and s.startswith("loop") and "groups=250" in s
     assert "r0=sum/addf" in s and "r1=count/add" in s
+    assert "kernel=fsum" in s  # SUM + COUNT of one compare: the fused filter+sum kernel with its count
+
+
+def test_plan_multi_aggregate_templates():
+    """One predicate set with 2-4 aggregates plans onto the multi-reduction
+    range kernel for every element type; one aggregate stays on the
+    single-reduction kernels."""
+    rng = np.random.default_rng(4)
+    for dt in range(6):
+        for aggs in (["SUM", "COUNT"], ["SUM", "COUNT", "MIN", "MAX"], ["MIN", "MAX"]):
+            base = T.random_program(dt, rng, npreds=int(rng.integers(1, 5)))
+            prog = T.build_multi(dt, base.preds, aggs)
+            st, s = plan(dt, prog.code, [T.make_column(dt, 64, rng)], prog.registers(64))
+            assert st == 0 and "kernel=mrange" in s, (dt, aggs, s)
+        prog = T.build_multi(dt, base.preds, ["MAX"])
+        st, s = plan(dt, prog.code, [T.make_column(dt, 64, rng)], prog.registers(64))
+        assert st == 0 and "kernel=range" in s, s
 
 
 def test_plan_templates_all_types():
@@ -175,5 +192,24 @@ def test_scan_groupby_variant_selection(lib):
             assert lib.voxel_scan_groupby_tune(v) == 0, v
         for v in (-2, 7, 9, 12, 32):
             assert lib.voxel_scan_groupby_tune(v) != 0, v
+        # a rejected id leaves the previous choice in place
+        assert lib.voxel_scan_groupby_tune(3) == 0
+        assert lib.voxel_scan_groupby_tune(7) != 0
+        assert lib.voxel_scan_groupby_tune_state() == 3
+        assert lib.voxel_scan_groupby_tune(-1) == 0
+        assert lib.voxel_scan_groupby_tune(12) != 0
+        assert lib.voxel_scan_groupby_tune_state() == -1
     finally:
         lib.voxel_scan_groupby_tune(-1)
+
+
+def test_scan_groupby_status_words(lib):
+    """Status words of the fused scan map to codes and messages on the host:
+    the bulk-copy timeout bit wins over the others and is reported as a
+    timeout, not an overflow."""
+    cases = [(0, 0, None), (1, 7, "not finite"), (2, 1, "dictionary"), (3, 1, "dictionary"),
+             (4, 6, "bulk-copy wait"), (5, 6, "bulk-copy wait"), (6, 6, "bulk-copy wait"), (8, 1, "unknown")]
+    for word, code, text in cases:
+        assert lib.voxel_scan_groupby_status_code(word) == code, word
+        if text:
+            assert text in capi.last_error(), (word, capi.last_error())

@@ -50,8 +50,12 @@ def assert_regs(dtype, code, got, want, rtol):
     for r in range(16):
         if got[r] == want[r]:
             continue
+        if dtype in (0, 1) and f64(got[r]) != f64(got[r]) and f64(want[r]) != f64(want[r]):
+            continue  # both NaN: the payload of a NaN register is not part of the result
         assert r in facc, f"R{r}: got {got[r]:#x} want {want[r]:#x}"
         g, w = f64(got[r]), f64(want[r])
+        if g != g and w != w:
+            continue  # both NaN: a NaN sum's payload is not part of the result
         assert abs(g - w) <= rtol * max(abs(w), 1e-300), f"R{r}: {g!r} vs {w!r}"
 
 
@@ -86,15 +90,22 @@ def test_config1_ground_truth(golden):
     assert abs(s - 375538740.218) < 1e-3  # docs/Benchmarks.md:7
     got, e = run_gpu(0, bc.filter_sum_count_program(), [x], regs + [0, 0])
     assert got[6] == 500720
+    # the SUM + COUNT program runs on the fused filter+sum kernel with its count, same sum
+    assert "kernel=fsum" in e.explain()
+    assert abs(f64(got[0]) - f64(c["sum_bits"])) <= F64_RTOL * s
     # jit_run entry point (voxel_c.cpp:80-101)
     code = np.asarray(bc.filter_sum_program(), np.uint32)
     j = capi.lib().voxel_jit_run(code.ctypes.data, code.size, x.ctypes.data, x.size, 500.0)
     assert abs(j - s) <= F64_RTOL * s
 
 
-def test_f32_programs_against_restatement():
+def test_f32_programs_against_reference_filters_and_restatement():
+    """f32 programs (no reference engine exists for f32): every register as
+    the restatement's, and the aggregates pinned to the rows the reference's
+    own VectorFilter<f32> + ColumnFilter select (COUNT, MIN, MAX exact; SUM
+    within 1e-6 relative)."""
     rng = np.random.default_rng(11)
-    for n in (8, 64, 1000, 4096, 65536):
+    for n in (8, 64, 1000, 4096, 65536, 1 << 20):
         col = T.make_column(T.F32, n, rng)
         for agg in T.AGGS:
             prog = T.random_program(T.F32, rng, agg=agg)
@@ -103,6 +114,22 @@ def test_f32_programs_against_restatement():
             assert st == 0
             got, _ = run_gpu(T.F32, prog.code, [col], regs)
             assert_regs(T.F32, prog.code, got, want[:16], F32_RTOL)
+            ref = oracle.f32_program_expect(prog.preds, [agg], col)[agg]
+            v = T.image_value(T.F32, got[0]) if agg != "COUNT" else got[0]
+            if agg == "SUM":
+                assert abs(v - ref) <= F32_RTOL * abs(ref) + 1e-30, (v, ref)
+            else:
+                assert v == ref, (agg, v, ref)
+        aggs = ["SUM", "COUNT", "MIN", "MAX"]
+        base = T.random_program(T.F32, rng, npreds=int(rng.integers(1, 5)))
+        prog = T.build_multi(T.F32, base.preds, aggs)
+        got, _ = run_gpu(T.F32, prog.code, [col], prog.registers(n))
+        ref = oracle.f32_program_expect(base.preds, aggs, col)
+        assert got[T.MULTI_ACC["COUNT"]] == ref["COUNT"]
+        assert T.image_value(T.F32, got[T.MULTI_ACC["MIN"]]) == ref["MIN"]
+        assert T.image_value(T.F32, got[T.MULTI_ACC["MAX"]]) == ref["MAX"]
+        s = T.image_value(T.F32, got[T.MULTI_ACC["SUM"]])
+        assert abs(s - ref["SUM"]) <= F32_RTOL * abs(ref["SUM"]) + 1e-30
         # fused fast path on f32 (f64 accumulation)
         code = bc.filter_sum_program()
         regs = [0, 0, n, T.reg_image(T.F32, 500.0), 8]
@@ -222,3 +249,59 @@ def test_unsupported_program_fails_loudly():
     with pytest.raises(VoxelError) as ei:
         e.run()
     assert ei.value.status == 2
+
+
+def test_multi_reduction_programs_against_reference():
+    """Programs with one predicate set and 2-4 aggregates (SUM, COUNT, MIN,
+    MAX of the same filter) run on the multi-reduction range kernel and give
+    the reference interpreter's registers (f32: the restatement's)."""
+    rng = np.random.default_rng(21)
+    combos = (["SUM", "COUNT"], ["SUM", "COUNT", "MIN", "MAX"], ["MIN", "MAX"], ["COUNT", "MAX", "SUM"],
+              ["MAX", "COUNT"])
+    for dt in range(6):
+        for aggs in combos:
+            for n in (8, 8 * int(rng.integers(2, 600)), 1 << 16, (1 << 20) + 8 * 37):
+                base = T.random_program(dt, rng, npreds=int(rng.integers(1, 5)))
+                prog = T.build_multi(dt, base.preds, aggs)
+                col = T.make_column(dt, n, rng)
+                regs = prog.registers(n)
+                if dt == T.F32:
+                    st, want, _ = oracle.engine_run_port(dt, prog.code, [col], regs)
+                    assert st == 0
+                else:
+                    want = oracle.engine_run_ref(dt, prog.code, [col], regs)
+                got, e = run_gpu(dt, prog.code, [col], regs)
+                assert "kernel=mrange" in e.explain(), e.explain()
+                assert_regs(dt, prog.code, got, want[:16], F32_RTOL if dt == T.F32 else F64_RTOL)
+
+
+def test_filter_sum_count_all_compares_against_reference():
+    """`filter x OP t; SUM(x); COUNT` for every element type and compare op,
+    with thresholds at zero, inside the data and NaN, over columns holding
+    zeros (and NaN for floats): the fused filter+sum kernel with its count
+    gives the reference interpreter's registers (f32: the restatement's)."""
+    rng = np.random.default_rng(22)
+    for dt in range(6):
+        kl = T.K_LANES[dt]
+        for op in range(6):
+            thresholds = [0, 500, 999] + ([-1] if dt in (T.F64, T.F32, T.I64, T.I32) else [])
+            if dt in (T.F64, T.F32):
+                thresholds.append(float("nan"))
+            for thr in thresholds:
+                n = kl * int(rng.integers(1, 5000))
+                col = T.make_column(dt, n, rng)
+                col[rng.random(n) < 0.05] = 0
+                if dt in (T.F64, T.F32):
+                    col[rng.random(n) < 0.02] = np.nan
+                fold = bc.addf(0, 0, 5) if dt in (T.F64, T.F32) else bc.add(0, 0, 5)
+                code = [bc.vload(0, 1, 0), bc.vfilter(op, 1, 0, 3), bc.vsum(5, 1), fold, bc.vcount(7, 1),
+                        bc.add(6, 6, 7), bc.add(1, 1, 4), bc.cmp(1, 2), bc.jnz(-8), bc.halt()]
+                regs = [0, 0, n, T.reg_image(dt, thr), kl, 0, 0]
+                if dt == T.F32:
+                    st, want, _ = oracle.engine_run_port(dt, code, [col], regs)
+                    assert st == 0
+                else:
+                    want = oracle.engine_run_ref(dt, code, [col], regs)
+                got, e = run_gpu(dt, code, [col], regs)
+                assert "kernel=fsum" in e.explain(), e.explain()
+                assert_regs(dt, code, got, want[:16], F32_RTOL if dt == T.F32 else F64_RTOL)

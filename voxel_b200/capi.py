@@ -127,6 +127,14 @@ _SIGS = {
     "voxel_dict_bitpack_decode_i32": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp]),
     "voxel_dict_decode": (C.c_int, [C.c_int, vp, sz, vp, sz, sz, sz, vp]),
     "voxel_rle_decode_i64": (C.c_int, [vp, vp, sz, sz, sz, vp]),
+    "voxel_delta_decode": (C.c_int, [C.c_int, vp, sz, u64, sz, sz, vp]),
+    "voxel_delta_decode_dev": (C.c_int, [C.c_int, vp, sz, u64, sz, sz, vp, vp]),
+    "voxel_delta_encode": (C.c_int, [C.c_int, vp, sz, vp]),
+    "voxel_delta_encode_dev": (C.c_int, [C.c_int, vp, sz, vp, vp]),
+    "voxel_for_decode_f64": (C.c_int, [vp, sz, dbl, dbl, sz, sz, vp]),
+    "voxel_for_decode_f64_dev": (C.c_int, [vp, sz, dbl, dbl, sz, sz, vp, vp]),
+    "voxel_for_encode_f64": (C.c_int, [vp, sz, vp, C.POINTER(dbl), C.POINTER(dbl)]),
+    "voxel_for_encode_f64_dev": (C.c_int, [vp, sz, vp, C.POINTER(dbl), C.POINTER(dbl), vp]),
     "voxel_bitpack_decode_dev": (C.c_int, [vp, sz, u32, sz, sz, sz, vp, vp]),
     "voxel_rle_decode_i64_dev": (C.c_int, [vp, vp, sz, sz, sz, vp, vp]),
     "voxel_dict_bitpack_decode_i32_dev": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp, vp]),
@@ -145,6 +153,9 @@ _SIGS = {
     "voxel_radix_sort_tmp_bytes": (sz, [C.c_int, sz]),
     "voxel_scan_groupby_tune": (C.c_int, [C.c_int]),
     "voxel_scan_groupby_last_variant": (C.c_int, []),
+    "voxel_scan_groupby_tune_state": (C.c_int, []),
+    "voxel_scan_groupby_check": (C.c_int, [C.c_void_p]),
+    "voxel_scan_groupby_status_code": (C.c_int, [C.c_int]),
     "voxel_agg_accumulate_dev": (C.c_int, [vp, vp, vp, sz, vp]),
     "voxel_agg_results": (sz, [vp, vp, vp, vp, vp, vp]),
     "voxel_dict_values": (sz, [vp, vp]),
@@ -211,6 +222,8 @@ def datagen() -> C.CDLL:
         _datagen.vgen_uniform_f64_mt.argtypes = [u64, sz, dbl, dbl, vp]
         _datagen.vgen_splitmix64.restype = None
         _datagen.vgen_splitmix64.argtypes = [u64, sz, vp]
+        _datagen.vgen_join_probe_i64.restype = None
+        _datagen.vgen_join_probe_i64.argtypes = [u64, vp, sz, dbl, dbl, sz, vp, C.c_uint]
     return _datagen
 
 

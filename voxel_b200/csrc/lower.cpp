@@ -18,6 +18,7 @@
 // one launch.  Anything the schedule cannot reproduce exactly is rejected with
 // a reason; there is no per-row interpretation on the device and no CPU path.
 #include "lower.h"
+#include "scan.h"
 
 #include <cstdio>
 #include <cstring>
@@ -783,6 +784,7 @@ std::string describe(const LoweredRegion& r) {
         os << " r" << k << "=" << kRed[d.kind % 4] << "/" << kAcc[d.acc % 7] << "[m=" << d.pmask << " a=" << int(d.a.kind)
            << ":" << int(d.a.col) << " b=" << int(d.b.kind) << ":" << int(d.b.col) << "]";
     }
+    os << " kernel=" << scan_kernel_name(p);
     return os.str();
 }
 

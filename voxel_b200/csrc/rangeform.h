@@ -141,4 +141,54 @@ inline bool range_form_of(const ScanParams& p, RangeForm* out) {
     }
 }
 
+// Most reductions a multi-reduction range form carries.
+constexpr int kMaxRangeRed = 4;
+
+// Range form of a program with 2..kMaxRangeRed reductions over one column that
+// all share the conjunction of every atom (the config-1 program's SUM and
+// COUNT of one VFILTER output; SUM + COUNT + MIN + MAX of one predicate).
+// Each reduction keeps its own kind, operands and canonical fold; the interval
+// and excluded values are those of range_form_t.  COUNT may count the column's
+// lanes (VCOUNT of a VFILTER output: passing nonzero values) or a constant.
+template <typename T>
+inline bool multi_range_form_t(const ScanParams& p, RangeForm* out) {
+    if (p.ncols != 1 || p.nred < 2 || p.nred > kMaxRangeRed || p.natoms < 1 || p.natoms > kMaxAtoms) return false;
+    const uint32_t all = (1u << p.natoms) - 1u;
+    constexpr bool kFloat = std::is_floating_point<T>::value;
+    for (int i = 0; i < p.nred; ++i) {
+        const Red& r = p.red[i];
+        if (r.pmask != all || r.kind > kRedMax) return false;
+        if (r.acc != range_acc(r.kind, kFloat)) return false;
+        const bool acol = r.a.kind == kOpCol && r.a.col == 0;
+        const bool aconst = r.a.kind == kOpConst || r.a.kind == kOpZero;
+        if (r.kind == kRedCount ? !(acol || aconst) : !acol) return false;
+        if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
+    }
+    // the interval: the single-reduction rewrite of the atoms with reduction 0
+    // (every reduction has the same predicate, so its interval is shared)
+    ScanParams q = p;
+    q.nred = 1;
+    q.red[0].kind = kRedSum;
+    q.red[0].acc = range_acc(kRedSum, kFloat);
+    q.red[0].a.kind = kOpCol;
+    q.red[0].a.col = 0;
+    q.red[0].b.kind = kOpZero;
+    if (!range_form_t<T>(q, out)) return false;
+    // range_form_t's code is 1 + 2 * kind + (excluded values present)
+    out->fast = (out->fast & 1u) ? 1u : 2u;  // 1: interval only, 2: with excluded values
+    out->pad = static_cast<uint32_t>(p.nred);
+    return true;
+}
+
+inline bool multi_range_form_of(const ScanParams& p, RangeForm* out) {
+    switch (p.dtype) {
+    case F64: return multi_range_form_t<double>(p, out);
+    case F32: return multi_range_form_t<float>(p, out);
+    case I64: return multi_range_form_t<int64_t>(p, out);
+    case I32: return multi_range_form_t<int32_t>(p, out);
+    case U64: return multi_range_form_t<uint64_t>(p, out);
+    default: return multi_range_form_t<uint32_t>(p, out);
+    }
+}
+
 }  // namespace vx

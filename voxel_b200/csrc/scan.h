@@ -16,6 +16,11 @@ int scan_scratch_init(void* scratch, cudaStream_t s);
 // values land in *d_out (device memory).  Returns a Status.
 int launch_scan(const ScanParams& p, ScanResult* d_out, void* scratch, cudaStream_t s);
 
+// Which kernel launch_scan runs for `p`: "fsum" (one atom, one masked SUM),
+// "range" (one reduction over an interval), "mrange" (2-4 reductions sharing
+// one interval) or "generic" (per-lane interpretation).  Host code only.
+const char* scan_kernel_name(const ScanParams& p);
+
 // Number of blocks launch_scan uses for `ngroups` groups of element type dt.
 int scan_grid(int dtype, uint64_t ndata, int ncols, int nred);
 

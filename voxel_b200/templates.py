@@ -118,6 +118,52 @@ def build(dtype: int, preds: list, agg: str, seg: int = 0) -> Program:
     return Program(dtype, preds, agg, code, regs, 0)
 
 
+# accumulator register of each aggregate in a multi-aggregate program
+MULTI_ACC = {"SUM": 0, "MIN": 3, "COUNT": 6, "MAX": 7}
+
+
+def build_multi(dtype: int, preds: list, aggs: list, seg: int = 0) -> Program:
+    """One predicate set, several aggregates of it in one loop: SUM into R0,
+    MIN into R3, COUNT into R6, MAX into R7 (the shape of the config-1 program
+    `filter x > t; SUM(x); COUNT` and of SUM+COUNT+MIN+MAX queries).  Each
+    aggregate is the single-aggregate template's lane formula over the shared
+    mask V4."""
+    assert 1 <= len(preds) <= 4 and aggs and len(set(aggs)) == len(aggs) and set(aggs) <= set(AGGS)
+    kl = K_LANES[dtype]
+    code = []
+    regs = {1: 0, 4: kl, 12: reg_image(dtype, 1), 13: reg_image(dtype, sentinel(dtype, "MIN")),
+            14: reg_image(dtype, sentinel(dtype, "MAX"))}
+    for i, p in enumerate(preds):
+        regs[8 + i] = reg_image(dtype, p.value)
+        code.append(bc.vsplat(8 + i, 8 + i))
+    code += [bc.vsplat(12, 12), bc.vsplat(13, 13), bc.vsplat(14, 14)]
+    head = len(code)
+    code.append(bc.vload(0, 1, seg))
+    code.append(bc.vcmp(preds[0].op, 4, 0, 8))
+    for i in range(1, len(preds)):
+        code.append(bc.vcmp(preds[i].op, 5, 0, 8 + i))
+        code.append(bc.vand(4, 4, 5))
+    for agg in aggs:
+        r = MULTI_ACC[agg]
+        if agg == "SUM":
+            code += [bc.vand(6, 4, 0), bc.vsum(5, 6)]
+            code.append(bc.addf(r, r, 5) if dtype in (F64, F32) else bc.add(r, r, 5))
+            regs[r] = 0
+        elif agg == "COUNT":
+            code += [bc.vand(6, 4, 12), bc.vcount(5, 6), bc.add(r, r, 5)]
+            regs[r] = 0
+        else:
+            red = bc.vred_min if agg == "MIN" else bc.vred_max
+            fold = bc.smin if agg == "MIN" else bc.smax
+            sv = 13 if agg == "MIN" else 14
+            code += [bc.vand(6, 4, 0), bc.vandn(7, 4, sv), bc.vor(6, 6, 7), red(5, 6), fold(r, r, 5)]
+            regs[r] = reg_image(dtype, sentinel(dtype, agg))
+    code += [bc.add(1, 1, 4), bc.cmp(1, 2)]
+    code.append(bc.jnz(head - len(code)))
+    code.append(bc.halt())
+    return Program(dtype, preds, ",".join(aggs), code, regs, MULTI_ACC[aggs[0]])
+
+
 def sql_reference(prog: Program, col: np.ndarray):
     """Scalar loop of the equivalent SQL query (Python / numpy)."""
     m = np.ones(col.size, bool)
