@@ -186,6 +186,20 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 # Secondary workloads (one JSON line each, same keys as the headline line).
 # --------------------------------------------------------------------------
 
+def _pinned(name: str, n: int, rank: int):
+    """The reference's full-size outputs for this workload (tests/golden/
+    fullsize.json) when this rank's inputs are the pinned ones, else None."""
+    try:
+        import fullsize
+    except ImportError:
+        return None
+    want = fullsize.load().get(name)
+    if not want or rank != 0:
+        return None
+    size = want.get("n", want.get("probe"))
+    return want if size == n else None
+
+
 def _common_line(metric, unit, value, world, args, ms_per_step, config, roofline, cpu, e2e, clk, launches, dtype,
                  higher=True):
     return {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
@@ -213,9 +227,10 @@ def _max_over_ranks(dist, dev, x):
 
 
 def workload_scan(args, L, rank, world, local, dist, dev):
-    """Fast-path filter+sum over 2^28 f64 U[0,1000) (mt19937_64 seed 42, the
-    reference's validation distribution), threshold 500: the streaming case of
-    the config-1 program, run through the engine with a device segment."""
+    """The config-1 program `filter x > 500; SUM(x); COUNT` over 2^28 f64
+    U[0,1000) (mt19937_64 seed 42, the reference's validation distribution):
+    its streaming case, run through the engine with a device segment (the
+    fused filter+sum kernel with its COUNT)."""
     import torch
 
     from voxel_b200 import bytecode as bc
@@ -224,7 +239,7 @@ def workload_scan(args, L, rank, world, local, dist, dev):
     host = np.empty(n, np.float64)
     capi.datagen().vgen_uniform_f64_mt(42 + rank, n, 0.0, 1000.0, host.ctypes.data)
     dcol = torch.from_numpy(host).to(dev)
-    code = np.asarray(bc.filter_sum_program(), np.uint32)
+    code = np.asarray(bc.filter_sum_count_program(), np.uint32)
     nbytes = n * 8
 
     def run_engine(e):
@@ -233,6 +248,7 @@ def workload_scan(args, L, rank, world, local, dist, dev):
         L.voxel_engine_set_scalar(e, 2, n)
         L.voxel_engine_set_scalar_f64(e, 3, 500.0)
         L.voxel_engine_set_scalar(e, 4, 4)
+        L.voxel_engine_set_scalar(e, 6, 0)
         L.voxel_engine_load_program(e, code.ctypes.data, code.size)
         if L.voxel_engine_run_status(e):
             raise RuntimeError(capi.last_error())
@@ -249,6 +265,16 @@ def workload_scan(args, L, rank, world, local, dist, dev):
             wall.append((time.perf_counter() - t0) * 1e3)
             dev_ms.append(L.voxel_engine_last_device_ms(e))
     result = L.voxel_engine_get_scalar_f64(e, 0)
+    result_count = L.voxel_engine_get_scalar(e, 6)
+    parity = None
+    want = _pinned("config1", n, rank)
+    if want is not None:
+        import struct
+
+        w0 = struct.unpack("<d", struct.pack("<Q", want["sum_count_r0"]))[0]
+        parity = {"against": "reference Engine<f64>::Run on the same rows (tests/golden/fullsize.json)",
+                  "count_exact_sum_1e-12": bool(result_count == want["sum_count_r6"]
+                                                 and abs(result - w0) <= 1e-12 * abs(w0))}
     L.voxel_engine_destroy(e)
     launch_ms = _max_over_ranks(dist, dev, statistics.mean(dev_ms))
     step_ms = _max_over_ranks(dist, dev, statistics.mean(wall))
@@ -271,16 +297,18 @@ def workload_scan(args, L, rank, world, local, dist, dev):
             m = 1 << 26
             out = C.c_double(0)
             threads = os.cpu_count() or 1
-            us = oracle.ref().vref_time_filter_sum_f64(2, code.ctypes.data, code.size, host.ctypes.data, m, 500.0, 2,
+            us = oracle.ref().vref_time_filter_sum_f64(3, code.ctypes.data, code.size, host.ctypes.data, m, 500.0, 2,
                                                        5, threads, C.byref(out))
             cpu = {"value": m * 8 / (us * 1e-6) / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"Engine<f64>::RunParallel, first {m} rows, median of 5 after 2 warm-ups"}
+                   "sample": f"Engine<f64>::Run on {threads} row chunks at once (the SUM+COUNT program is outside "
+                             f"the fast path RunParallel needs), first {m} rows, median of 5 after 2 warm-ups"}
     line = _common_line(
-        "fast-path filter+sum GB/s vs HBM peak", UNIT, world * nbytes / (launch_ms * 1e-3) / 1e9, world, args,
+        "filter+sum+count GB/s vs HBM peak", UNIT, world * nbytes / (launch_ms * 1e-3) / 1e9, world, args,
         step_ms,
-        {"workload": f"engine fast path VLOAD,VFILTER_GT,VSUM,ADDF,ADD,CMP,JNZ over {n} f64 U[0,1000) "
+        {"workload": f"config-1 program VLOAD,VFILTER_GT,VSUM,ADDF,VCOUNT,ADD,ADD,CMP,JNZ over {n} f64 U[0,1000) "
                      "(mt19937_64 seed 42), threshold 500; device-resident segment",
-         "rows_per_gpu": n, "algorithmic_bytes_per_step": nbytes, "result_R0": result,
+         "rows_per_gpu": n, "algorithmic_bytes_per_step": nbytes, "result_R0": result, "result_R6": result_count,
+         "parity": parity,
          "l2": "input (2.1 GB) larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}",
          "ms_per_step_note": "wall time of Engine::Run incl. launch, sync and register read-back"},
         _roofline("fsum_kernel", nbytes, launch_ms), cpu,
@@ -335,6 +363,15 @@ def workload_sort(args, L, rank, world, local, dist, dev):
     flip = work ^ torch.tensor(-(1 << 63), dtype=torch.int64, device=dev)
     checked = bool(torch.all(flip[1:] >= flip[:-1]).item()) and bool(torch.equal(src[idx.long()], work))
     del flip
+    parity = None
+    want = _pinned("sort", n, rank)
+    if want is not None:
+        import fullsize
+
+        ok = (fullsize.sha(work.cpu().numpy()) == want["keys_sha"]
+              and fullsize.sha(idx.cpu().numpy()) == want["idx_sha"])
+        parity = {"against": "reference RadixSort<u64>::Sort on the same keys (tests/golden/fullsize.json)",
+                  "keys_and_permutation_bit_exact": bool(ok)}
     # end to end: host keys in, sorted keys + ids out
     hk = torch.from_numpy(keys.view(np.int64)).pin_memory()
     hout = torch.empty(n, dtype=torch.int64).pin_memory()
@@ -372,6 +409,7 @@ def workload_sort(args, L, rank, world, local, dist, dev):
         "radix sort M keys/s", "M keys/s", world * n / (launch_ms * 1e-3) / 1e6, world, args, launch_ms,
         {"workload": f"stable LSD radix sort, {n} u64 keys SplitMix64 seed 3001 + u32 row ids",
          "rows_per_gpu": n, "result_checked": checked, "passes": passes, "algorithmic_bytes_per_step": nbytes,
+         "parity": parity,
          "l2": "keys (2.1 GB) larger than L2; no flush", "parallelism": f"replicas x{world}"},
         _roofline("radix_onesweep", nbytes, launch_ms), cpu,
         {"value": world * n / (e_ms * 1e-3) / 1e6, "unit": "M keys/s", "h2d_bytes_per_step": n * 8,
@@ -386,32 +424,18 @@ def workload_join(args, L, rank, world, local, dist, dev):
     (probe, build) pairs in probe order plus COUNT and SUM(payload)."""
     import torch
 
+    import fullsize
+
     nb = 1 << 24
     npr = args.rows if args.rows != ROWS else 1 << 29
-    bkeys = np.empty(nb, np.uint64)
-    capi.datagen().vgen_splitmix64(3002 + rank, nb, bkeys.ctypes.data)
-    bkeys &= np.uint64(0xFFFFFFFFFFFFFFFE)  # build keys even, miss keys odd
-    build = torch.from_numpy(bkeys.view(np.int64)).to(dev)
+    # build: even SplitMix64 keys; probe: 90% Zipf(0.8) over the build keys,
+    # 10% odd keys that never match (host generator, the pinned inputs)
+    hb, hp = fullsize.join_input(nb, npr, 3002 + rank, 3003 + rank)
+    bkeys = hb.view(np.uint64)
+    build = torch.from_numpy(hb).to(dev)
     payload = torch.arange(nb, dtype=torch.int64, device=dev)
-    g = torch.Generator(device=dev)
-    g.manual_seed(3003 + rank)
-    w = torch.arange(1, nb + 1, dtype=torch.float64, device=dev).pow_(-0.8)
-    cdf = torch.cumsum(w, 0)
-    cdf /= cdf[-1].clone()
-    del w
-    perm = torch.randperm(nb, device=dev, generator=g)
-    probe = torch.empty(npr, dtype=torch.int64, device=dev)
-    chunk = 1 << 26
-    for s0 in range(0, npr, chunk):
-        m = min(chunk, npr - s0)
-        u = torch.rand(m, dtype=torch.float64, device=dev, generator=g)
-        r = torch.searchsorted(cdf, u).clamp_(max=nb - 1)
-        k = build[perm[r]]
-        miss = torch.rand(m, device=dev, generator=g) < 0.1
-        odd = torch.randint(0, 1 << 62, (m,), device=dev, generator=g) * 2 + 1
-        probe[s0:s0 + m] = torch.where(miss, odd, k)
-        del u, r, k, miss, odd
-    del cdf, perm
+    probe = torch.from_numpy(hp).to(dev)
+    del hp
     left = torch.empty(npr, dtype=torch.int32, device=dev)
     right = torch.empty(npr, dtype=torch.int32, device=dev)
     cs = torch.zeros(2, dtype=torch.int64, device=dev)
@@ -439,6 +463,13 @@ def workload_join(args, L, rank, world, local, dist, dev):
         torch.cuda.synchronize()
     launch_ms = _max_over_ranks(dist, dev, statistics.mean(a.elapsed_time(b) for a, b in evs))
     nbytes = nb * 16 + npr * 8 + matches * 8
+    parity = None
+    want = _pinned("join", npr, rank)
+    if want is not None:
+        ok = (matches == want["matches"] and int(cs[1].item()) & ((1 << 64) - 1) == want["payload_sum"]
+              and fullsize.sha(left[:matches].cpu().numpy(), right[:matches].cpu().numpy()) == want["pairs_sha"])
+        parity = {"against": "reference HashJoin<i64> Build + ProbeAllMatches on the same keys "
+                             "(tests/golden/fullsize.json)", "count_sum_pairs_bit_exact": bool(ok)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
@@ -463,6 +494,7 @@ def workload_join(args, L, rank, world, local, dist, dev):
         {"workload": f"build {nb} unique i64 + u64 payload; probe {npr} i64, 90% Zipf(0.8) over build keys, 10% "
                      "misses; all pairs in probe order + COUNT + SUM(payload)",
          "build_rows": nb, "probe_rows_per_gpu": npr, "matches": matches, "algorithmic_bytes_per_step": nbytes,
+         "parity": parity,
          "m_probes_per_s": npr / (launch_ms * 1e-3) / 1e6, "parallelism": f"replicas x{world}",
          "l2": "probe (4.3 GB) larger than L2; no flush"},
         _roofline("hashjoin", nbytes, launch_ms), cpu,
@@ -1066,6 +1098,25 @@ def main() -> None:
     e2e = {"value": world * nbytes / (e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": int(ng) * (4 + 8 * 4) + 8, "ms_per_step": e_ms}
 
+    # the last timed step's groups against the reference's full-size output
+    parity = None
+    want = _pinned("config2", d["n"], rank)
+    if want is not None:
+        import fullsize
+
+        g = int(out["ng"][0].item())
+        ok = g == want["groups"]
+        if ok:
+            host_out = {k: out[k][:g].cpu().numpy() for k in ("keys", "sum", "min", "max", "cnt")}
+            ok = (fullsize.sha(host_out["keys"]) == want["keys_sha"]
+                  and fullsize.sha(host_out["cnt"].view(np.uint64)) == want["count_sha"]
+                  and fullsize.sha(host_out["min"]) == want["min_sha"]
+                  and fullsize.sha(host_out["max"]) == want["max_sha"]
+                  and bool(np.all(np.abs(host_out["sum"] - np.asarray(want["sums"]))
+                                  <= 1e-12 * np.abs(np.asarray(want["sums"])))))
+        parity = {"against": "reference HashAggregator on the same 2^25 rows (tests/golden/fullsize.json)",
+                  "keys_counts_minmax_bit_exact_sums_1e-12": bool(ok)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -1093,6 +1144,8 @@ def main() -> None:
         "clocks": clk.summary(),
         "gpu_launches": args.steps,
     }
+    if parity is not None:
+        line["config"]["parity"] = parity
     print(json.dumps(line), flush=True)
 
 
