@@ -522,6 +522,41 @@ size_t vo_rle_build_i64(const int64_t* d, size_t n, int64_t* values, uint32_t* r
     return k;
 }
 
+/* encoding.hpp:292-306 (DeltaEncoding<T>::Build): deltas[i] = data[i] - data[i-1],
+   data[-1] = 0, wrapping in T's width (w = 4 or 8 bytes; T's bits as unsigned). */
+void vo_delta_build(int w, const void* data, size_t n, void* deltas) {
+    uint64_t prev = 0;
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t x = w == 8 ? ((const uint64_t*)data)[i] : ((const uint32_t*)data)[i];
+        uint64_t d = x - prev;
+        if (w == 8) ((uint64_t*)deltas)[i] = d; else ((uint32_t*)deltas)[i] = (uint32_t)d;
+        prev = x;
+    }
+}
+
+/* encoding.hpp:317-330 (DeltaEncoding<T>::DecodeBatch): a running wrapping sum
+   from BaseValue over deltas[0..offset), then out[i] = running for the next
+   rows while i < cnt and offset + i < n (later outputs are left alone). */
+void vo_delta_decode(int w, const void* deltas, size_t n, uint64_t base, size_t off, size_t cnt, void* out) {
+    uint64_t run = base;
+    for (size_t i = 0; i < off && i < n; ++i)
+        run += w == 8 ? ((const uint64_t*)deltas)[i] : ((const uint32_t*)deltas)[i];
+    for (size_t i = 0; i < cnt && off + i < n; ++i) {
+        run += w == 8 ? ((const uint64_t*)deltas)[off + i] : ((const uint32_t*)deltas)[off + i];
+        if (w == 8) ((uint64_t*)out)[i] = run; else ((uint32_t*)out)[i] = (uint32_t)run;
+    }
+}
+
+/* encoding.hpp:489-500 (FrameOfReferenceEncoding::DecodeBatch):
+   BaseValue + (f64)code * Scale, each operation rounded (no contraction). */
+void vo_for_decode_f64(const int32_t* code, size_t n, double base, double scale, size_t off, size_t cnt,
+                       double* out) {
+    for (size_t i = 0; i < cnt && off + i < n; ++i) {
+        volatile double prod = (double)code[off + i] * scale;
+        out[i] = base + prod;
+    }
+}
+
 void vo_rle_decode_i64(const int64_t* values, const uint32_t* runs, size_t nruns, size_t off,
                        size_t cnt, int64_t* out) {
     /* encoding.hpp:231-257, including its u32 running total */

@@ -61,6 +61,10 @@ void vo_dict_decode_i32(const int32_t* dict, size_t card, const uint32_t* idx, s
                         size_t offset, size_t count, int32_t* out);
 /* RLEEncoding<i64> (encoding.hpp:202-257); returns the run count. */
 size_t vo_rle_build_i64(const int64_t* data, size_t n, int64_t* values, uint32_t* runs);
+void vo_delta_build(int w, const void* data, size_t n, void* deltas);
+void vo_delta_decode(int w, const void* deltas, size_t n, uint64_t base, size_t off, size_t cnt, void* out);
+void vo_for_decode_f64(const int32_t* code, size_t n, double base, double scale, size_t off, size_t cnt,
+                       double* out);
 void vo_rle_decode_i64(const int64_t* values, const uint32_t* runs, size_t nruns, size_t offset,
                        size_t count, int64_t* out);
 

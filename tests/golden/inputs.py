@@ -140,3 +140,23 @@ def config2(n: int, seed: int, card: int = 1000) -> dict:
     width = encode.bit_width(idx)
     packed = encode.bitpack(idx, width)
     return dict(n=n, key=key, dict=dict_, idx=idx, width=width, packed=packed, price=price, qty=qty)
+
+
+def codec_ints(npt, n: int, seed: int) -> np.ndarray:
+    """A mostly increasing integer column with negative steps and wraps (the
+    delta codec's inputs): a random walk of steps in [-1000, 100000)."""
+    rng = np.random.default_rng(seed)
+    steps = rng.integers(-1000, 100_000, size=n, dtype=np.int64)
+    start = int(rng.integers(-(2**40), 2**40))
+    info = np.iinfo(npt)
+    walk = (start + np.cumsum(steps)).astype(object) if n else np.zeros(0, object)
+    mod = 1 << info.bits
+    vals = [(int(v) % mod) for v in walk]
+    out = np.array(vals, dtype=np.uint64 if info.bits == 64 else np.uint32)
+    return out.view(npt) if out.size else np.zeros(0, npt)
+
+
+def codec_f64(n: int, seed: int) -> np.ndarray:
+    """A price-like f64 column for the frame-of-reference codec."""
+    rng = np.random.default_rng(seed)
+    return rng.lognormal(3.0, 1.0, n) - 10.0

@@ -14,6 +14,8 @@ import json
 import os
 import sys
 
+import ctypes as C
+
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -264,6 +266,41 @@ def op_cases():
     return ops
 
 
+def codec_cases():
+    """DeltaEncoding<T> and FrameOfReferenceEncoding run by the reference."""
+    L = oracle.ref()
+    rng = np.random.default_rng(9101)
+    delta = []
+    for name, dt, npt in (("i64", 2, np.int64), ("i32", 3, np.int32), ("u64", 4, np.uint64), ("u32", 5, np.uint32)):
+        for n in (0, 1, 7, 2048, 2049, 50_000):
+            seed = int(rng.integers(1 << 31))
+            data = inputs.codec_ints(npt, n, seed)
+            deltas = np.zeros(max(n, 1), npt)
+            base = int(getattr(L, f"vref_delta_build_{name}")(data.ctypes.data, n, deltas.ctypes.data))
+            decs = []
+            for off, cnt in ((0, n), (0, n + 5), (n // 3, n // 2), (max(n - 1, 0), 4), (n + 2, 3), (5, 0)):
+                out = np.zeros(max(cnt, 1), npt)
+                getattr(L, f"vref_delta_decode_{name}")(deltas.ctypes.data, n, base, off, cnt, out.ctypes.data)
+                decs.append(dict(offset=off, count=cnt, digest=digest(out[:cnt])))
+            delta.append(dict(dtype=dt, n=n, seed=seed, base=base, deltas_digest=digest(deltas[:n]), decodes=decs))
+    fr = []
+    for n in (0, 1, 5, 4096, 100_001):
+        seed = int(rng.integers(1 << 31))
+        x = inputs.codec_f64(n, seed)
+        codes = np.zeros(max(n, 1), np.int32)
+        base, scale = C.c_double(), C.c_double()
+        L.vref_for_build_f64(x.ctypes.data, n, codes.ctypes.data, C.byref(base), C.byref(scale))
+        decs = []
+        for off, cnt in ((0, n), (n // 2, n), (n + 1, 2)):
+            out = np.zeros(max(cnt, 1))
+            L.vref_for_decode_f64(codes.ctypes.data, n, base.value, scale.value, off, cnt, out.ctypes.data)
+            m = max(0, min(cnt, n - off))
+            decs.append(dict(offset=off, count=cnt, digest=digest(out[:m])))
+        fr.append(dict(n=n, seed=seed, base=base.value, scale=scale.value, codes_digest=digest(codes[:n]),
+                       decodes=decs))
+    return dict(delta=delta, frame_of_reference=fr)
+
+
 def C_size():
     import ctypes
     return ctypes.c_size_t(0)
@@ -287,7 +324,8 @@ def main():
     if not oracle.have_ref():
         raise SystemExit("the reference library is required to generate golden vectors")
     doc = dict(source="reference VoxelVM operators compiled by oracle/build_oracle.py",
-               kat=kat_cases(), config1=config1(), programs=program_cases(), ops=op_cases())
+               kat=kat_cases(), config1=config1(), programs=program_cases(), ops=op_cases(),
+               codecs=codec_cases())
     with open(OUT, "w") as f:
         json.dump(doc, f, separators=(",", ":"))
     print(f"wrote {OUT}: {len(doc['programs'])} program cases, {os.path.getsize(OUT)} bytes")

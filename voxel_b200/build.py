@@ -40,6 +40,7 @@ CORE_SOURCES = [
     "engine.cpp",
     "filter.cu",
     "decode.cu",
+    "delta.cu",
     "groupby.cu",
     "radix.cu",
     "join.cu",
@@ -116,7 +117,7 @@ def build(force: bool = False, jobs: int | None = None) -> str:
         print("[build] pybind11 missing: voxel_py not built", file=sys.stderr)
     dsrc = os.path.join(CSRC, "datagen.cpp")
     if os.path.exists(dsrc) and (force or _stale(DATAGEN_SO, [dsrc])):
-        subprocess.check_call(["g++", "-O3", "-std=c++17", "-shared", "-fPIC", dsrc, "-o", DATAGEN_SO])
+        subprocess.check_call(["g++", "-O3", "-std=c++17", "-shared", "-fPIC", dsrc, "-o", DATAGEN_SO, "-lpthread"])
     return LIB_SO
 
 

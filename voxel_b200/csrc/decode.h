@@ -19,4 +19,12 @@ size_t rle_scratch_bytes(uint64_t nruns);
 int launch_rle_decode_i64(const int64_t* values, const uint32_t* runs, uint64_t nruns, uint64_t offset,
                           uint64_t count, int64_t* out, void* scratch, int* err, cudaStream_t s);
 
+// delta.cu: DeltaEncoding / FrameOfReferenceEncoding codecs
+size_t delta_scratch_bytes(uint64_t limit);
+int launch_delta_decode(int dtype, const void* deltas, uint64_t n, uint64_t base_bits, uint64_t offset,
+                        uint64_t count, void* out, void* scratch, int* err, cudaStream_t s);
+int launch_delta_encode(int dtype, const void* data, uint64_t n, void* deltas, cudaStream_t s);
+int launch_for_decode_f64(const int32_t* code, uint64_t n, double base, double scale, uint64_t offset,
+                          uint64_t count, double* out, cudaStream_t s);
+
 }  // namespace vx
