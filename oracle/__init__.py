@@ -52,6 +52,12 @@ def port() -> C.CDLL:
         L.vo_dict_build_i32.argtypes = [vp, sz, vp, vp]
         L.vo_dict_decode_i32.restype = None
         L.vo_dict_decode_i32.argtypes = [vp, sz, vp, sz, sz, sz, vp]
+        L.vo_delta_build.restype = None
+        L.vo_delta_build.argtypes = [C.c_int, vp, sz, vp]
+        L.vo_delta_decode.restype = None
+        L.vo_delta_decode.argtypes = [C.c_int, vp, sz, u64, sz, sz, vp]
+        L.vo_for_decode_f64.restype = None
+        L.vo_for_decode_f64.argtypes = [vp, sz, dbl, dbl, sz, sz, vp]
         L.vo_rle_build_i64.restype = sz
         L.vo_rle_build_i64.argtypes = [vp, sz, vp, vp]
         L.vo_rle_decode_i64.restype = None
@@ -130,6 +136,21 @@ def ref() -> C.CDLL:
             f = getattr(L, f"vref_hashjoin_{k}")
             f.restype = sz
             f.argtypes = [vp, sz, vp, sz, vp, vp, sz, C.c_int]
+        for t in ("i64", "i32", "u64", "u32"):
+            f = getattr(L, f"vref_delta_build_{t}")
+            f.restype = u64
+            f.argtypes = [vp, sz, vp]
+            f = getattr(L, f"vref_delta_decode_{t}")
+            f.restype = None
+            f.argtypes = [vp, sz, u64, sz, sz, vp]
+        L.vref_for_build_f64.restype = None
+        L.vref_for_build_f64.argtypes = [vp, sz, vp, C.POINTER(dbl), C.POINTER(dbl)]
+        L.vref_for_decode_f64.restype = None
+        L.vref_for_decode_f64.argtypes = [vp, sz, dbl, dbl, sz, sz, vp]
+        L.vref_scalar_filter_gt_f32.restype = sz
+        L.vref_scalar_filter_gt_f32.argtypes = [vp, vp, C.c_float, sz]
+        L.vref_scalar_sum_f32.restype = C.c_float
+        L.vref_scalar_sum_f32.argtypes = [vp, sz]
         L.vref_scan_groupby.restype = sz
         L.vref_scan_groupby.argtypes = [vp, sz, u32, vp, sz, vp, vp, sz, dbl, i32, i32, C.c_int,
                                         vp, vp, vp, vp, vp, C.POINTER(dbl)]
@@ -200,3 +221,59 @@ def scan_groupby_ref(packed, width, dict_, price, qty, pthr, qlo, qhi, threads=1
                                 C.byref(us))
     o = np.argsort(ok[:g], kind="stable")
     return ok[:g][o], s[:g][o], mn[:g][o], mx[:g][o], c[:g][o], us.value * 1e-6
+
+
+def f32_selection_ref(preds, col):
+    """The rows an f32 program's conjunctive predicates select, decided by the
+    reference's own operators: VectorFilter<f32>::Apply* per predicate
+    (filter.hpp:42-288) and ColumnFilter::AndWith (526-547), then
+    SelectionVector::BuildFromBitmap (378-399).  preds: (op, value) pairs,
+    op 0 EQ .. 5 GE.  Returns the ascending row ids."""
+    L = ref()
+    col = np.ascontiguousarray(col, dtype=np.float32)
+    n = col.size
+    words = max((n + 63) // 64, 1)
+    bms = []
+    for op, v in preds:
+        bm = np.zeros(words, np.uint64)
+        L.vref_vfilter_f32(op, col.ctypes.data, n, float(np.float32(v)), 0.0, bm.ctypes.data)
+        bms.append(bm)
+    ptrs = (C.c_void_p * len(bms))(*[b.ctypes.data for b in bms])
+    out = np.zeros(words, np.uint64)
+    L.vref_column_filter_and(ptrs, len(bms), n, out.ctypes.data)
+    sel = np.zeros(max(n, 1), np.uint32)
+    k = L.vref_selection_from_bitmap(out.ctypes.data, n, sel.ctypes.data)
+    return sel[:k]
+
+
+def f32_filter_gt_ref(col, threshold):
+    """simd/scalar.hpp:214-227: the values > threshold in row order."""
+    col = np.ascontiguousarray(col, dtype=np.float32)
+    out = np.zeros(max(col.size, 1), np.float32)
+    k = ref().vref_scalar_filter_gt_f32(out.ctypes.data, col.ctypes.data, float(np.float32(threshold)), col.size)
+    return out[:k]
+
+
+def f32_program_expect(preds, aggs, col):
+    """Expected results of an f32 filter/aggregate program whose rows are
+    selected by the reference's VectorFilter<f32> + ColumnFilter: COUNT is the
+    number of selected rows, SUM their exact sum (the programs accumulate in
+    f64; compare within 1e-6 relative), MIN / MAX the extreme selected value or
+    the template's sentinel when nothing is selected."""
+    import math
+
+    from voxel_b200 import templates as T
+
+    sel = f32_selection_ref([(p.op, p.value) for p in preds], col)
+    vals = np.asarray(col, np.float32)[sel]
+    out = {}
+    for a in aggs:
+        if a == "COUNT":
+            out[a] = int(sel.size)
+        elif a == "SUM":
+            out[a] = math.fsum(vals.astype(np.float64))
+        elif vals.size == 0:
+            out[a] = float(T.sentinel(T.F32, a))
+        else:
+            out[a] = float(vals.min() if a == "MIN" else vals.max())
+    return out

@@ -182,3 +182,66 @@ def test_restatement_matches_reference_live():
             st, mine, _ = oracle.engine_run_port(dt, prog.code, [col], regs)
             assert st == 0
             assert mine == oracle.engine_run_ref(dt, prog.code, [col], regs)
+
+
+def test_f32_restatement_pinned_to_reference_filters():
+    """f32 has no reference engine (Engine<f32> does not compile), so the
+    restated f32 programs are pinned to the reference's own f32 operators:
+    rows selected by VectorFilter<f32> + ColumnFilter give COUNT exactly,
+    MIN / MAX exactly and SUM within 1e-6; for `x > t` the selected values
+    equal the reference's scalar_filter_gt_f32 compaction."""
+    if not oracle.have_ref():
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(31)
+    for n in (8, 64, 1000, 8 * 4093):
+        col = T.make_column(T.F32, n, rng)
+        for aggs in (["SUM"], ["COUNT"], ["MIN"], ["MAX"], ["SUM", "COUNT", "MIN", "MAX"]):
+            base = T.random_program(T.F32, rng, npreds=int(rng.integers(1, 5)))
+            prog = T.build_multi(T.F32, base.preds, aggs) if len(aggs) > 1 else T.build(T.F32, base.preds, aggs[0])
+            st, got, _ = oracle.engine_run_port(T.F32, prog.code, [col], prog.registers(n))
+            assert st == 0
+            want = oracle.f32_program_expect(base.preds, aggs, col)
+            for a in aggs:
+                reg = T.MULTI_ACC[a] if len(aggs) > 1 else 0
+                v = T.image_value(T.F32, got[reg]) if a != "COUNT" else got[reg]
+                if a == "SUM":
+                    assert abs(v - want[a]) <= 1e-6 * abs(want[a]) + 1e-30, (a, v, want[a])
+                else:
+                    assert v == want[a], (a, v, want[a])
+        sel = oracle.f32_selection_ref([(4, 500.0)], col)
+        assert (col[sel] == oracle.f32_filter_gt_ref(col, 500.0)).all()
+
+
+def test_codec_restatement_against_reference(golden):
+    """The restated delta and frame-of-reference decoders reproduce the
+    reference's DeltaEncoding / FrameOfReferenceEncoding outputs (golden
+    fixtures, and the live reference build at random offsets)."""
+    import ctypes as C
+
+    P = oracle.port()
+    np_t = {2: np.int64, 3: np.int32, 4: np.uint64, 5: np.uint32}
+    for case in golden["codecs"]["delta"]:
+        dt, n = case["dtype"], case["n"]
+        w = 8 if dt in (2, 4) else 4
+        data = inputs.codec_ints(np_t[dt], n, case["seed"])
+        deltas = np.zeros(max(n, 1), np_t[dt])
+        P.vo_delta_build(w, data.ctypes.data, n, deltas.ctypes.data)
+        assert hashlib.sha256(deltas[:n].tobytes()).hexdigest() == case["deltas_digest"]
+        for d in case["decodes"]:
+            out = np.zeros(max(d["count"], 1), np_t[dt])
+            P.vo_delta_decode(w, deltas.ctypes.data, n, case["base"], d["offset"], d["count"], out.ctypes.data)
+            assert hashlib.sha256(out[:d["count"]].tobytes()).hexdigest() == d["digest"]
+    for case in golden["codecs"]["frame_of_reference"]:
+        n = case["n"]
+        if not oracle.have_ref():
+            break
+        x = inputs.codec_f64(n, case["seed"])
+        codes = np.zeros(max(n, 1), np.int32)
+        base, scale = C.c_double(), C.c_double()
+        oracle.ref().vref_for_build_f64(x.ctypes.data, n, codes.ctypes.data, C.byref(base), C.byref(scale))
+        for d in case["decodes"]:
+            m = max(0, min(d["count"], n - d["offset"]))
+            out = np.zeros(max(m, 1))
+            P.vo_for_decode_f64(codes.ctypes.data, n, base.value, scale.value, d["offset"], d["count"],
+                                out.ctypes.data)
+            assert hashlib.sha256(out[:m].tobytes()).hexdigest() == d["digest"]

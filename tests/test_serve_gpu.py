@@ -1,11 +1,18 @@
 """Serving loop: every request's result is the same run alone (submitted and
 awaited one at a time) and run inside a concurrent mix of programs, group-bys
-and joins under a tight working-memory budget; and each equals the direct
-(non-served) entry points.  Requests larger than the whole budget are refused
-with VOXEL_ECAPACITY."""
+and joins under a tight working-memory budget; and each equals the reference:
+program registers the reference interpreter's (f32: the restatement's, with
+its aggregates pinned to the reference's f32 filters), group-by rows
+HashAggregator's (keys, counts, min, max exact; sums within 1e-12), join pairs
+HashJoin::ProbeAllMatches's in probe order.  Requests larger than the whole
+budget are refused with VOXEL_ECAPACITY."""
+import struct
+
 import numpy as np
 import pytest
 import torch
+
+import oracle
 
 from voxel_b200 import capi
 from voxel_b200 import templates as T
@@ -101,45 +108,63 @@ def test_results_identical_alone_and_in_the_mix():
     for key, want in alone.items():
         same(mixed[key], want)
 
-    # and both equal the direct entry points
-    L = capi.lib()
+    # and each equals the reference on the same inputs
     for i, (prog, col) in enumerate(progs):
-        b = L.voxel_batch_create()
-        regs = np.array(prog.registers(col.numel()), np.uint64)
-        code = np.asarray(prog.code, np.uint32)
-        assert L.voxel_batch_add(b, prog.dtype, code.ctypes.data, code.size, regs.ctypes.data, col.data_ptr(),
-                                 col.numel(), 0, 0, None) == 0
-        assert L.voxel_batch_launch(b, 0, None) == 0 and L.voxel_batch_fetch(b, None) == 0
-        out = np.zeros(64, np.uint64)
-        cnt = np.zeros(1, np.uint64)
-        L.voxel_batch_result(b, 0, out.ctypes.data, cnt.ctypes.data, None)
-        L.voxel_batch_destroy(b)
-        assert [int(x) for x in out] == alone[("p", i)]["registers"] and int(cnt[0]) == alone[("p", i)]["count"]
         c = col.cpu().numpy()
+        regs = prog.registers(c.size)
+        if prog.dtype == T.F32:
+            st, want, _ = oracle.engine_run_port(prog.dtype, prog.code, [c], regs)
+            assert st == 0
+            ref = oracle.f32_program_expect(prog.preds, [prog.agg], c)[prog.agg]
+            got0 = alone[("p", i)]["registers"][0]
+            v = T.image_value(T.F32, got0) if prog.agg != "COUNT" else got0
+            assert (abs(v - ref) <= 1e-6 * abs(ref) + 1e-30) if prog.agg == "SUM" else v == ref
+        else:
+            want = oracle.engine_run_ref(prog.dtype, prog.code, [c], regs)
+        got = alone[("p", i)]["registers"]
+        for r in range(16):
+            if got[r] == want[r]:
+                continue
+            assert prog.dtype in (T.F64, T.F32) and r == 0 and prog.agg == "SUM", (i, r, got[r], want[r])
+            g, w = f64(got[r]), f64(want[r])
+            assert abs(g - w) <= (1e-6 if prog.dtype == T.F32 else 1e-12) * abs(w), (i, g, w)
+        # the selection: the rows the reference's VectorFilter + ColumnFilter pass
         m = np.ones(c.size, bool)
         for q in prog.preds:
             v = np.float32(q.value) if prog.dtype == T.F32 else T.NP[prog.dtype](q.value)
             m &= [np.equal, np.not_equal, np.less, np.less_equal, np.greater, np.greater_equal][q.op](c, v)
         assert (alone[("p", i)]["selection"] == np.flatnonzero(m)).all()
+        assert alone[("p", i)]["count"] == int(m.sum())
+    L = oracle.ref()
     for i, (keys, vals, ng) in enumerate(groups):
-        k = keys.cpu().numpy()
+        k = keys.cpu().numpy().astype(np.uint32)
         v = vals.cpu().numpy()
-        present = np.unique(k)
+        ok = np.zeros(ng, np.uint32)
+        sm, mn, mx = (np.zeros(ng) for _ in range(3))
+        cnt = np.zeros(ng, np.uint64)
+        g = L.vref_hashagg_u32_f64(k.ctypes.data, v.ctypes.data, k.size, ng, ok.ctypes.data, sm.ctypes.data,
+                                   mn.ctypes.data, mx.ctypes.data, cnt.ctypes.data)
+        o = np.argsort(ok[:g], kind="stable")
         r = alone[("g", i)]
-        assert (r["keys"] == present).all()
-        assert (r["count"] == np.bincount(k, minlength=ng)[present]).all()
-        np.testing.assert_allclose(r["sum"], np.bincount(k, weights=v, minlength=ng)[present], rtol=1e-12,
-                                   atol=1e-9)
+        assert (r["keys"] == ok[:g][o]).all()
+        assert (r["count"] == cnt[:g][o]).all()
+        assert (r["min"] == mn[:g][o]).all() and (r["max"] == mx[:g][o]).all()
+        np.testing.assert_allclose(r["sum"], sm[:g][o], rtol=1e-12, atol=1e-9)
     for i, (b, pay, p) in enumerate(joins):
-        left = torch.zeros(p.numel(), dtype=torch.int32, device=DEV)
-        right = torch.zeros(p.numel(), dtype=torch.int32, device=DEV)
-        cs = torch.zeros(4, dtype=torch.int64, device=DEV)
-        assert L.voxel_hashjoin_i64_dev(b.data_ptr(), pay.data_ptr(), b.numel(), p.data_ptr(), p.numel(),
-                                        left.data_ptr(), right.data_ptr(), p.numel(), 1, cs.data_ptr(), None) == 0
-        m = int(cs[0])
+        hb = b.cpu().numpy()
+        hp = p.cpu().numpy()
+        wl = np.zeros(hp.size, np.uint32)
+        wr = np.zeros(hp.size, np.uint32)
+        m = int(L.vref_hashjoin_i64(hb.ctypes.data, hb.size, hp.ctypes.data, hp.size, wl.ctypes.data,
+                                    wr.ctypes.data, hp.size, 1))
         r = alone[("j", i)]
-        assert r["count"] == m and r["aux"] == int(cs[1])
-        assert (r["left"] == left[:m].cpu().numpy()).all() and (r["right"] == right[:m].cpu().numpy()).all()
+        assert r["count"] == m
+        assert (r["left"].view(np.uint32) == wl[:m]).all() and (r["right"].view(np.uint32) == wr[:m]).all()
+        assert r["aux"] == int(wr[:m].astype(np.uint64).sum())  # payload = build row id
+
+
+def f64(b):
+    return struct.unpack("<d", struct.pack("<Q", b & 0xFFFFFFFFFFFFFFFF))[0]
 
 
 def test_request_larger_than_budget_is_refused():
