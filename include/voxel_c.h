@@ -399,6 +399,29 @@ int       voxel_radix_sort_dev(int dtype, void* d_keys, uint32_t* d_idx, size_t 
 size_t    voxel_radix_sort_tmp_bytes(int dtype, size_t n);
 
 /* ================================================================
+ * Additive: merge, semi and anti joins (reference ops/join.hpp:216-310) over
+ * integer keys (dtype 2 i64, 3 i32, 4 u64, 5 u32); row ids are u32.
+ * voxel_merge_join: MergeJoin<TKey> over keys sorted ascending.  unique = 0:
+ *   Join (218-244), every (left, right) pair of equal keys, left-major with
+ *   right rows ascending; unique = 1: JoinUnique (246-268), the t-th left row
+ *   of a key pairs with the t-th right row of that key.  Writes at most
+ *   max_matches pairs and returns how many it wrote ((size_t)-1 on error);
+ *   the _dev form writes {written, all matches} to d_count2.
+ * voxel_semi_join: SemiJoin (294-310, anti = 0) / AntiJoin (273-290, anti =
+ *   1): the ascending left row ids whose key is / is not among the right keys
+ *   (no order assumed); out holds nl entries; returns the count.
+ * ================================================================ */
+size_t    voxel_merge_join(int dtype, const void* left, size_t nl, const void* right, size_t nr,
+                           uint32_t* left_out, uint32_t* right_out, size_t max_matches, int unique);
+int       voxel_merge_join_dev(int dtype, const void* d_left, size_t nl, const void* d_right, size_t nr,
+                               uint32_t* d_left_out, uint32_t* d_right_out, size_t max_matches, int unique,
+                               uint64_t* d_count2, void* stream);
+size_t    voxel_semi_join(int dtype, const void* left, size_t nl, const void* right, size_t nr, uint32_t* out,
+                          int anti);
+int       voxel_semi_join_dev(int dtype, const void* d_left, size_t nl, const void* d_right, size_t nr,
+                              uint32_t* d_out, int anti, uint64_t* d_count, void* stream);
+
+/* ================================================================
  * Additive: hash join on i64 keys (HashJoin<TKey>, join.hpp:36-165).
  * Pairs (probe_idx, build_idx) in ascending probe order; for equal build
  * keys the newest build row comes first (the reference's LIFO chains).

@@ -52,6 +52,10 @@ def port() -> C.CDLL:
         L.vo_dict_build_i32.argtypes = [vp, sz, vp, vp]
         L.vo_dict_decode_i32.restype = None
         L.vo_dict_decode_i32.argtypes = [vp, sz, vp, sz, sz, sz, vp]
+        L.vo_merge_join_i64.restype = sz
+        L.vo_merge_join_i64.argtypes = [vp, sz, vp, sz, vp, vp, sz, C.c_int]
+        L.vo_semi_join_i64.restype = sz
+        L.vo_semi_join_i64.argtypes = [vp, sz, vp, sz, vp, C.c_int]
         L.vo_delta_build.restype = None
         L.vo_delta_build.argtypes = [C.c_int, vp, sz, vp]
         L.vo_delta_decode.restype = None
@@ -147,6 +151,13 @@ def ref() -> C.CDLL:
         L.vref_for_build_f64.argtypes = [vp, sz, vp, C.POINTER(dbl), C.POINTER(dbl)]
         L.vref_for_decode_f64.restype = None
         L.vref_for_decode_f64.argtypes = [vp, sz, dbl, dbl, sz, sz, vp]
+        for t in ("i64", "i32", "u64", "u32"):
+            f = getattr(L, f"vref_merge_join_{t}")
+            f.restype = sz
+            f.argtypes = [vp, sz, vp, sz, vp, vp, C.c_int]
+            f = getattr(L, f"vref_semi_join_{t}")
+            f.restype = sz
+            f.argtypes = [vp, sz, vp, sz, vp, C.c_int]
         L.vref_scalar_filter_gt_f32.restype = sz
         L.vref_scalar_filter_gt_f32.argtypes = [vp, vp, C.c_float, sz]
         L.vref_scalar_sum_f32.restype = C.c_float

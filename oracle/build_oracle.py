@@ -35,8 +35,14 @@ ORACLE_SO = os.path.join(BUILD, "libvoxel_oracle.so")
 REF_SO = os.path.join(REF_OUT, "libvoxel_ref.so")
 
 
+# Where the reference sources are mounted in the build container.  This recipe
+# is the one place that names it; everything else asks reference_root().
+DEFAULT_REFERENCE_ROOT = "/root/reference"
+
+
 def reference_root() -> str:
-    return os.environ.get("VOXEL_REFERENCE_ROOT", "/root/reference")
+    """$VOXEL_REFERENCE_ROOT, else the build container's mount point."""
+    return os.environ.get("VOXEL_REFERENCE_ROOT", DEFAULT_REFERENCE_ROOT)
 
 
 def _newer(target: str, *sources: str) -> bool:

@@ -178,6 +178,29 @@ void delta_decode_t(const T* deltas, size_t n, uint64_t base, size_t offset, siz
     e.Deltas.assign(deltas, deltas + n);
     e.DecodeBatch(out, offset, count);
 }
+// join.hpp:216-310 (MergeJoin<TKey>::Join / JoinUnique, SemiJoin, AntiJoin)
+template <typename T>
+size_t merge_join_t(const T* l, size_t nl, const T* r, size_t nr, uint32_t* lo, uint32_t* ro, int unique) {
+    ops::MergeJoin<T> j;
+    sz m = 0;
+    if (unique) j.JoinUnique(l, nl, r, nr, lo, ro, m);
+    else j.Join(l, nl, r, nr, lo, ro, m);
+    return m;
+}
+template <typename T>
+size_t semi_join_t(const T* l, size_t nl, const T* r, size_t nr, uint32_t* out, int anti) {
+    Arena arena;
+    sz m = 0;
+    if (anti) {
+        ops::AntiJoin<T> j;
+        j.Join(l, nl, r, nr, out, m, arena);
+    } else {
+        ops::SemiJoin<T> j;
+        j.Join(l, nl, r, nr, out, m, arena);
+    }
+    return m;
+}
+
 extern "C" {
 
 int vref_engine_run(int dtype, const uint32_t* code, size_t len, const void* const* segs,
@@ -351,6 +374,15 @@ void vref_for_decode_f64(const int32_t* codes, size_t n, double base, double sca
     e.EncodedValues.assign(codes, codes + n);
     e.DecodeBatch(out, offset, count);
 }
+
+size_t vref_merge_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* lo, uint32_t* ro, int u) { return merge_join_t<i64>(l, nl, r, nr, lo, ro, u); }
+size_t vref_merge_join_i32(const int32_t* l, size_t nl, const int32_t* r, size_t nr, uint32_t* lo, uint32_t* ro, int u) { return merge_join_t<i32>(l, nl, r, nr, lo, ro, u); }
+size_t vref_merge_join_u64(const uint64_t* l, size_t nl, const uint64_t* r, size_t nr, uint32_t* lo, uint32_t* ro, int u) { return merge_join_t<u64>(l, nl, r, nr, lo, ro, u); }
+size_t vref_merge_join_u32(const uint32_t* l, size_t nl, const uint32_t* r, size_t nr, uint32_t* lo, uint32_t* ro, int u) { return merge_join_t<u32>(l, nl, r, nr, lo, ro, u); }
+size_t vref_semi_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<i64>(l, nl, r, nr, o, a); }
+size_t vref_semi_join_i32(const int32_t* l, size_t nl, const int32_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<i32>(l, nl, r, nr, o, a); }
+size_t vref_semi_join_u64(const uint64_t* l, size_t nl, const uint64_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<u64>(l, nl, r, nr, o, a); }
+size_t vref_semi_join_u32(const uint32_t* l, size_t nl, const uint32_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<u32>(l, nl, r, nr, o, a); }
 
 // filter.hpp:378-399 (SelectionVector::BuildFromBitmap)
 size_t vref_selection_from_bitmap(const uint64_t* bm, size_t rows, uint32_t* out) {

@@ -718,3 +718,51 @@ size_t vo_scan_groupby(const uint64_t* packed, size_t nwords, uint32_t width, co
     free(k); free(v); free(p);
     return g;
 }
+
+/* join.hpp:218-268 (MergeJoin<TKey>::Join / JoinUnique) over sorted i64 keys:
+   two cursors; on equal keys Join emits the whole right run for the left row
+   and rewinds the right cursor, JoinUnique emits one pair and advances both.
+   Stops writing at cap; returns the pairs written. */
+size_t vo_merge_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* lo, uint32_t* ro,
+                         size_t cap, int unique) {
+    size_t m = 0, li = 0, ri = 0;
+    while (li < nl && ri < nr) {
+        if (l[li] < r[ri]) ++li;
+        else if (r[ri] < l[li]) ++ri;
+        else if (unique) {
+            if (m < cap) { lo[m] = (uint32_t)li; ro[m] = (uint32_t)ri; ++m; }
+            ++li; ++ri;
+        } else {
+            size_t start = ri;
+            while (ri < nr && r[ri] == l[li]) {
+                if (m < cap) { lo[m] = (uint32_t)li; ro[m] = (uint32_t)ri; ++m; }
+                ++ri;
+            }
+            ++li;
+            ri = start;
+        }
+    }
+    return m;
+}
+
+static int cmp_i64(const void* a, const void* b) {
+    int64_t x = *(const int64_t*)a, y = *(const int64_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+/* join.hpp:273-310 (AntiJoin / SemiJoin): left rows in order whose key is
+   (anti = 0) / is not (anti = 1) in the set of right keys. */
+size_t vo_semi_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* out, int anti) {
+    int64_t* s = (int64_t*)malloc((nr ? nr : 1) * 8);
+    memcpy(s, r, nr * 8);
+    qsort(s, nr, 8, cmp_i64);
+    size_t m = 0;
+    for (size_t i = 0; i < nl; ++i) {
+        size_t lo = 0, hi = nr;
+        while (lo < hi) { size_t mid = (lo + hi) / 2; if (s[mid] < l[i]) lo = mid + 1; else hi = mid; }
+        int found = lo < nr && s[lo] == l[i];
+        if (found != anti) out[m++] = (uint32_t)i;
+    }
+    free(s);
+    return m;
+}

@@ -160,3 +160,27 @@ def codec_f64(n: int, seed: int) -> np.ndarray:
     """A price-like f64 column for the frame-of-reference codec."""
     rng = np.random.default_rng(seed)
     return rng.lognormal(3.0, 1.0, n) - 10.0
+
+
+def merge_join_input(npt, nl: int, nr: int, dup: int, seed: int):
+    """Sorted left / right key columns of one integer type with runs of equal
+    keys (up to `dup` copies) and keys on one side only."""
+    rng = np.random.default_rng(seed)
+    info = np.iinfo(npt)
+    lo = max(int(info.min), -(2**40))
+    hi = min(int(info.max), 2**40)
+    pool = np.unique(rng.integers(lo, hi, size=max(nl, nr) // 2 + 8, dtype=np.int64))
+
+    def side(n):
+        if n == 0:
+            return np.zeros(0, npt)
+        k = pool[rng.integers(0, pool.size, size=n)]
+        k = np.repeat(k, rng.integers(1, dup + 1, size=n))[:n]
+        return np.sort(k).astype(npt)
+
+    return side(nl), side(nr)
+
+
+def shuffled(a: np.ndarray, seed: int) -> np.ndarray:
+    """A seeded permutation of `a` (the semi / anti joins' unordered left side)."""
+    return np.random.default_rng(seed + 1).permutation(a) if a.size else a

@@ -301,6 +301,35 @@ def codec_cases():
     return dict(delta=delta, frame_of_reference=fr)
 
 
+def join_family_cases():
+    """MergeJoin (Join, JoinUnique), SemiJoin and AntiJoin run by the reference."""
+    L = oracle.ref()
+    rng = np.random.default_rng(9201)
+    out = []
+    for name, dt, npt in (("i64", 2, np.int64), ("i32", 3, np.int32), ("u64", 4, np.uint64), ("u32", 5, np.uint32)):
+        for nl, nr, dup in ((0, 5, 1), (5, 0, 1), (1, 1, 1), (300, 200, 1), (2000, 1500, 4), (40_000, 30_000, 3)):
+            seed = int(rng.integers(1 << 31))
+            lk, rk = inputs.merge_join_input(npt, nl, nr, dup, seed)
+            case = dict(dtype=dt, nl=nl, nr=nr, dup=dup, seed=seed)
+            for unique in (0, 1):
+                cap = max(1, nl * min(max(nr, 1), dup * 4))
+                lo = np.zeros(cap, np.uint32)
+                ro = np.zeros(cap, np.uint32)
+                m = int(getattr(L, f"vref_merge_join_{name}")(lk.ctypes.data, nl, rk.ctypes.data, nr, lo.ctypes.data,
+                                                             ro.ctypes.data, unique))
+                assert m <= cap
+                case[f"merge{unique}"] = dict(matches=m, digest=digest(lo[:m], ro[:m]))
+            for anti in (0, 1):
+                o = np.zeros(max(nl, 1), np.uint32)
+                # the semi / anti joins assume no order: shuffle the left side for them
+                ls = inputs.shuffled(lk, seed)
+                m = int(getattr(L, f"vref_semi_join_{name}")(ls.ctypes.data, nl, rk.ctypes.data, nr, o.ctypes.data,
+                                                            anti))
+                case[f"semi{anti}"] = dict(matches=m, digest=digest(o[:m]))
+            out.append(case)
+    return out
+
+
 def C_size():
     import ctypes
     return ctypes.c_size_t(0)
@@ -325,7 +354,7 @@ def main():
         raise SystemExit("the reference library is required to generate golden vectors")
     doc = dict(source="reference VoxelVM operators compiled by oracle/build_oracle.py",
                kat=kat_cases(), config1=config1(), programs=program_cases(), ops=op_cases(),
-               codecs=codec_cases())
+               codecs=codec_cases(), joins=join_family_cases())
     with open(OUT, "w") as f:
         json.dump(doc, f, separators=(",", ":"))
     print(f"wrote {OUT}: {len(doc['programs'])} program cases, {os.path.getsize(OUT)} bytes")

@@ -143,7 +143,9 @@ def test_reference_c_example_builds_against_this_library(tmp_path):
     import shutil
     import subprocess
 
-    src = os.path.join(os.environ.get("VOXEL_REFERENCE_ROOT", "/root/reference"), "examples", "c_test.cpp")
+    from oracle import build_oracle
+
+    src = os.path.join(build_oracle.reference_root(), "examples", "c_test.cpp")
     if not os.path.exists(src) or shutil.which("g++") is None:
         pytest.skip("reference sources not present")
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -108,10 +108,13 @@ def test_noalloc_table_recovers_after_flagged_calls():
     st, got = _call(True, d, t)
     assert st == 0, capi.last_error()
     _same(got, want)
-    # an infinite price passes "price > 20" and makes a non-finite product
+    # an infinite price (with a qty in range) passes the predicate and makes a
+    # non-finite product
     bad = t["price"].clone()
     bad[1234] = float("inf")
-    tb = dict(t, price=bad)
+    badq = t["qty"].clone()
+    badq[1234] = 20
+    tb = dict(t, price=bad, qty=badq)
     st, _ = _call(True, d, tb, want_status=1)
     assert st == 0
     assert L.voxel_scan_groupby_status_code(1) == 7

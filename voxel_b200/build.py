@@ -44,6 +44,7 @@ CORE_SOURCES = [
     "groupby.cu",
     "radix.cu",
     "join.cu",
+    "mjoin.cu",
     "ops.cu",
     "estimator.cu",
     "batch.cu",

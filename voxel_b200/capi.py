@@ -127,6 +127,10 @@ _SIGS = {
     "voxel_dict_bitpack_decode_i32": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp]),
     "voxel_dict_decode": (C.c_int, [C.c_int, vp, sz, vp, sz, sz, sz, vp]),
     "voxel_rle_decode_i64": (C.c_int, [vp, vp, sz, sz, sz, vp]),
+    "voxel_merge_join": (sz, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int]),
+    "voxel_merge_join_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
+    "voxel_semi_join": (sz, [C.c_int, vp, sz, vp, sz, vp, C.c_int]),
+    "voxel_semi_join_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, C.c_int, vp, vp]),
     "voxel_delta_decode": (C.c_int, [C.c_int, vp, sz, u64, sz, sz, vp]),
     "voxel_delta_decode_dev": (C.c_int, [C.c_int, vp, sz, u64, sz, sz, vp, vp]),
     "voxel_delta_encode": (C.c_int, [C.c_int, vp, sz, vp]),

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "join.h"
+#include "join_table.cuh"
 #include "radix.h"
 #include "voxel_c.h"
 #include "vx_common.cuh"
@@ -27,19 +28,6 @@
 namespace vx {
 
 namespace {
-
-struct __align__(16) Slot {
-    int64_t key;
-    uint32_t start;
-    uint32_t len;  // 0 = empty
-};
-
-__device__ __forceinline__ uint64_t mix64(uint64_t x) {
-    // splitmix64 finaliser, the mixer HashValue<i64> uses (ops/hash.hpp:328-333)
-    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
-    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
-    return x ^ (x >> 31);
-}
 
 // sorted keys -> runs: flag the first row of every distinct key
 __global__ void run_heads_kernel(const int64_t* __restrict__ skeys, uint64_t n, uint32_t* __restrict__ head) {
@@ -75,25 +63,6 @@ __global__ void insert_runs_kernel(const int64_t* __restrict__ skeys, const uint
 constexpr int kJThreads = 256;
 constexpr int kJItems = 4;  // probes per thread (8 blocks per SM; measured best)
 constexpr int kJTile = kJThreads * kJItems;
-
-__device__ __forceinline__ Slot lookup(const Slot* __restrict__ table, uint64_t mask, int64_t k) {
-    uint64_t h = mix64(static_cast<uint64_t>(k)) & mask;
-    for (uint64_t probes = 0; probes <= mask; ++probes) {
-        Slot s;
-        const uint4 raw = __ldg(reinterpret_cast<const uint4*>(table + h));
-        s.key = static_cast<int64_t>((static_cast<uint64_t>(raw.y) << 32) | raw.x);
-        s.start = raw.z;
-        s.len = raw.w;
-        if (s.len == 0) break;
-        if (s.key == k) return s;
-        h = (h + 1) & mask;
-    }
-    Slot miss;
-    miss.key = 0;
-    miss.start = 0;
-    miss.len = 0;
-    return miss;
-}
 
 __global__ void __launch_bounds__(kJThreads, 8) probe_kernel(
     const Slot* __restrict__ table, uint64_t mask, const uint32_t* __restrict__ srows,
