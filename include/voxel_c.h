@@ -72,6 +72,12 @@ uint64_t  voxel_engine_get_scalar_i64(void* engine, size_t reg);                
  * ================================================================ */
 double    voxel_jit_run(const uint32_t* code, size_t code_len,
                         const double* data, size_t data_len, double threshold);      /* voxel_c.h:40 */
+/* Additive (the reference's pybind jit_compile, bindings/voxel_bindings.cpp:329-340):
+ * 0 when the program lowers, with jit_run's registers, onto one fused GPU
+ * kernel schedule (host code only); *schedule_bytes = the schedule's size and
+ * kernel (cap bytes) = the kernel's name; else a VOXEL_E* code. */
+int       voxel_jit_compile(const uint32_t* code, size_t code_len, size_t* schedule_bytes, char* kernel,
+                            size_t cap);
 
 /* ================================================================
  * Instruction encoding - reference bindings/voxel_c.h:46-65
@@ -237,6 +243,32 @@ int       voxel_rle_decode_i64_dev(const int64_t* d_values, const uint32_t* d_ru
 /* device variants of the dictionary decoders; they return after the kernel
  * (an index outside the dictionary is reported as VOXEL_EINVAL) */
 /* ================================================================
+ * Additive: window functions of Engine<T> (reference exec/engine.hpp:176-300)
+ * for dtype 0 f64, 2 i64, 3 i32, 4 u64, 5 u32.  kind: 0 WindowDelta, 1
+ * WindowSum, 2 WindowMean, 3 WindowStdDev, 4 WindowVariance, 5
+ * WindowQuantile (quantile in [0, 1]; the first min(window, 128) values of
+ * each window).  Every window is evaluated in the reference's operation
+ * order (left-to-right sums in T, one rounding per operation), so outputs are
+ * bit-identical.  Returns the number of outputs written, as the reference
+ * does (0 for an empty or invalid request); the _dev form stores it in
+ * *n_out and returns a status.
+ * voxel_time_window_sum: TimeWindowSum (228-241): out[(ts[i] - start) /
+ * duration] += values[i] for buckets in [0, out_len) (out is added to, not
+ * cleared); returns the largest bucket touched + 1.  f64 bucket sums are
+ * added in parallel (within 1e-12 of the reference's row order); integers
+ * are exact.
+ * ================================================================ */
+size_t    voxel_window(int dtype, int kind, const void* data, size_t count, void* out, size_t out_len,
+                       uint8_t window, double quantile);
+int       voxel_window_dev(int dtype, int kind, const void* d_data, size_t count, void* d_out, size_t out_len,
+                           uint8_t window, double quantile, size_t* n_out, void* stream);
+size_t    voxel_time_window_sum(int dtype, const int64_t* timestamps, const void* values, size_t count,
+                                int64_t start_time, int64_t duration, void* out, size_t out_len);
+int       voxel_time_window_sum_dev(int dtype, const int64_t* d_timestamps, const void* d_values, size_t count,
+                                    int64_t start_time, int64_t duration, void* d_out, size_t out_len,
+                                    size_t* n_out, void* stream);
+
+/* ================================================================
  * Additive: delta and frame-of-reference codecs.
  * DeltaEncoding<T> (reference data/encoding.hpp:281-354), T an integer type
  * (dtype 2 i64, 3 i32, 4 u64, 5 u32; base_bits = BaseValue's bits):
@@ -285,7 +317,7 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
 /* kernel variant of the calling thread's fused scan:
- *   -1 = default: the autotuner times variants 1, 2, 3 and 5 on the first
+ *   -1 = default: the autotuner times variants 1, 2, 3, 5 and 7 on the first
  *        call of each (dictionary size, row count) of 65,536 rows or more and
  *        keeps the fastest (1 for smaller scans and when tuning is off);
  *    1 / 2 = 32-bit-word group table fed by a per-warp row queue, 4 / 8 rows
@@ -295,11 +327,14 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  *        (a producer warp keeps them in flight while 16 warps aggregate); needs
  *        16-byte-aligned packed keys, at least 2048 rows, at most 2^19 rows per
  *        SM and a table that fits beside two stages, else runs variant 1;
+ *    7 = lean word table: 16-byte queue entries, MIN / MAX screened by the
+ *        high 32 bits of the order keys (scans of fewer than 2^32 rows; else 1);
  *    4 / 8 / 16 = warp-merged rows, 192-bit shared atomics, that many rows per thread;
  *    0 = TMA-fed private warp tables (dictionaries up to 1024 entries).
- * All but 0 give bit-identical results.  voxel_scan_groupby_last_variant
- * reports the kernel the last call ran: 0 warp-merged, 1 TMA-fed, 2 word table
- * with queue, 3 word table direct, 4 word table fed by bulk copies. */
+ * All but 0 give bit-identical results; the autotuner also times 7.
+ * voxel_scan_groupby_last_variant reports the kernel the last call ran: 0
+ * warp-merged, 1 TMA-fed, 2 word table with queue, 3 word table direct, 4
+ * word table fed by bulk copies, 5 lean word table. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
 /* the calling thread's current variant id (as passed to voxel_scan_groupby_tune) */

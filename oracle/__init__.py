@@ -52,6 +52,10 @@ def port() -> C.CDLL:
         L.vo_dict_build_i32.argtypes = [vp, sz, vp, vp]
         L.vo_dict_decode_i32.restype = None
         L.vo_dict_decode_i32.argtypes = [vp, sz, vp, sz, sz, sz, vp]
+        L.vo_window_f64.restype = sz
+        L.vo_window_f64.argtypes = [C.c_int, vp, sz, vp, sz, C.c_uint, dbl]
+        L.vo_time_window_sum_f64.restype = sz
+        L.vo_time_window_sum_f64.argtypes = [vp, vp, sz, i64, i64, vp, sz]
         L.vo_merge_join_i64.restype = sz
         L.vo_merge_join_i64.argtypes = [vp, sz, vp, sz, vp, vp, sz, C.c_int]
         L.vo_semi_join_i64.restype = sz
@@ -158,6 +162,13 @@ def ref() -> C.CDLL:
             f = getattr(L, f"vref_semi_join_{t}")
             f.restype = sz
             f.argtypes = [vp, sz, vp, sz, vp, C.c_int]
+        for t in ("f64", "i64", "i32", "u64", "u32"):
+            f = getattr(L, f"vref_window_{t}")
+            f.restype = sz
+            f.argtypes = [C.c_int, vp, sz, vp, sz, C.c_uint8, dbl]
+            f = getattr(L, f"vref_time_window_sum_{t}")
+            f.restype = sz
+            f.argtypes = [vp, vp, sz, i64, i64, vp, sz]
         L.vref_scalar_filter_gt_f32.restype = sz
         L.vref_scalar_filter_gt_f32.argtypes = [vp, vp, C.c_float, sz]
         L.vref_scalar_sum_f32.restype = C.c_float

@@ -201,6 +201,20 @@ size_t semi_join_t(const T* l, size_t nl, const T* r, size_t nr, uint32_t* out, 
     return m;
 }
 
+// exec/engine.hpp:176-300 (Engine<T>::WindowDelta / Sum / Mean / StdDev /
+// Variance / Quantile and TimeWindowSum, static members)
+template <typename T>
+size_t window_t(int kind, const T* d, size_t n, T* out, size_t outLen, uint8_t w, double q) {
+    switch (kind) {
+    case 0: return Engine<T>::WindowDelta(d, n, out, outLen);
+    case 1: return Engine<T>::WindowSum(d, n, out, outLen, w);
+    case 2: return Engine<T>::WindowMean(d, n, out, outLen, w);
+    case 3: return Engine<T>::WindowStdDev(d, n, out, outLen, w);
+    case 4: return Engine<T>::WindowVariance(d, n, out, outLen, w);
+    default: return Engine<T>::WindowQuantile(d, n, out, outLen, w, q);
+    }
+}
+
 extern "C" {
 
 int vref_engine_run(int dtype, const uint32_t* code, size_t len, const void* const* segs,
@@ -383,6 +397,17 @@ size_t vref_semi_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t 
 size_t vref_semi_join_i32(const int32_t* l, size_t nl, const int32_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<i32>(l, nl, r, nr, o, a); }
 size_t vref_semi_join_u64(const uint64_t* l, size_t nl, const uint64_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<u64>(l, nl, r, nr, o, a); }
 size_t vref_semi_join_u32(const uint32_t* l, size_t nl, const uint32_t* r, size_t nr, uint32_t* o, int a) { return semi_join_t<u32>(l, nl, r, nr, o, a); }
+
+size_t vref_window_f64(int k, const double* d, size_t n, double* o, size_t ol, uint8_t w, double q) { return window_t<f64>(k, d, n, o, ol, w, q); }
+size_t vref_window_i64(int k, const int64_t* d, size_t n, int64_t* o, size_t ol, uint8_t w, double q) { return window_t<i64>(k, d, n, o, ol, w, q); }
+size_t vref_window_i32(int k, const int32_t* d, size_t n, int32_t* o, size_t ol, uint8_t w, double q) { return window_t<i32>(k, d, n, o, ol, w, q); }
+size_t vref_window_u64(int k, const uint64_t* d, size_t n, uint64_t* o, size_t ol, uint8_t w, double q) { return window_t<u64>(k, d, n, o, ol, w, q); }
+size_t vref_window_u32(int k, const uint32_t* d, size_t n, uint32_t* o, size_t ol, uint8_t w, double q) { return window_t<u32>(k, d, n, o, ol, w, q); }
+size_t vref_time_window_sum_f64(const int64_t* ts, const double* v, size_t n, int64_t st, int64_t dur, double* o, size_t ol) { return Engine<f64>::TimeWindowSum(ts, v, n, st, dur, o, ol); }
+size_t vref_time_window_sum_i64(const int64_t* ts, const int64_t* v, size_t n, int64_t st, int64_t dur, int64_t* o, size_t ol) { return Engine<i64>::TimeWindowSum(ts, v, n, st, dur, o, ol); }
+size_t vref_time_window_sum_i32(const int64_t* ts, const int32_t* v, size_t n, int64_t st, int64_t dur, int32_t* o, size_t ol) { return Engine<i32>::TimeWindowSum(ts, v, n, st, dur, o, ol); }
+size_t vref_time_window_sum_u64(const int64_t* ts, const uint64_t* v, size_t n, int64_t st, int64_t dur, uint64_t* o, size_t ol) { return Engine<u64>::TimeWindowSum(ts, v, n, st, dur, o, ol); }
+size_t vref_time_window_sum_u32(const int64_t* ts, const uint32_t* v, size_t n, int64_t st, int64_t dur, uint32_t* o, size_t ol) { return Engine<u32>::TimeWindowSum(ts, v, n, st, dur, o, ol); }
 
 // filter.hpp:378-399 (SelectionVector::BuildFromBitmap)
 size_t vref_selection_from_bitmap(const uint64_t* bm, size_t rows, uint32_t* out) {

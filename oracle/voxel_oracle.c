@@ -766,3 +766,68 @@ size_t vo_semi_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr
     free(s);
     return m;
 }
+
+/* exec/engine.hpp:182-300 (Engine<f64>::WindowDelta .. WindowQuantile): each
+   window summed left to right, mean = sum / w, ssq = sum of (x - mean)^2,
+   quantile from the sorted first min(w, 128) values with linear
+   interpolation.  kind 0 delta, 1 sum, 2 mean, 3 stddev, 4 variance, 5
+   quantile.  Returns the outputs written. */
+static int cmp_f64(const void* a, const void* b) {
+    double x = *(const double*)a, y = *(const double*)b;
+    return x < y ? -1 : x > y;
+}
+
+size_t vo_window_f64(int kind, const double* d, size_t n, double* out, size_t out_len, unsigned w, double q) {
+    if (kind == 0) {
+        if (n < 2) return 0;
+        size_t m = n - 1 < out_len ? n - 1 : out_len;
+        for (size_t i = 0; i < m; ++i) out[i] = d[i + 1] - d[i];
+        return m;
+    }
+    if (w == 0 || n < w) return 0;
+    if (kind >= 3 && w < 2) return 0;
+    if (kind == 5 && !(q >= 0.0 && q <= 1.0)) return 0;
+    size_t m = n - w + 1 < out_len ? n - w + 1 : out_len;
+    for (size_t j = 0; j < m; ++j) {
+        if (kind == 5) {
+            double buf[128];
+            size_t ww = w < 128 ? w : 128;
+            for (size_t k = 0; k < ww; ++k) buf[k] = d[j + k];
+            qsort(buf, ww, 8, cmp_f64);
+            double pos = q * (double)(ww - 1);
+            size_t lo = (size_t)pos;
+            if (lo >= ww) lo = ww - 1;
+            size_t hi = lo + 1;
+            if (hi >= ww) hi = lo;
+            if (lo == hi) { out[j] = buf[lo]; continue; }
+            volatile double t = (buf[hi] - buf[lo]) * (pos - (double)lo);
+            out[j] = buf[lo] + t;
+            continue;
+        }
+        double sum = 0.0;
+        for (size_t k = 0; k < w; ++k) sum += d[j + k];
+        if (kind == 1) { out[j] = sum; continue; }
+        double mean = sum / (double)w;
+        if (kind == 2) { out[j] = mean; continue; }
+        double ssq = 0.0;
+        for (size_t k = 0; k < w; ++k) { volatile double dd = d[j + k] - mean; volatile double p = dd * dd; ssq += p; }
+        out[j] = kind == 4 ? ssq / (double)w : sqrt(ssq / (double)w);
+    }
+    return m;
+}
+
+/* exec/engine.hpp:228-241 (TimeWindowSum): out[(ts - start) / dur] += v for
+   buckets in [0, out_len), in row order; returns the largest bucket + 1. */
+size_t vo_time_window_sum_f64(const int64_t* ts, const double* v, size_t n, int64_t start, int64_t dur, double* out,
+                              size_t out_len) {
+    if (dur <= 0 || n == 0 || out_len == 0) return 0;
+    size_t maxb = 0;
+    for (size_t i = 0; i < n; ++i) {
+        int64_t b = (ts[i] - start) / dur;
+        if (b >= 0 && (size_t)b < out_len) {
+            out[b] += v[i];
+            if ((size_t)b > maxb) maxb = (size_t)b;
+        }
+    }
+    return maxb + 1;
+}

@@ -62,6 +62,9 @@ void vo_dict_decode_i32(const int32_t* dict, size_t card, const uint32_t* idx, s
 /* RLEEncoding<i64> (encoding.hpp:202-257); returns the run count. */
 size_t vo_rle_build_i64(const int64_t* data, size_t n, int64_t* values, uint32_t* runs);
 void vo_delta_build(int w, const void* data, size_t n, void* deltas);
+size_t vo_window_f64(int kind, const double* d, size_t n, double* out, size_t out_len, unsigned w, double q);
+size_t vo_time_window_sum_f64(const int64_t* ts, const double* v, size_t n, int64_t start, int64_t dur, double* out,
+                              size_t out_len);
 size_t vo_merge_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* lo, uint32_t* ro,
                          size_t cap, int unique);
 size_t vo_semi_join_i64(const int64_t* l, size_t nl, const int64_t* r, size_t nr, uint32_t* out, int anti);

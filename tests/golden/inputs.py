@@ -184,3 +184,25 @@ def merge_join_input(npt, nl: int, nr: int, dup: int, seed: int):
 def shuffled(a: np.ndarray, seed: int) -> np.ndarray:
     """A seeded permutation of `a` (the semi / anti joins' unordered left side)."""
     return np.random.default_rng(seed + 1).permutation(a) if a.size else a
+
+
+WINDOW_NP = {0: np.float64, 2: np.int64, 3: np.int32, 4: np.uint64, 5: np.uint32}
+
+
+def window_values(dtype: int, n: int, seed: int) -> np.ndarray:
+    """A noisy trend with repeats (ties for the quantile), per element type."""
+    rng = np.random.default_rng(seed)
+    base = np.cumsum(rng.normal(0.0, 3.0, n)) + rng.integers(0, 5, n) * 0.5
+    if dtype == 0:
+        return base.astype(np.float64)
+    v = np.round(base * 1000).astype(np.int64)
+    if dtype in (4, 5):
+        v = np.abs(v)
+    return v.astype(WINDOW_NP[dtype])
+
+
+def time_window_input(dtype: int, n: int, seed: int):
+    """Non-decreasing i64 timestamps (steps 0-3) and values of the element type."""
+    rng = np.random.default_rng(seed)
+    ts = np.cumsum(rng.integers(0, 4, n)).astype(np.int64) - 50
+    return ts, window_values(dtype, n, seed + 7)

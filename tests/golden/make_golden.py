@@ -330,6 +330,45 @@ def join_family_cases():
     return out
 
 
+def window_cases():
+    """Engine<T>::Window* and TimeWindowSum run by the reference."""
+    L = oracle.ref()
+    rng = np.random.default_rng(9301)
+    out = []
+    for name, dt in (("f64", 0), ("i64", 2), ("i32", 3), ("u64", 4), ("u32", 5)):
+        for n in (0, 1, 3, 9, 1000, 70_001):
+            seed = int(rng.integers(1 << 31))
+            x = inputs.window_values(dt, n, seed)
+            for kind in range(6):
+                for w, q in ((1, 0.5), (2, 0.0), (3, 1.0), (8, 0.25), (37, 0.9), (255, 0.5)):
+                    if kind == 0 and w != 2:
+                        continue
+                    for out_len in (n, max(n // 3, 1)):
+                        o = np.zeros(max(out_len, 1), x.dtype)
+                        m = int(getattr(L, f"vref_window_{name}")(kind, x.ctypes.data, n, o.ctypes.data, out_len, w,
+                                                                 q))
+                        out.append(dict(dtype=dt, n=n, seed=seed, kind=kind, window=w, q=q, out_len=out_len,
+                                        written=m, digest=digest(o[:m])))
+    tw = []
+    for name, dt in (("f64", 0), ("i64", 2), ("i32", 3), ("u64", 4), ("u32", 5)):
+        for n, dur, start in ((0, 10, 0), (100, 7, 3), (5000, 60, -100), (50_000, 1, 0)):
+            seed = int(rng.integers(1 << 31))
+            ts, v = inputs.time_window_input(dt, n, seed)
+            for out_len in (1, 64, 10_000):
+                if dt == 0 and n * out_len > 100_000_000:
+                    continue  # f64 buckets are stored as values: keep the fixture small
+                o = np.zeros(out_len, v.dtype)
+                o[:] = inputs.window_values(dt, out_len, seed + 1)[:out_len] if out_len else o
+                o0 = o.copy()
+                m = int(getattr(L, f"vref_time_window_sum_{name}")(ts.ctypes.data, v.ctypes.data, n, start, dur,
+                                                                  o.ctypes.data, out_len))
+                changed = np.flatnonzero(o != o0) if dt == 0 else np.zeros(0, np.int64)
+                tw.append(dict(dtype=dt, n=n, seed=seed, start=start, duration=dur, out_len=out_len, returned=m,
+                               changed=[[int(i), float(o[i])] for i in changed] if dt == 0 else None,
+                               digest=digest(o) if dt != 0 else None, init_digest=digest(o0)))
+    return dict(windows=out, time_windows=tw)
+
+
 def C_size():
     import ctypes
     return ctypes.c_size_t(0)
@@ -354,7 +393,7 @@ def main():
         raise SystemExit("the reference library is required to generate golden vectors")
     doc = dict(source="reference VoxelVM operators compiled by oracle/build_oracle.py",
                kat=kat_cases(), config1=config1(), programs=program_cases(), ops=op_cases(),
-               codecs=codec_cases(), joins=join_family_cases())
+               codecs=codec_cases(), joins=join_family_cases(), windows=window_cases())
     with open(OUT, "w") as f:
         json.dump(doc, f, separators=(",", ":"))
     print(f"wrote {OUT}: {len(doc['programs'])} program cases, {os.path.getsize(OUT)} bytes")

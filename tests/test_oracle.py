@@ -271,3 +271,28 @@ def test_join_family_restatement_against_reference(golden):
             o = np.zeros(max(ls.size, 1), np.uint32)
             m = P.vo_semi_join_i64(ls.ctypes.data, ls.size, rk.ctypes.data, rk.size, o.ctypes.data, anti)
             assert m == want["matches"] and hashlib.sha256(o[:m].tobytes()).hexdigest() == want["digest"]
+
+
+def test_window_restatement_against_reference(golden):
+    """The restated f64 window functions reproduce the reference's
+    Engine<f64>::Window* outputs bit for bit, and TimeWindowSum's buckets."""
+    P = oracle.port()
+    for c in golden["windows"]["windows"]:
+        if c["dtype"] != 0:
+            continue
+        x = inputs.window_values(0, c["n"], c["seed"])
+        o = np.zeros(max(c["out_len"], 1))
+        m = P.vo_window_f64(c["kind"], x.ctypes.data, c["n"], o.ctypes.data, c["out_len"], c["window"], c["q"])
+        assert m == c["written"], c
+        assert hashlib.sha256(o[:m].tobytes()).hexdigest() == c["digest"], c
+    for c in golden["windows"]["time_windows"]:
+        if c["dtype"] != 0:
+            continue
+        ts, v = inputs.time_window_input(0, c["n"], c["seed"])
+        o = inputs.window_values(0, c["out_len"], c["seed"] + 1)[: c["out_len"]].copy()
+        assert hashlib.sha256(o.tobytes()).hexdigest() == c["init_digest"]
+        m = P.vo_time_window_sum_f64(ts.ctypes.data, v.ctypes.data, c["n"], c["start"], c["duration"],
+                                     o.ctypes.data, c["out_len"])
+        assert m == c["returned"]
+        for i, val in c["changed"]:
+            assert o[i] == val

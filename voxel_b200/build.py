@@ -45,6 +45,7 @@ CORE_SOURCES = [
     "radix.cu",
     "join.cu",
     "mjoin.cu",
+    "window.cu",
     "ops.cu",
     "estimator.cu",
     "batch.cu",

@@ -127,6 +127,11 @@ _SIGS = {
     "voxel_dict_bitpack_decode_i32": (C.c_int, [vp, sz, u32, vp, sz, sz, sz, sz, vp]),
     "voxel_dict_decode": (C.c_int, [C.c_int, vp, sz, vp, sz, sz, sz, vp]),
     "voxel_rle_decode_i64": (C.c_int, [vp, vp, sz, sz, sz, vp]),
+    "voxel_jit_compile": (C.c_int, [vp, sz, C.POINTER(sz), C.c_char_p, sz]),
+    "voxel_window": (sz, [C.c_int, C.c_int, vp, sz, vp, sz, C.c_uint8, dbl]),
+    "voxel_window_dev": (C.c_int, [C.c_int, C.c_int, vp, sz, vp, sz, C.c_uint8, dbl, C.POINTER(sz), vp]),
+    "voxel_time_window_sum": (sz, [C.c_int, vp, vp, sz, i64, i64, vp, sz]),
+    "voxel_time_window_sum_dev": (C.c_int, [C.c_int, vp, vp, sz, i64, i64, vp, sz, C.POINTER(sz), vp]),
     "voxel_merge_join": (sz, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int]),
     "voxel_merge_join_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
     "voxel_semi_join": (sz, [C.c_int, vp, sz, vp, sz, vp, C.c_int]),

@@ -1,0 +1,415 @@
+// Window functions of Engine<T> (reference include/voxel/exec/engine.hpp:176-300).
+//
+//   WindowDelta (182-192):    out[i] = data[i+1] - data[i], i < min(count-1, outLen).
+//   WindowSum (195-214):      out[j] = data[j] + ... + data[j+w-1], summed left to
+//                             right in T, j < min(count-w+1, outLen); w >= 1.
+//   WindowMean (217-222):     WindowSum, then out[j] /= (T)w.
+//   TimeWindowSum (228-241):  out[(ts[i] - start) / dur] += values[i] for buckets in
+//                             [0, outLen) (C++ division: truncation toward zero);
+//                             returns the largest bucket touched + 1 (1 if none).
+//   WindowStdDev / Variance (244-275): per window, sum -> mean = sum / w ->
+//                             ssq = sum of (x - mean)^2, all in T; out = sqrt(ssq / w)
+//                             (integers: the double square root truncated back to T)
+//                             or ssq / w; w >= 2.
+//   WindowQuantile (278-300): the first min(w, 128) values of each window; pos =
+//                             q * (w'-1), lo = floor(pos), hi = lo + 1 (clamped);
+//                             vLo, vHi = the lo-th and hi-th smallest; out = vLo +
+//                             (T)((f64)(vHi - vLo) * (pos - lo)); w >= 2, 0 <= q <= 1.
+//
+// Each window is evaluated in exactly the reference's operation order (the same
+// left-to-right sums, one rounding per operation, no fused multiply-add), so the
+// outputs are bit-identical for every element type.  B200 design: blocks stage a
+// tile of outputs plus its halo of w-1 inputs in shared memory with coalesced
+// loads, and each thread evaluates windows from there (O(w) shared reads per
+// output, as the definition is); the quantile keeps each thread's window sorted
+// in local memory and slides it (one removal and one insertion per output);
+// the time-bucketed sum reduces runs of equal buckets in registers and warps
+// and adds them to the output with global atomics.
+#include <cmath>
+#include <cstdint>
+#include <type_traits>
+
+#include "voxel_c.h"
+#include "vx_common.cuh"
+#include "vx_runtime.h"
+
+namespace vx {
+
+namespace {
+
+constexpr int kWThreads = 256;
+constexpr int kWTile = 2048;    // outputs per block step
+constexpr int kWMaxWin = 256;   // u8 windows: at most 255 inputs per window
+constexpr int kQMax = 128;      // WindowQuantile's buffer (engine.hpp:284)
+constexpr int kQRun = 32;       // consecutive quantile outputs per thread
+
+enum WinKind : int { kDelta = 0, kSum = 1, kMean = 2, kStdDev = 3, kVariance = 4, kQuantile = 5 };
+
+template <typename T>
+__device__ __forceinline__ T w_add(T a, T b) {
+    if constexpr (std::is_same<T, double>::value) return __dadd_rn(a, b);
+    else return static_cast<T>(a + b);
+}
+template <typename T>
+__device__ __forceinline__ T w_sub(T a, T b) {
+    if constexpr (std::is_same<T, double>::value) return __dsub_rn(a, b);
+    else return static_cast<T>(a - b);
+}
+template <typename T>
+__device__ __forceinline__ T w_mul(T a, T b) {
+    if constexpr (std::is_same<T, double>::value) return __dmul_rn(a, b);
+    else return static_cast<T>(a * b);
+}
+template <typename T>
+__device__ __forceinline__ T w_div(T a, T b) {
+    if constexpr (std::is_same<T, double>::value) return __ddiv_rn(a, b);
+    else return static_cast<T>(a / b);
+}
+template <typename T>
+__device__ __forceinline__ T w_sqrt(T a) {
+    if constexpr (std::is_same<T, double>::value) return __dsqrt_rn(a);
+    else return static_cast<T>(__dsqrt_rn(static_cast<double>(a)));  // std::sqrt of an integer, back to T
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kWThreads) window_kernel(const T* __restrict__ data, uint64_t nout, uint32_t w,
+                                                           T* __restrict__ out) {
+    __shared__ T s[kWTile + kWMaxWin];
+    const uint32_t halo = KIND == kDelta ? 1u : w - 1u;
+    const T tw = static_cast<T>(w);
+    for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kWTile; t0 < nout;
+         t0 += static_cast<uint64_t>(gridDim.x) * kWTile) {
+        const uint32_t nt = static_cast<uint32_t>(nout - t0 < kWTile ? nout - t0 : kWTile);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nt + halo; i += blockDim.x) s[i] = __ldg(data + t0 + i);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nt; j += blockDim.x) {
+            T r;
+            if constexpr (KIND == kDelta) {
+                r = w_sub<T>(s[j + 1], s[j]);
+            } else {
+                T sum = T(0);
+                for (uint32_t k = 0; k < w; ++k) sum = w_add<T>(sum, s[j + k]);
+                if constexpr (KIND == kSum) {
+                    r = sum;
+                } else if constexpr (KIND == kMean) {
+                    r = w_div<T>(sum, tw);
+                } else {
+                    const T mean = w_div<T>(sum, tw);
+                    T ssq = T(0);
+                    for (uint32_t k = 0; k < w; ++k) {
+                        const T d = w_sub<T>(s[j + k], mean);
+                        ssq = w_add<T>(ssq, w_mul<T>(d, d));
+                    }
+                    r = KIND == kVariance ? w_div<T>(ssq, tw) : w_sqrt<T>(w_div<T>(ssq, tw));
+                }
+            }
+            out[t0 + j] = r;
+        }
+    }
+}
+
+// first index in buf[0, n) with buf[i] >= v (strict weak order of T)
+template <typename T>
+__device__ __forceinline__ int lower_idx(const T* buf, int n, T v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (buf[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWThreads) quantile_kernel(const T* __restrict__ data, uint64_t nout, int wq,
+                                                             int lo, int hi, double frac, T* __restrict__ out) {
+    T buf[kQMax];
+    const uint64_t nruns = (nout + kQRun - 1) / kQRun;
+    for (uint64_t run = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; run < nruns;
+         run += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t j0 = run * kQRun;
+        const uint64_t j1 = j0 + kQRun < nout ? j0 + kQRun : nout;
+        // the first window, insertion-sorted
+        for (int k = 0; k < wq; ++k) {
+            const T v = __ldg(data + j0 + k);
+            int p = k;
+            while (p > 0 && v < buf[p - 1]) {
+                buf[p] = buf[p - 1];
+                --p;
+            }
+            buf[p] = v;
+        }
+        for (uint64_t j = j0; j < j1; ++j) {
+            const T vlo = buf[lo];
+            T r = vlo;
+            if (lo != hi) {
+                const T vhi = buf[hi];
+                if constexpr (std::is_same<T, double>::value) {
+                    r = __dadd_rn(vlo, __dmul_rn(__dsub_rn(vhi, vlo), frac));
+                } else {
+                    const double d = static_cast<double>(static_cast<T>(vhi - vlo));
+                    r = static_cast<T>(vlo + static_cast<T>(__dmul_rn(d, frac)));
+                }
+            }
+            out[j] = r;
+            if (j + 1 < j1) {  // slide: drop data[j], take data[j + wq]
+                const T gone = __ldg(data + j), come = __ldg(data + j + wq);
+                int p = lower_idx<T>(buf, wq, gone);
+                if (p >= wq) p = wq - 1;  // NaN-free input always finds it
+                for (int q = p; q + 1 < wq; ++q) buf[q] = buf[q + 1];
+                int ins = lower_idx<T>(buf, wq - 1, come);
+                for (int q = wq - 1; q > ins; --q) buf[q] = buf[q - 1];
+                buf[ins] = come;
+            }
+        }
+    }
+}
+
+// out[bucket] += values[i]; *maxb = max bucket touched.  Each thread sums its
+// rows' runs of equal buckets (ts is meant to be non-decreasing, so runs are
+// long); a warp whose 32 threads all hold one run of one bucket adds it once.
+constexpr int kTRows = 16;
+
+template <typename T>
+__device__ __forceinline__ void add_out(T* out, uint64_t b, T v) {
+    if constexpr (std::is_same<T, double>::value) atomicAdd(out + b, v);
+    else if constexpr (sizeof(T) == 8) atomicAdd(reinterpret_cast<unsigned long long*>(out + b), static_cast<unsigned long long>(v));
+    else atomicAdd(reinterpret_cast<unsigned int*>(out + b), static_cast<unsigned int>(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = w_add<T>(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWThreads) time_window_kernel(const int64_t* __restrict__ ts,
+                                                                const T* __restrict__ vals, uint64_t n,
+                                                                int64_t start, int64_t dur, uint64_t nout,
+                                                                T* __restrict__ out, unsigned long long* maxb) {
+    const uint64_t nchunks = (n + kTRows - 1) / kTRows;
+    uint64_t mymax = 0;
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps_total = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t w0 = static_cast<uint64_t>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    for (uint64_t wb = w0; wb * 32 < nchunks; wb += nwarps_total) {  // warp-uniform loop
+        const uint64_t chunk = wb * 32 + lane;
+        const uint64_t r0 = chunk * kTRows;
+        int64_t cur = -1;
+        T acc = T(0);
+        bool single = true;  // this thread's rows: one valid bucket (or no rows)
+        int64_t first = -1;
+        for (int k = 0; k < kTRows; ++k) {
+            const uint64_t i = r0 + k;
+            if (i >= n) break;
+            const int64_t b = (ts[i] - start) / dur;
+            if (b < 0 || static_cast<uint64_t>(b) >= nout) {
+                single = false;
+                continue;
+            }
+            if (static_cast<uint64_t>(b) > mymax) mymax = static_cast<uint64_t>(b);
+            if (b != cur) {
+                if (cur >= 0) {
+                    add_out<T>(out, static_cast<uint64_t>(cur), acc);
+                    single = false;
+                }
+                if (first < 0) first = b;
+                cur = b;
+                acc = T(0);
+            }
+            acc = w_add<T>(acc, vals[i]);
+        }
+        // the whole warp on one bucket: one atomic
+        const int64_t b0 = __shfl_sync(0xffffffffu, cur, 0);
+        const bool same = single && cur == b0 && first == cur && cur >= 0;
+        if (__all_sync(0xffffffffu, same)) {
+            const T s = warp_sum<T>(acc);
+            if (lane == 0) add_out<T>(out, static_cast<uint64_t>(b0), s);
+        } else if (cur >= 0) {
+            add_out<T>(out, static_cast<uint64_t>(cur), acc);
+        }
+    }
+    unsigned long long m = mymax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+        m = y > m ? y : m;
+    }
+    if (lane == 0 && m) atomicMax(maxb, m);
+}
+
+int w_grid(uint64_t work, int per_sm = 8) {
+    const int sms = sm_count() > 0 ? sm_count() : 148;
+    const uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
+    return static_cast<int>(work < 1 ? 1 : (work < cap ? work : cap));
+}
+
+bool win_type(int dtype) { return dtype == F64 || dtype == I64 || dtype == I32 || dtype == U64 || dtype == U32; }
+
+// number of outputs the reference writes (0: nothing)
+uint64_t win_count(int kind, uint64_t count, uint64_t out_len, uint32_t w, double q) {
+    if (kind == kDelta) return count < 2 ? 0 : (count - 1 < out_len ? count - 1 : out_len);
+    if (w == 0 || count < w) return 0;
+    if ((kind == kStdDev || kind == kVariance || kind == kQuantile) && w < 2) return 0;
+    if (kind == kQuantile && !(q >= 0.0 && q <= 1.0)) return 0;
+    const uint64_t nw = count - w + 1;
+    return nw < out_len ? nw : out_len;
+}
+
+template <typename T>
+int launch_t(int kind, const void* d_data, uint64_t nout, uint32_t w, double q, void* d_out, cudaStream_t s) {
+    const T* in = static_cast<const T*>(d_data);
+    T* o = static_cast<T*>(d_out);
+    const uint64_t tiles = (nout + kWTile - 1) / kWTile;
+    switch (kind) {
+    case kDelta: window_kernel<T, kDelta><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
+    case kSum: window_kernel<T, kSum><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
+    case kMean: window_kernel<T, kMean><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
+    case kStdDev: window_kernel<T, kStdDev><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
+    case kVariance: window_kernel<T, kVariance><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
+    default: {
+        const int wq = static_cast<int>(w < static_cast<uint32_t>(kQMax) ? w : kQMax);
+        const double pos = q * static_cast<double>(wq - 1);
+        int lo = static_cast<int>(pos);
+        if (lo >= wq) lo = wq - 1;
+        int hi = lo + 1;
+        if (hi >= wq) hi = lo;
+        const double frac = pos - static_cast<double>(lo);
+        const uint64_t runs = (nout + kQRun - 1) / kQRun;
+        quantile_kernel<T><<<w_grid((runs + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(in, nout, wq, lo, hi,
+                                                                                            frac, o);
+        break;
+    }
+    }
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int launch_window(int dtype, int kind, const void* d_data, uint64_t nout, uint32_t w, double q, void* d_out,
+                  cudaStream_t s) {
+    if (!nout) return kOk;
+    switch (dtype) {
+    case F64: return launch_t<double>(kind, d_data, nout, w, q, d_out, s);
+    case I64: return launch_t<int64_t>(kind, d_data, nout, w, q, d_out, s);
+    case I32: return launch_t<int32_t>(kind, d_data, nout, w, q, d_out, s);
+    case U64: return launch_t<uint64_t>(kind, d_data, nout, w, q, d_out, s);
+    default: return launch_t<uint32_t>(kind, d_data, nout, w, q, d_out, s);
+    }
+}
+
+int check_args(int dtype, int kind) {
+    if (!win_type(dtype)) {
+        set_error(kErrInvalidArg, "window functions: element type %d has no engine (f64, i64, i32, u64, u32)", dtype);
+        return kErrInvalidArg;
+    }
+    if (kind < kDelta || kind > kQuantile) {
+        set_error(kErrInvalidArg, "window function kind %d outside 0..5", kind);
+        return kErrInvalidArg;
+    }
+    return kOk;
+}
+
+template <typename T>
+int launch_time_t(const int64_t* ts, const void* vals, uint64_t n, int64_t start, int64_t dur, void* out,
+                  uint64_t nout, unsigned long long* maxb, cudaStream_t s) {
+    const uint64_t chunks = (n + kTRows - 1) / kTRows;
+    time_window_kernel<T><<<w_grid((chunks + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(
+        ts, static_cast<const T*>(vals), n, start, dur, nout, static_cast<T*>(out), maxb);
+    VX_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int launch_time_window(int dtype, const int64_t* ts, const void* vals, uint64_t n, int64_t start, int64_t dur,
+                       void* out, uint64_t nout, unsigned long long* maxb, cudaStream_t s) {
+    switch (dtype) {
+    case F64: return launch_time_t<double>(ts, vals, n, start, dur, out, nout, maxb, s);
+    case I64: return launch_time_t<int64_t>(ts, vals, n, start, dur, out, nout, maxb, s);
+    case I32: return launch_time_t<int32_t>(ts, vals, n, start, dur, out, nout, maxb, s);
+    case U64: return launch_time_t<uint64_t>(ts, vals, n, start, dur, out, nout, maxb, s);
+    default: return launch_time_t<uint32_t>(ts, vals, n, start, dur, out, nout, maxb, s);
+    }
+}
+
+}  // namespace
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+int voxel_window_dev(int dtype, int kind, const void* d_data, size_t count, void* d_out, size_t out_len,
+                     uint8_t window, double quantile, size_t* n_out, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    if (int st = check_args(dtype, kind)) return st;
+    const uint64_t nout = win_count(kind, count, out_len, window, quantile);
+    if (n_out) *n_out = nout;
+    return launch_window(dtype, kind, d_data, nout, window, quantile, d_out, static_cast<cudaStream_t>(stream));
+}
+
+size_t voxel_window(int dtype, int kind, const void* data, size_t count, void* out, size_t out_len, uint8_t window,
+                    double quantile) {
+    clear_error();
+    if (ensure_device() || check_args(dtype, kind)) return 0;
+    const uint64_t nout = win_count(kind, count, out_len, window, quantile);
+    if (!nout) return 0;
+    const uint64_t nin = kind == kDelta ? nout + 1 : nout + window - 1;  // inputs the outputs read
+    const size_t es = dtype_size(dtype);
+    cudaStream_t s = thread_stream();
+    DevBuf din(nin * es), dout(nout * es);
+    if (!din.ok(nin * es) || !dout.ok(nout * es)) return 0;
+    if (h2d(din.p, data, nin * es, s)) return 0;
+    if (launch_window(dtype, kind, din.p, nout, window, quantile, dout.p, s)) return 0;
+    if (d2h(out, dout.p, nout * es, s) || sync(s)) return 0;
+    return nout;
+}
+
+int voxel_time_window_sum_dev(int dtype, const int64_t* d_ts, const void* d_values, size_t count, int64_t start,
+                              int64_t duration, void* d_out, size_t out_len, size_t* n_out, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    if (int st = check_args(dtype, kSum)) return st;
+    if (duration <= 0 || count == 0 || out_len == 0) {
+        if (n_out) *n_out = 0;
+        return kOk;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static thread_local DevBuf mb;
+    if (!mb.p) {
+        mb = DevBuf(16);
+        if (!mb.p) return kErrOutOfMemory;
+    }
+    VX_CUDA(cudaMemsetAsync(mb.p, 0, 8, s));
+    if (int st = launch_time_window(dtype, d_ts, d_values, count, start, duration, d_out, out_len,
+                                    mb.as<unsigned long long>(), s))
+        return st;
+    uint64_t m = 0;
+    if (int st = d2h(&m, mb.p, 8, s)) return st;
+    if (int st = sync(s)) return st;
+    if (n_out) *n_out = m + 1;  // engine.hpp:240: the largest bucket touched + 1
+    return kOk;
+}
+
+size_t voxel_time_window_sum(int dtype, const int64_t* ts, const void* values, size_t count, int64_t start,
+                             int64_t duration, void* out, size_t out_len) {
+    clear_error();
+    if (ensure_device() || check_args(dtype, kSum)) return 0;
+    if (duration <= 0 || count == 0 || out_len == 0) return 0;
+    const size_t es = dtype_size(dtype);
+    cudaStream_t s = thread_stream();
+    DevBuf dts(count * 8), dv(count * es), dout(out_len * es);
+    if (!dts.ok(count * 8) || !dv.ok(count * es) || !dout.ok(out_len * es)) return 0;
+    if (h2d(dts.p, ts, count * 8, s) || h2d(dv.p, values, count * es, s) || h2d(dout.p, out, out_len * es, s))
+        return 0;
+    size_t n = 0;
+    if (voxel_time_window_sum_dev(dtype, dts.as<int64_t>(), dv.p, count, start, duration, dout.p, out_len, &n, s))
+        return 0;
+    if (d2h(out, dout.p, out_len * es, s) || sync(s)) return 0;
+    return n;
+}
+
+}  // extern "C"
