@@ -105,3 +105,55 @@ def test_operators():
     assert nb.is_null(5) and nb.null_count() == 1 and nb.valid_count() == 99
     nb.set_all_null()
     assert nb.null_count() == 100
+
+
+def test_jit_compile_and_segment_view():
+    """jit_compile reports whether a program lowers onto one fused kernel
+    (bindings/voxel_bindings.cpp:329-340; host code, no device work), and
+    SegmentF64 is a borrowed view of an f64 buffer (97-103)."""
+    r = V.jit_compile(bc.filter_sum_program())
+    assert r["compiled"] is True and r["code_size"] > 0 and r["kernel"] == "fsum"
+    # jit_run sets R0-R3 only: with R4 = 0 the SUM + COUNT loop never advances,
+    # and the reference's JIT compiles only the fused filter+sum pattern
+    assert V.jit_compile(bc.filter_sum_count_program()) == {"compiled": False}
+    bad = [bc.vload(0, 1, 0), bc.enc(0x80, 6, 6, 0), bc.add(1, 1, 4), bc.cmp(1, 2), bc.jnz(-4), bc.halt()]
+    assert V.jit_compile(bad) == {"compiled": False}
+    x = np.arange(10, dtype=np.float64) * 1.5
+    s = V.SegmentF64(x)
+    assert len(s) == 10 and s.size == 10 and s[3] == 4.5
+    s2 = V.SegmentF64(x, 4)
+    assert len(s2) == 4 and s2[3] == 4.5
+    with pytest.raises(IndexError):
+        s2[4]
+    assert len(V.SegmentF64()) == 0
+    for name in ("window_delta", "window_sum", "window_mean", "window_stddev", "window_variance",
+                 "window_quantile", "time_window_sum"):
+        assert hasattr(V.EngineF64, name), name
+
+
+@pytest.mark.gpu
+def test_engine_f64_window_methods_match_reference():
+    """EngineF64's window methods (bindings/voxel_bindings.cpp:127-171) give
+    the reference's Engine<f64>::Window* outputs bit for bit."""
+    if not oracle.have_ref():
+        pytest.skip("reference library not built")
+    R = oracle.ref()
+    rng = np.random.default_rng(5)
+    x = np.cumsum(rng.normal(size=100_003))
+    e = V.EngineF64()
+    for kind, call in ((0, lambda o: e.window_delta(x, o)), (1, lambda o: e.window_sum(x, o, 9)),
+                       (2, lambda o: e.window_mean(x, o, 9)), (3, lambda o: e.window_stddev(x, o, 12)),
+                       (4, lambda o: e.window_variance(x, o, 12)), (5, lambda o: e.window_quantile(x, o, 30, 0.75))):
+        w, q = {0: (2, 0), 1: (9, 0), 2: (9, 0), 3: (12, 0), 4: (12, 0), 5: (30, 0.75)}[kind]
+        want = np.zeros(x.size)
+        m = R.vref_window_f64(kind, x.ctypes.data, x.size, want.ctypes.data, x.size, w, q)
+        got = np.zeros(x.size)
+        assert call(got) == m
+        assert (got[:m].view(np.uint64) == want[:m].view(np.uint64)).all(), kind
+    ts = np.cumsum(rng.integers(0, 3, 5000)).astype(np.int64)
+    v = rng.normal(size=5000)
+    want = np.zeros(100)
+    m = R.vref_time_window_sum_f64(ts.ctypes.data, v.ctypes.data, 5000, 10, 37, want.ctypes.data, 100)
+    got = np.zeros(100)
+    assert e.time_window_sum(ts, v, 10, 37, got) == m
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)

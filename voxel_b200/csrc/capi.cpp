@@ -1,6 +1,8 @@
 // C ABI: engines, instruction encoders, host-side helper objects, errors.
 // (Operator entry points live next to their kernels.)
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
@@ -167,6 +169,36 @@ double voxel_jit_run(const uint32_t* code, size_t code_len, const double* data, 
     e.load_program(code, code_len);
     if (e.run() != vx::kOk) return 0.0;
     return as_f64(e.reg(0));
+}
+
+// JIT compile (reference bindings/voxel_bindings.cpp:329-340 compiles the
+// fused loop to x86 and reports its code size): here "compiled" means the
+// program lowers, with the registers jit_run sets, onto one fused GPU kernel
+// schedule.  No device work: the lowering is host code.  *schedule_bytes gets
+// the size of the lowered schedule (the kernel parameter block).
+int voxel_jit_compile(const uint32_t* code, size_t code_len, size_t* schedule_bytes, char* kernel, size_t cap) {
+    vx::clear_error();
+    static const double probe[64] = {0.0};  // any column: the lowering reads counts, not values
+    Engine e(vx::F64);
+    e.add_segment(probe, 64);
+    e.reg(0) = 0;
+    e.reg(1) = 0;
+    e.reg(2) = 64;
+    e.reg(3) = f64_bits(0.0);
+    e.load_program(code, code_len);
+    const int st = e.plan();
+    if (st) return st;
+    if (schedule_bytes) *schedule_bytes = sizeof(vx::ScanParams);
+    if (kernel && cap) {
+        const std::string& ex = e.explain();
+        const size_t k = ex.find("kernel=");
+        std::string name = k == std::string::npos ? "" : ex.substr(k + 7);
+        while (!name.empty() && (name.back() == '\n' || name.back() == ' ')) name.pop_back();
+        const size_t sp = name.find_first_of(" \n");
+        if (sp != std::string::npos) name = name.substr(0, sp);
+        std::snprintf(kernel, cap, "%s", name.c_str());
+    }
+    return vx::kOk;
 }
 
 // ---- instruction encoders (reference bindings/voxel_c.cpp:106-145) -------------

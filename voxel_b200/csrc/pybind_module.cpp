@@ -10,6 +10,7 @@
 #include <pybind11/stl.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -135,6 +136,11 @@ struct DictionaryEncodingF64 {
     ~DictionaryEncodingF64() { voxel_dict_destroy(h); }
 };
 
+struct SegmentF64 {
+    py::array_t<double, py::array::c_style | py::array::forcecast> arr;  // borrowed, like Segment<f64>
+    size_t n = 0;
+};
+
 struct RLEEncodingF64 {
     std::vector<double> values;
     std::vector<uint32_t> runs;
@@ -156,6 +162,35 @@ void bind_engine(py::module_& m, const char* name, const char* get_typed, bool f
     if (f64_scalars) {
         c.def("get_scalar_f64", [](E& e, size_t i) { return voxel_engine_get_scalar_f64(e.h, i); });
         c.def("set_scalar_f64", [](E& e, size_t i, double v) { voxel_engine_set_scalar_f64(e.h, i, v); });
+        // window functions (reference bindings/voxel_bindings.cpp:127-171): results written into `out`
+        using F64Arr = py::array_t<double, py::array::c_style | py::array::forcecast>;
+        using OutArr = py::array_t<double, py::array::c_style>;
+        auto win = [](int kind, F64Arr data, OutArr out, uint8_t w, double q) {
+            return voxel_window(0, kind, data.data(), static_cast<size_t>(data.size()), out.mutable_data(),
+                                static_cast<size_t>(out.size()), w, q);
+        };
+        c.def("window_delta", [win](E&, F64Arr d, OutArr o) { return win(0, d, o, 2, 0.0); }, py::arg("data"),
+              py::arg("out"));
+        c.def("window_sum", [win](E&, F64Arr d, OutArr o, uint8_t w) { return win(1, d, o, w, 0.0); },
+              py::arg("data"), py::arg("out"), py::arg("window"));
+        c.def("window_mean", [win](E&, F64Arr d, OutArr o, uint8_t w) { return win(2, d, o, w, 0.0); },
+              py::arg("data"), py::arg("out"), py::arg("window"));
+        c.def("window_stddev", [win](E&, F64Arr d, OutArr o, uint8_t w) { return win(3, d, o, w, 0.0); },
+              py::arg("data"), py::arg("out"), py::arg("window"));
+        c.def("window_variance", [win](E&, F64Arr d, OutArr o, uint8_t w) { return win(4, d, o, w, 0.0); },
+              py::arg("data"), py::arg("out"), py::arg("window"));
+        c.def("window_quantile",
+              [win](E&, F64Arr d, OutArr o, uint8_t w, double q) { return win(5, d, o, w, q); }, py::arg("data"),
+              py::arg("out"), py::arg("window"), py::arg("quantile"));
+        c.def("time_window_sum",
+              [](E&, py::array_t<int64_t, py::array::c_style | py::array::forcecast> ts, F64Arr v, int64_t start,
+                 int64_t dur, OutArr out) {
+                  const size_t cnt = std::min<size_t>(static_cast<size_t>(ts.size()), static_cast<size_t>(v.size()));
+                  return voxel_time_window_sum(0, ts.data(), v.data(), cnt, start, dur, out.mutable_data(),
+                                               static_cast<size_t>(out.size()));
+              },
+              py::arg("timestamps"), py::arg("values"), py::arg("start_time"), py::arg("duration_sec"),
+              py::arg("out"));
     }
     if (get_typed) {
         c.def(get_typed, [](E& e, size_t i) {
@@ -388,6 +423,41 @@ PYBIND11_MODULE(voxel_py, m) {
         if (st) fail("JIT compilation failed");
         return r;
     }, py::arg("code"), py::arg("data"), py::arg("threshold"), py::arg("total_count"));
+
+    // reference bindings/voxel_bindings.cpp:329-340: {"compiled": bool, "code_size", "code_ptr"}; the
+    // compiled form here is the lowered GPU kernel schedule (no host code pointer: 0), named in "kernel"
+    m.def("jit_compile", [](const std::vector<uint32_t>& code) {
+        size_t bytes = 0;
+        char kernel[32] = {0};
+        if (voxel_jit_compile(code.data(), code.size(), &bytes, kernel, sizeof(kernel)) != 0)
+            return py::dict(py::arg("compiled") = false);
+        return py::dict(py::arg("compiled") = true, py::arg("code_size") = bytes, py::arg("code_ptr") = 0,
+                        py::arg("kernel") = std::string(kernel));
+    }, py::arg("code"));
+
+    // reference bindings/voxel_bindings.cpp:97-103: a view of an f64 buffer
+    py::class_<SegmentF64>(m, "SegmentF64")
+        .def(py::init<>())
+        .def(py::init([](py::array_t<double, py::array::c_style | py::array::forcecast> a, size_t n) {
+                 SegmentF64 s;
+                 s.arr = a;
+                 s.n = std::min<size_t>(n, static_cast<size_t>(a.size()));
+                 return s;
+             }),
+             py::arg("data"), py::arg("count"))
+        .def(py::init([](py::array_t<double, py::array::c_style | py::array::forcecast> a) {
+                 SegmentF64 s;
+                 s.arr = a;
+                 s.n = static_cast<size_t>(a.size());
+                 return s;
+             }),
+             py::arg("data"))
+        .def("__getitem__", [](const SegmentF64& s, size_t i) {
+            if (i >= s.n) throw py::index_error("segment index out of range");
+            return s.arr.data()[i];
+        })
+        .def("__len__", [](const SegmentF64& s) { return s.n; })
+        .def_property_readonly("size", [](const SegmentF64& s) { return s.n; });
 
     m.attr("__version__") = "1.0.0";
 }
