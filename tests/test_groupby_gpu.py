@@ -77,9 +77,10 @@ def test_full_size_properties():
 
 def test_every_variant_gives_identical_bits():
     """The exact kernel variants (merged 192-bit atomics at 4/8/16 rows per
-    thread, 32-bit word table with and without the warp queue at 4/8) sum the
-    same integers, so every output bit agrees; the TMA-fed variant (compensated
-    f64 per warp) and all of them match the oracle."""
+    thread, 32-bit word table with and without the warp queue at 4/8, the
+    lean word table) sum the same integers, so every output bit agrees; the
+    TMA-fed variant (compensated f64 per warp) and all of them match the
+    oracle."""
     L = capi.lib()
     cases = [inputs.config2(1 << 20, 31), inputs.config2(333_333, 32, card=4096), inputs.config2(5000, 33, card=3),
              inputs.config2(1_000_003, 35, card=700)]
@@ -89,7 +90,7 @@ def test_every_variant_gives_identical_bits():
             for pthr, qlo, qhi in preds:
                 w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], pthr, qlo, qhi)
                 base = None
-                for v in (4, 8, 16, 1, 2, 3, 5, 6, 0):
+                for v in (4, 8, 16, 1, 2, 3, 5, 6, 7, 0):
                     assert L.voxel_scan_groupby_tune(v) == 0
                     got = gpu_scan_groupby(d, pthr, qlo, qhi)
                     k, s, mn, mx, c = got
@@ -145,5 +146,39 @@ def test_negative_and_mixed_sign_values_are_exact():
             k, s, mn, mx, c = gpu_scan_groupby(d, -np.inf, -1000, 1000)
             assert (k == w[0]).all() and (c == w[4]).all() and (mn == w[2]).all() and (mx == w[3]).all()
             np.testing.assert_allclose(s, exact, rtol=1e-14, atol=1e-300)
+    finally:
+        L.voxel_scan_groupby_tune(-1)
+
+
+def test_lean_word_table_extremes_and_negative_products():
+    """The lean variant screens MIN / MAX with the high 32 bits of the order
+    keys: prices that tie in those bits, negative prices and negative
+    products (qty < 0) still give the oracle's rows and the other variants'
+    bits.  (Zeros of both signs in one group are left out: the reference keeps
+    whichever comes first, these kernels order -0 below +0.)"""
+    L = capi.lib()
+    rng = np.random.default_rng(41)
+    d = inputs.config2(600_000, 42, card=64)
+    base = 37.0
+    ties = base + rng.integers(0, 1 << 20, d["n"]) * np.finfo(np.float64).eps * base  # same top 32 bits, mostly
+    price = np.where(rng.random(d["n"]) < 0.5, ties, -d["price"])
+    qty = d["qty"].copy()
+    qty[::3] = -qty[::3]
+    d = dict(d, price=np.ascontiguousarray(price), qty=np.ascontiguousarray(qty))
+    try:
+        for pthr, qlo, qhi in ((-1e9, -100, 100), (36.99, -50, 50), (-1e9, -1, -1)):
+            w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], pthr, qlo, qhi)
+            outs = []
+            for v in (1, 7):
+                assert L.voxel_scan_groupby_tune(v) == 0
+                got = gpu_scan_groupby(d, pthr, qlo, qhi)
+                k, s, mn, mx, c = got
+                assert (k == w[0]).all() and (c == w[4]).all()
+                assert (mn.view(np.uint64) == w[2].view(np.uint64)).all()
+                assert (mx.view(np.uint64) == w[3].view(np.uint64)).all()
+                np.testing.assert_allclose(s, w[1], rtol=1e-12, atol=1e-300)
+                outs.append(got)
+            for a, b in zip(*outs):
+                assert a.size == b.size and (a.view(np.uint8) == b.view(np.uint8)).all()
     finally:
         L.voxel_scan_groupby_tune(-1)

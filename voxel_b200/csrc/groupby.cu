@@ -959,6 +959,188 @@ __global__ void __launch_bounds__(kTwThreads, 1) scan_groupby_tw_kernel(
     finalize_groups<kTwThreads>(g, dict, card, done, out_keys, out_sum, out_min, out_max, out_count, out_ngroups);
 }
 
+// ---------------------------------------------------------------------------
+// Lean word table (variant 7): the queue-fed word table with less work per
+// passing row.
+//  - A queue entry is one 16-byte slot {u32 row, i32 qty, f64 price}: one
+//    shared store to push it, one load to consume it.
+//  - The ring holds 160 entries (31 left over + 4 x 32 pushed per tile), so a
+//    tile's pushes come first and its consumes after them, from one place.
+//  - MIN / MAX are screened with the high 32 bits of the group's order keys
+//    (one 8-byte shared load and two compares); only a row that can move
+//    them (a new extreme, or a tie in the high bits: rare) updates the 64-bit
+//    keys, straight in the global table, and then the screen.
+//  - SUM and COUNT are the word table's: the same integers, so every variant
+//    gives identical bits.
+// Rows are indexed with 32 bits: the host runs it for n < 2^32.
+// ---------------------------------------------------------------------------
+constexpr int kLeanQueue = 160;
+
+struct __align__(16) LeanEntry {
+    uint32_t row;
+    int32_t qty;
+    double price;
+};
+
+__host__ __device__ constexpr size_t lean_smem_bytes(uint32_t card) {
+    return static_cast<size_t>(card) * (kWords * 4 + 4 + 8) + 16;
+}
+
+template <int RPT>
+__global__ void __launch_bounds__(kGbThreads, 3) scan_groupby_lean_kernel(
+    const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
+    const double* __restrict__ price, const int32_t* __restrict__ qty, uint32_t n, double pthr, int32_t qlo,
+    int32_t qhi, GlobalGroups g, unsigned int* done, int32_t* out_keys, double* out_sum, double* out_min,
+    double* out_max, uint64_t* out_count, uint64_t* out_ngroups, int* status) {
+    constexpr uint32_t kTile = kGbThreads * RPT;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2* s_mm = reinterpret_cast<uint2*>(smem);                      // {hi32(min key), hi32(max key)}
+    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mm + card);          // 5 words per group
+    uint32_t* s_cnt = s_w + kWords * card;
+    __shared__ LeanEntry s_queue[kGbThreads / 32][kLeanQueue];
+
+    for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < kWords; ++k) s_w[kWords * i + k] = 0;
+        s_cnt[i] = 0;
+        s_mm[i] = make_uint2(0xFFFFFFFFu, 0u);
+    }
+    __syncthreads();
+    auto flush_table = [&]() {
+        for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
+            const unsigned int c = s_cnt[i];
+            if (!c) continue;
+            fix_atomic_add(&g.sum[3 * i], fix_from_words(s_w + kWords * i));
+            atomicAdd(&g.cnt[i], static_cast<unsigned long long>(c));
+#pragma unroll
+            for (int k = 0; k < kWords; ++k) s_w[kWords * i + k] = 0;
+            s_cnt[i] = 0;
+        }
+    };
+
+    const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    const uint32_t tiles_per_flush = (1u << 19) / kTile;  // the word table sums below 2^139 per 2^19 rows
+    bool bad_value = false, bad_key = false;
+    uint32_t since_flush = 0;
+    const int lane = threadIdx.x & 31;
+    const unsigned lanemask_lt = (1u << lane) - 1;
+    LeanEntry* Q = s_queue[threadIdx.x >> 5];
+    int qn = 0, qh = 0;  // warp-uniform: entries [qh, qh + qn) of the ring
+    const uint32_t qspan = qlo <= qhi ? static_cast<uint32_t>(qhi) - static_cast<uint32_t>(qlo) : 0u;
+    const double pcut = qlo <= qhi ? pthr : __longlong_as_double(0x7FF0000000000000ll);
+
+    auto consume = [&](int cnt) {
+        const bool valid = lane < cnt;
+        uint32_t gi = 0;
+        double p = 0.0, v = 0.0;
+        if (valid) {
+            int e = qh + lane;
+            if (e >= kLeanQueue) e -= kLeanQueue;
+            const LeanEntry en = Q[e];
+            p = en.price;
+            gi = key_bits(packed, en.row, width, mask);
+            v = __dmul_rn(p, static_cast<double>(en.qty));  // one rounded multiply, as the reference materialises it
+        }
+        const bool mayneg = __any_sync(0xffffffffu, valid && v < 0.0);
+        if (!valid) return;
+        if (gi >= card) {
+            bad_key = true;
+            return;
+        }
+        RowWords w;
+        if (!row_words(v, &w)) bad_value = true;
+        else if (mayneg) words_add<true>(s_w + kWords * gi, w, v < 0.0);
+        else words_add<false>(s_w + kWords * gi, w, false);
+        atomicAdd(&s_cnt[gi], 1u);
+        const uint64_t key = f64_order_key(p);
+        const uint32_t khi = static_cast<uint32_t>(key >> 32);
+        const uint2 mm = s_mm[gi];
+        if (khi <= mm.x) {
+            atomicMin(&g.mn[gi], static_cast<unsigned long long>(key));
+            atomicMin(&s_mm[gi].x, khi);
+        }
+        if (khi >= mm.y) {
+            atomicMax(&g.mx[gi], static_cast<unsigned long long>(key));
+            atomicMax(&s_mm[gi].y, khi);
+        }
+    };
+    auto drain = [&]() {
+        __syncwarp();
+        while (qn >= 32) {
+            consume(32);
+            __syncwarp();  // the consumed entries are free for the next pushes
+            qh += 32;
+            if (qh >= kLeanQueue) qh -= kLeanQueue;
+            qn -= 32;
+        }
+    };
+
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (since_flush == tiles_per_flush) {
+            __syncwarp();
+            consume(qn);
+            qn = 0;
+            __syncthreads();
+            flush_table();
+            __syncthreads();
+            since_flush = 0;
+        }
+        ++since_flush;
+        const uint32_t r0 = t * kTile + threadIdx.x * RPT;
+        double pv[RPT];
+        int32_t qv[RPT];
+        if (r0 + RPT <= n) {
+#pragma unroll
+            for (int k = 0; k < RPT; k += 4) {
+                const double2* pp = reinterpret_cast<const double2*>(price + r0 + k);
+                const double2 a = __ldcs(pp), b = __ldcs(pp + 1);
+                const int4 q = __ldcs(reinterpret_cast<const int4*>(qty + r0 + k));
+                pv[k] = a.x; pv[k + 1] = a.y; pv[k + 2] = b.x; pv[k + 3] = b.y;
+                qv[k] = q.x; qv[k + 1] = q.y; qv[k + 2] = q.z; qv[k + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                const bool in = r0 + k < n;
+                pv[k] = in ? price[r0 + k] : __longlong_as_double(0x7FF8000000000000ll);  // NaN never passes
+                qv[k] = in ? qty[r0 + k] : 0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const bool pass =
+                pv[k] > pcut && static_cast<uint32_t>(qv[k]) - static_cast<uint32_t>(qlo) <= qspan;
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) {
+                int pos = qh + qn + __popc(m & lanemask_lt);
+                if (pos >= kLeanQueue) pos -= kLeanQueue;
+                LeanEntry en;
+                en.row = r0 + k;
+                en.qty = qv[k];
+                en.price = pv[k];
+                Q[pos] = en;
+            }
+            qn += __popc(m);
+        }
+        drain();
+    }
+    __syncwarp();
+    consume(qn);
+    if (bad_value) atomicOr(status, 1);
+    if (bad_key) atomicOr(status, 2);
+    __syncthreads();
+    flush_table();
+    __threadfence();
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    finalize_groups<kGbThreads>(g, dict, card, done, out_keys, out_sum, out_min, out_max, out_count, out_ngroups);
+}
+
 __global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* done) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < card; i += gridDim.x * blockDim.x) {
         g.sum[3 * i] = 0;
@@ -1101,6 +1283,36 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
     return kOk;
 }
 
+template <int RPT>
+int launch_lean(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+                const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+                int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
+    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * RPT;
+    const size_t smem = lean_smem_bytes(card);
+    static thread_local bool attr_set = false;
+    if (!attr_set) {
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_lean_kernel<RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(lean_smem_bytes(kMaxGroups))));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_groupby_lean_kernel<RPT>, kGbThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int sms = sm_count() > 0 ? sm_count() : 148;
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (grid < 1) grid = 1;
+    GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
+    scan_groupby_lean_kernel<RPT><<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
+        packed, width, dict, card, price, qty, static_cast<uint32_t>(n), pthr, qlo, qhi, g, S.g_done, ok, os, omn,
+        omx, oc, ong, static_cast<int*>(S.status.p));
+    VX_CUDA(cudaGetLastError());
+    S.last_grid = static_cast<int>(grid);
+    S.last_kernel = 5;
+    return kOk;
+}
+
 }  // namespace
 
 size_t scan_groupby_smem_bytes(uint32_t card) { return static_cast<size_t>(card) * 5 * 8 + 16; }
@@ -1154,6 +1366,11 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
         if (const int tw = tw_stages(packed, width, card, n, tw_max_dyn()))
             return launch_tw(*this, tw, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys,
                              out_sum, out_min, out_max, out_count, out_ngroups, s);
+    const bool lean_ok = n < (1ull << 32);
+#define VX_LAUNCH_LEAN()                                                                                       \
+    launch_lean<4>(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum, out_min, \
+                   out_max, out_count, out_ngroups, s)
+    if (use_lean && lean_ok) return VX_LAUNCH_LEAN();
     if (autotune && !use_tma && n >= (1u << 16)) {  // smaller scans take the default
         // the word-table variants give identical bits: time them on this call's
         // data once per (dictionary size, rows) and keep the fastest
@@ -1162,15 +1379,16 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
             case 1: return VX_LAUNCH_RPT(8, 1);
             case 2: return VX_LAUNCH_RPT(4, 2);
             case 3: return VX_LAUNCH_RPT(8, 2);
+            case 4: return lean_ok ? VX_LAUNCH_LEAN() : VX_LAUNCH_RPT(4, 1);
             default: return VX_LAUNCH_RPT(4, 1);
             }
         };
         int cl = 0;
         while (cl < 31 && (2u << cl) <= card) ++cl;
-        const std::string family = "scan_groupby_card" + std::to_string(cl);
+        const std::string family = "scan_groupby_v2_card" + std::to_string(cl);
         const std::string key = tune_key(family.c_str(), F64, n);
         int c = 0;
-        if (!tune_lookup(key, &c)) c = tune_pick(key, 4, 0, s, variant);
+        if (!tune_lookup(key, &c)) c = tune_pick(key, 5, 0, s, variant);
         return variant(c);
     }
     if (mode == 1) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 1) : VX_LAUNCH_RPT(4, 1);
@@ -1181,6 +1399,7 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
     default: return VX_LAUNCH_RPT(4, 0);
     }
 #undef VX_LAUNCH_RPT
+#undef VX_LAUNCH_LEAN
 }
 
 // Status word bits the fused scan kernels OR in: 4 a bounded bulk-copy wait ran
@@ -1300,7 +1519,7 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
 int voxel_scan_groupby_tune(int variant) {
     clear_error();
     // validate before touching the state: a rejected id leaves the previous choice in place
-    const bool known = variant == -1 || (variant >= 0 && variant <= 6) || variant == 8 || variant == 16;
+    const bool known = variant == -1 || (variant >= 0 && variant <= 7) || variant == 8 || variant == 16;
     if (!known) {
         set_error(kErrInvalidArg, "unknown fused-scan variant %d", variant);
         return kErrInvalidArg;
@@ -1309,6 +1528,14 @@ int voxel_scan_groupby_tune(int variant) {
     S.autotune = variant == -1;  // -1: the autotuner's choice per shape (word table + queue, 4 rows, untuned)
     if (variant == -1) variant = 1;
     S.use_tw = false;
+    S.use_lean = false;
+    if (variant == 7) {  // lean word table (16-byte queue entries, screened MIN / MAX)
+        S.use_tma = false;
+        S.use_lean = true;
+        S.mode = 1;
+        S.rows_per_thread = 4;
+        return kOk;
+    }
     if (variant == 0) {
         S.use_tma = true;
         return kOk;
@@ -1341,6 +1568,7 @@ int voxel_scan_groupby_tune(int variant) {
 int voxel_scan_groupby_tune_state(void) {
     const ScanGroupBy& S = scan_groupby_state();
     if (S.autotune) return -1;
+    if (S.use_lean) return 7;
     if (S.use_tma) return 0;
     if (S.use_tw) return 6;
     if (S.mode == 1) return S.rows_per_thread == 8 ? 2 : 1;

@@ -22,11 +22,12 @@ struct ScanGroupBy {
     int rows_per_thread = 4;  // rows per thread of the shared-table variants: 4, 8 (16: merged only)
     bool use_tma = false;     // TMA-fed private-table variant when the dictionary fits
     bool use_tw = false;      // bulk-copy-fed word table (when the shape allows it)
+    bool use_lean = false;    // lean word table (16-byte queue entries, screened MIN / MAX), when n < 2^32
     int mode = 1;             // 0: merged 192-bit atomics, 1: 32-bit word table + warp queue, 2: word table direct
     bool autotune = true;     // pick among the bit-identical word-table variants per shape (unless one was forced)
     int last_grid = 0;
     int last_kernel = 0;      // 0: merged 192-bit atomics, 1: TMA-fed, 2: word table + queue, 3: word table direct,
-                              // 4: bulk-copy-fed word table
+                              // 4: bulk-copy-fed word table, 5: lean word table
 
     int prepare(uint32_t card, cudaStream_t s);
     int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
