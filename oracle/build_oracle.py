@@ -92,6 +92,36 @@ def build_reference(force: bool = False) -> str | None:
     return REF_SO
 
 
+REF_PY_DIR = os.path.join(REF_OUT, "refpy")
+
+
+def build_reference_py(force: bool = False) -> str | None:
+    """The reference's own pybind module (bindings/voxel_bindings.cpp) as
+    oracle/_ref/refpy/voxel_py*.so, for running the reference's Python front
+    end (bindings/voxel_query.py) to make golden vectors.  A separate
+    directory, so it never shadows this backend's voxel_py."""
+    import sysconfig
+
+    root = reference_root()
+    src = os.path.join(root, "bindings", "voxel_bindings.cpp")
+    if not os.path.isfile(src):
+        return None
+    try:
+        import pybind11
+    except ImportError:
+        return None
+    ext = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    out = os.path.join(REF_PY_DIR, "voxel_py" + ext)
+    if not force and _newer(out, src, __file__):
+        return out
+    os.makedirs(REF_PY_DIR, exist_ok=True)
+    cmd = ["g++", "-std=c++20", "-O2", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared", "-pthread",
+           "-w", "-I", os.path.join(root, "include"), "-I", root, "-I", pybind11.get_include(),
+           "-I", sysconfig.get_paths()["include"], src, "-o", out]
+    subprocess.check_call(cmd)
+    return out
+
+
 def build(force: bool = False) -> dict:
     out = {"oracle": build_restatement(force)}
     try:

@@ -32,7 +32,7 @@ def test_module_surface_and_encoders():
         assert a.raw == b
     x = I.jnz(-6)
     assert x.op() == 0x52 and x.imm12() == 0xFFA and I.vload(2, 1, 3, 7).imm12() == (3 << 8) | 7
-    assert V.EngineF64.k_lanes() == 4 and V.EngineU32.k_lanes() == 8
+    assert V.EngineF64.k_lanes == 4 and V.EngineU32.k_lanes == 8 and V.EngineF64().k_lanes == 4
 
 
 @pytest.mark.gpu

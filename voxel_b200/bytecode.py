@@ -41,6 +41,7 @@ def jnz(off) -> int: return enc(OP["JNZ"], 0, 0, 0, off & 0xFFF)
 def jz(off) -> int: return enc(OP["JZ"], 0, 0, 0, off & 0xFFF)
 def jl(off) -> int: return enc(OP["JL"], 0, 0, 0, off & 0xFFF)
 def jle(off) -> int: return enc(OP["JLE"], 0, 0, 0, off & 0xFFF)
+def jge(off) -> int: return enc(OP["JGE"], 0, 0, 0, off & 0xFFF)
 def jmp(off) -> int: return enc(OP["JMP"], 0, 0, 0, off & 0xFFF)
 def vload(vd, ra, seg, count=0) -> int: return enc(OP["VLOAD"], vd, ra, 0, ((seg & 0xF) << 8) | (count & 0xFF))
 def vsplat(vd, ra) -> int: return enc(OP["VSPLAT"], vd, ra)

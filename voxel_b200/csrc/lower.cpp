@@ -495,6 +495,29 @@ int lower_region(const std::vector<uint32_t>& code, size_t pc0, size_t loop_end,
         }
         case OP_CMP: {
             flags = FlagSrc{};
+            // `CMP acc, r; JLE 2; MOVR acc, r` (JGE: max) keeps the smaller (larger) of
+            // the accumulator and a reduction result in signed 64-bit order -- the
+            // MIN / MAX fold the Python query builder emits (bindings/voxel_query.py:
+            // 116-139; JLE / JGE jump on the signed flags of ra - rb)
+            if (pc + 2 < end) {
+                const uint32_t jr = code[pc + 1], mr = code[pc + 2];
+                const uint8_t jop = jr & 0xFF;
+                const bool self_ok = loop ? (R[ra].k == SVal::Carried) : known(ra);
+                if ((jop == OP_JLE || jop == OP_JGE) && f_simm(jr) == 2 && (mr & 0xFF) == OP_MOVR &&
+                    f_rd(mr) == ra && f_ra(mr) == rb && ra != rb && R[rb].k == SVal::Temp && self_ok) {
+                    const int k = R[rb].red;
+                    if (red_acc_reg[k] >= 0)
+                        return B.fail("reduction folded into two accumulators", pc), kErrUnsupportedProgram;
+                    red_acc_reg[k] = static_cast<int>(ra);
+                    out.params.red[k].acc = jop == OP_JLE ? kAccMin : kAccMax;
+                    out.params.acc0[k] = loop ? regs[ra] : R[ra].v;
+                    R[ra].k = SVal::Acc;
+                    R[ra].red = k;
+                    flags.k = FlagSrc::Data;
+                    pc += 2;
+                    break;
+                }
+            }
             if (known(ra) && known(rb)) {
                 flags.k = FlagSrc::Const;
                 flags.value = static_cast<int64_t>(R[ra].v - R[rb].v);

@@ -158,7 +158,9 @@ void bind_engine(py::module_& m, const char* name, const char* get_typed, bool f
                       py::arg("result_reg") = 0)
                  .def("get_scalar", &PyEngine::get_scalar)
                  .def("set_scalar", &PyEngine::set_scalar)
-                 .def_static("k_lanes", []() { return 32 / sizeof(T); });
+                 // a read-only class property, as Engine<T>::kLanes is bound in the reference
+                 // (voxel_bindings.cpp:126): EngineF64.k_lanes and engine.k_lanes are both 4
+                 .def_property_readonly_static("k_lanes", [](py::object) { return 32 / sizeof(T); });
     if (f64_scalars) {
         c.def("get_scalar_f64", [](E& e, size_t i) { return voxel_engine_get_scalar_f64(e.h, i); });
         c.def("set_scalar_f64", [](E& e, size_t i, double v) { voxel_engine_set_scalar_f64(e.h, i, v); });

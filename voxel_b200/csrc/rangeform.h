@@ -63,8 +63,11 @@ inline uint64_t host_to_bits(T v) {
     }
 }
 
+// count_col: also accept a COUNT of the column's lanes (VCOUNT of a VFILTER
+// output: passing nonzero values), which the single-program scan kernel
+// evaluates; the batched executor's kernels count constants only.
 template <typename T>
-inline bool range_form_t(const ScanParams& p, RangeForm* out) {
+inline bool range_form_t(const ScanParams& p, RangeForm* out, bool count_col = false) {
     if (p.ncols != 1 || p.nred != 1 || p.natoms < 1 || p.natoms > kMaxAtoms) return false;
     const uint32_t all = (1u << p.natoms) - 1u;
     const Red& r = p.red[0];
@@ -72,7 +75,8 @@ inline bool range_form_t(const ScanParams& p, RangeForm* out) {
     constexpr bool kFloat = std::is_floating_point<T>::value;
     if (r.acc != range_acc(r.kind, kFloat)) return false;
     // COUNT counts a constant (the VCOUNT of M & one); the others reduce the column
-    if (r.kind == kRedCount ? (r.a.kind != kOpConst && r.a.kind != kOpZero) : (r.a.kind != kOpCol || r.a.col != 0))
+    const bool acol = r.a.kind == kOpCol && r.a.col == 0;
+    if (r.kind == kRedCount ? !(r.a.kind == kOpConst || r.a.kind == kOpZero || (count_col && acol)) : !acol)
         return false;
     if (r.b.kind != kOpConst && r.b.kind != kOpZero) return false;
     const T lowest = kFloat ? -std::numeric_limits<T>::infinity() : std::numeric_limits<T>::lowest();
@@ -130,14 +134,14 @@ inline bool range_form_t(const ScanParams& p, RangeForm* out) {
 }
 
 
-inline bool range_form_of(const ScanParams& p, RangeForm* out) {
+inline bool range_form_of(const ScanParams& p, RangeForm* out, bool count_col = false) {
     switch (p.dtype) {
-    case F64: return range_form_t<double>(p, out);
-    case F32: return range_form_t<float>(p, out);
-    case I64: return range_form_t<int64_t>(p, out);
-    case I32: return range_form_t<int32_t>(p, out);
-    case U64: return range_form_t<uint64_t>(p, out);
-    default: return range_form_t<uint32_t>(p, out);
+    case F64: return range_form_t<double>(p, out, count_col);
+    case F32: return range_form_t<float>(p, out, count_col);
+    case I64: return range_form_t<int64_t>(p, out, count_col);
+    case I32: return range_form_t<int32_t>(p, out, count_col);
+    case U64: return range_form_t<uint64_t>(p, out, count_col);
+    default: return range_form_t<uint32_t>(p, out, count_col);
     }
 }
 

@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
 // same bits.
 template <int OP, typename T>
 __device__ __forceinline__ bool cmp_op(T v, T t) {
-    if constexpr (OP == 0) return v == t;
+    if constexpr (OP == 6) return true;  // no predicate: every lane keeps its value
+    else if constexpr (OP == 0) return v == t;
     else if constexpr (OP == 1) return v != t;
     else if constexpr (OP == 2) return v < t;
     else if constexpr (OP == 3) return v <= t;
@@ -206,8 +207,8 @@ __global__ void __launch_bounds__(kThreads, 6) fsum_kernel(const __grid_constant
     }
 }
 
-bool fsum_sum_red(const Red& r) {
-    if (r.kind != kRedSum || r.pmask != 1u || r.a.kind != kOpCol || r.a.col != 0) return false;
+bool fsum_sum_red(const Red& r, uint32_t pmask) {
+    if (r.kind != kRedSum || r.pmask != pmask || r.a.kind != kOpCol || r.a.col != 0) return false;
     if (!(r.b.kind == kOpZero || (r.b.kind == kOpConst && r.b.bits == 0))) return false;
     return r.acc == kAccAdd || r.acc == kAccSub || r.acc == kAccAddF || r.acc == kAccTAdd;
 }
@@ -215,13 +216,14 @@ bool fsum_sum_red(const Red& r) {
 // one column, one compare atom, a masked SUM of the column (failing lanes are
 // zero), and optionally the COUNT of the same VFILTER output
 bool fsum_shape(const ScanParams& p) {
-    if (p.ncols != 1 || p.natoms != 1 || p.nred < 1 || p.nred > 2) return false;
-    const Atom& a = p.atom[0];
-    if (a.col != 0 || a.op > 5) return false;
-    if (!fsum_sum_red(p.red[0])) return false;
+    // one compare atom, or none (every lane kept: SUM / COUNT of the column)
+    if (p.ncols != 1 || p.natoms > 1 || p.nred < 1 || p.nred > 2) return false;
+    if (p.natoms == 1 && (p.atom[0].col != 0 || p.atom[0].op > 5)) return false;
+    const uint32_t pm = p.natoms ? 1u : 0u;
+    if (!fsum_sum_red(p.red[0], pm)) return false;
     if (p.nred == 1) return true;
     const Red& c = p.red[1];
-    if (c.kind != kRedCount || c.pmask != 1u || c.acc != kAccAdd || c.a.kind != kOpCol || c.a.col != 0) return false;
+    if (c.kind != kRedCount || c.pmask != pm || c.acc != kAccAdd || c.a.kind != kOpCol || c.a.col != 0) return false;
     return c.b.kind == kOpZero || (c.b.kind == kOpConst && c.b.bits == 0);
 }
 
@@ -241,6 +243,7 @@ bool pass_implies_nonzero(int op, uint64_t thr_bits) {
 }
 
 bool pass_implies_nonzero_of(const ScanParams& p) {
+    if (p.natoms == 0) return false;
     switch (p.dtype) {
     case F64: return pass_implies_nonzero<double>(p.atom[0].op, p.atom[0].thr);
     case F32: return pass_implies_nonzero<float>(p.atom[0].op, p.atom[0].thr);
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(kThreads, 6) range_scan_kernel(const __grid_co
     // NaN), the others when bc is
     const uint32_t cnt_pass = (!t_isnan<T>(ac) && ac != T(0)) ? 1u : 0u;
     const uint32_t cnt_fail = (!t_isnan<T>(bc) && bc != T(0)) ? 1u : 0u;
+    const bool cnt_col = RK == kRedCount && p.red[0].a.kind == kOpCol;  // VCOUNT of the column's passing lanes
     Acc acc[1];
     acc[0].u = acc_identity(accop);
     acc[0].k = {0.0, 0.0};
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 6) range_scan_kernel(const __grid_co
         for (int u = 0; u < kFsUnroll; ++u) {
             const uint64_t j = j0 + u * stride;
             if (j >= p.ndata) continue;
-            uint32_t pm = 0;
+            uint32_t pm = 0, nz = 0;
             T x[KL];
 #pragma unroll
             for (int l = 0; l < KL; ++l) {
@@ -303,12 +307,13 @@ __global__ void __launch_bounds__(kThreads, 6) range_scan_kernel(const __grid_co
                 bool pass = y >= lo && y <= hi;
                 if constexpr (NE) pass = pass && y != n0 && y != n1;
                 pm |= pass ? 1u << l : 0u;
+                if constexpr (RK == kRedCount) nz |= (pass && y != T(0)) ? 1u << l : 0u;  // NaN never passes
                 if constexpr (RK != kRedCount) x[l] = pass ? y : bc;
             }
             uint64_t r;
             if constexpr (RK == kRedCount) {
                 const uint32_t np = __popc(pm);
-                r = cnt_pass * np + cnt_fail * (KL - np);
+                r = (cnt_col ? __popc(nz) : cnt_pass * np) + cnt_fail * (KL - np);
             } else {
                 r = reduce_group<T>(RK, x);
             }
@@ -574,13 +579,14 @@ int launch_fsum(const ScanParams& p, ScanResult* d_out, void* scratch, cudaStrea
 #define VX_FS(OP)                                                                                        \
     (p.nred == 2 ? fsum_kernel<T, OP, 1><<<grid, kThreads, 0, s>>>(p, vec, cnt_all, part, done, d_out)  \
                  : fsum_kernel<T, OP, 0><<<grid, kThreads, 0, s>>>(p, vec, cnt_all, part, done, d_out))
-    switch (p.atom[0].op) {
+    switch (p.natoms ? p.atom[0].op : 6) {
     case 0: VX_FS(0); break;
     case 1: VX_FS(1); break;
     case 2: VX_FS(2); break;
     case 3: VX_FS(3); break;
     case 4: VX_FS(4); break;
-    default: VX_FS(5); break;
+    case 5: VX_FS(5); break;
+    default: VX_FS(6); break;
     }
 #undef VX_FS
     VX_CUDA(cudaGetLastError());
@@ -605,7 +611,7 @@ template <typename T>
 int dispatch(const ScanParams& p, int grid, ScanResult* d_out, void* scratch, cudaStream_t s) {
     if (fsum_shape(p)) return launch_fsum<T>(p, d_out, scratch, s);
     RangeForm rf;
-    if (range_form_of(p, &rf)) return launch_range<T>(p, rf, d_out, scratch, s);
+    if (range_form_of(p, &rf, true)) return launch_range<T>(p, rf, d_out, scratch, s);
     if (multi_range_form_of(p, &rf)) return launch_mrange<T>(p, rf, d_out, scratch, s);
     if (p.ncols <= 1 && p.nred <= 2) return launch_t<T, 1, 2, 4>(p, grid, d_out, scratch, s);
     if (p.ncols <= 1) return launch_t<T, 1, kMaxRed, 2>(p, grid, d_out, scratch, s);
@@ -691,7 +697,7 @@ __global__ void __launch_bounds__(kThreads) seg_agg_kernel(const T* col, uint64_
 const char* scan_kernel_name(const ScanParams& p) {
     RangeForm rf;
     if (fsum_shape(p)) return "fsum";
-    if (range_form_of(p, &rf)) return "range";
+    if (range_form_of(p, &rf, true)) return "range";
     if (multi_range_form_of(p, &rf)) return "mrange";
     return "generic";
 }
