@@ -67,14 +67,14 @@ def test_join_family_against_live_reference():
             cap = lk.size * (dup * 2 if not unique else 1) + 16
             wl = np.zeros(cap, np.uint32)
             wr = np.zeros(cap, np.uint32)
-            m = R[f"vref_merge_join_{NAME[dt]}"](lk.ctypes.data, lk.size, rk.ctypes.data, rk.size, wl.ctypes.data,
+            m = getattr(R, f"vref_merge_join_{NAME[dt]}")(lk.ctypes.data, lk.size, rk.ctypes.data, rk.size, wl.ctypes.data,
                                                  wr.ctypes.data, unique)
             lo, ro = merge(dt, lk, rk, cap, unique)
             assert lo.size == m and (lo == wl[:m]).all() and (ro == wr[:m]).all(), (dt, unique)
         ls = inputs.shuffled(lk, 7)
         for anti in (0, 1):
             w = np.zeros(ls.size, np.uint32)
-            m = R[f"vref_semi_join_{NAME[dt]}"](ls.ctypes.data, ls.size, rk.ctypes.data, rk.size, w.ctypes.data, anti)
+            m = getattr(R, f"vref_semi_join_{NAME[dt]}")(ls.ctypes.data, ls.size, rk.ctypes.data, rk.size, w.ctypes.data, anti)
             o = semi(dt, ls, rk, anti)
             assert o.size == m and (o == w[:m]).all(), (dt, anti)
 

@@ -63,7 +63,7 @@ def test_windows_against_live_reference_large():
         x = inputs.window_values(dt, n, 300 + dt)
         for kind, w, q in ((1, 16, 0), (2, 5, 0), (3, 32, 0), (4, 7, 0), (5, 21, 0.37), (0, 2, 0)):
             want = np.zeros(n, x.dtype)
-            m = R[f"vref_window_{NAME[dt]}"](kind, x.ctypes.data, n, want.ctypes.data, n, w, q)
+            m = getattr(R, f"vref_window_{NAME[dt]}")(kind, x.ctypes.data, n, want.ctypes.data, n, w, q)
             got = np.zeros(n, x.dtype)
             g = L.voxel_window(dt, kind, x.ctypes.data, n, got.ctypes.data, n, w, q)
             assert g == m and (got[:m].view(np.uint8) == want[:m].view(np.uint8)).all(), (dt, kind)
