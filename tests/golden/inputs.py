@@ -125,7 +125,11 @@ def config2(n: int, seed: int, card: int = 1000) -> dict:
     from voxel_b200 import encode
 
     rng = np.random.default_rng(seed)
-    values = np.sort(rng.choice(np.arange(-50000, 50000, dtype=np.int64), size=card, replace=False)).astype(np.int32)
+    if card <= 100_000:
+        values = np.sort(rng.choice(np.arange(-50000, 50000, dtype=np.int64), size=card, replace=False)).astype(np.int32)
+    else:  # large dictionaries: distinct i32 values over the whole range
+        values = np.unique(rng.integers(-(2**31), 2**31 - 1, size=card + card // 4 + 16, dtype=np.int64))
+        values = np.sort(rng.permutation(values)[:card]).astype(np.int32)
     rank = zipf_alias_keys(n, card, 1.1, rng)
     perm = rng.permutation(card)
     code = perm[rank]                      # position of each row's key in the sorted value list

@@ -212,7 +212,7 @@ def test_scan_groupby_status_words(lib):
     the bulk-copy timeout bit wins over the others and is reported as a
     timeout, not an overflow."""
     cases = [(0, 0, None), (1, 7, "not finite"), (2, 1, "dictionary"), (3, 1, "dictionary"),
-             (4, 6, "bulk-copy wait"), (5, 6, "bulk-copy wait"), (6, 6, "bulk-copy wait"), (8, 1, "unknown")]
+             (4, 6, "bounded wait"), (5, 6, "bounded wait"), (6, 6, "bounded wait"), (8, 1, "unknown")]
     for word, code, text in cases:
         assert lib.voxel_scan_groupby_status_code(word) == code, word
         if text:

@@ -182,3 +182,26 @@ def test_lean_word_table_extremes_and_negative_products():
                 assert a.size == b.size and (a.view(np.uint8) == b.view(np.uint8)).all()
     finally:
         L.voxel_scan_groupby_tune(-1)
+
+
+def test_large_dictionaries_against_reference():
+    """Dictionaries beyond the 4,096-entry shared-memory tables (here up to
+    about a million distinct keys present) take the global-table path and
+    give the reference HashAggregator's rows: keys, counts, min / max exact,
+    sums within 1e-12."""
+    if not oracle.have_ref():
+        pytest.skip("reference library not built")
+    L = capi.lib()
+    for n, card, seed in ((1 << 22, 1 << 20, 51), (1 << 21, 5000, 52), (1 << 23, 1 << 22, 53)):
+        d = inputs.config2(n, seed, card=card)
+        assert d["dict"].size > 4096
+        k, s, mn, mx, c = gpu_scan_groupby(d)
+        assert L.voxel_scan_groupby_last_variant() == 6
+        wk, ws, wmn, wmx, wc, _ = oracle.scan_groupby_ref(d["packed"], d["width"], d["dict"], d["price"], d["qty"],
+                                                          20.0, 10, 50, threads=1)
+        assert k.size == wk.size and (k == wk).all() and (c == wc).all()
+        assert (mn.view(np.uint64) == wmn.view(np.uint64)).all() and (mx.view(np.uint64) == wmx.view(np.uint64)).all()
+        np.testing.assert_allclose(s, ws, rtol=1e-12, atol=0)
+        # a second call on the same state: the finalize left the table at rest
+        k2, s2, _, _, c2 = gpu_scan_groupby(d)
+        assert (k2 == k).all() and (c2 == c).all() and (s2.view(np.uint64) == s.view(np.uint64)).all()

@@ -30,6 +30,7 @@
 #include "voxel_c.h"
 #include "vx_common.cuh"
 #include "vx_runtime.h"
+#include "vx_scan.cuh"
 
 namespace vx {
 
@@ -1141,6 +1142,144 @@ __global__ void __launch_bounds__(kGbThreads, 3) scan_groupby_lean_kernel(
     finalize_groups<kGbThreads>(g, dict, card, done, out_keys, out_sum, out_min, out_max, out_count, out_ngroups);
 }
 
+// ---------------------------------------------------------------------------
+// Large dictionaries (more than kMaxGroups entries: the shared-memory tables
+// do not fit).  Passing rows are added straight into the global table in HBM:
+// the exact 192-bit sum with 64-bit atomics (carries from the returned old
+// values), the count, and MIN / MAX keys only when a plain read of the
+// current key shows the row can improve it.  A separate single-pass kernel
+// then compacts the non-empty groups in key order (tiles of groups claimed in
+// launch order, output offsets by decoupled look-back) and resets the table.
+// The sums are the same integers as the shared-table kernels', so the rows
+// are bit-identical to theirs.
+// ---------------------------------------------------------------------------
+template <int RPT>
+__global__ void __launch_bounds__(kGbThreads) scan_groupby_global_kernel(
+    const uint64_t* __restrict__ packed, uint32_t width, uint32_t card, const double* __restrict__ price,
+    const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi, GlobalGroups g, int* status) {
+    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * RPT;
+    const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
+    const uint32_t qspan = qlo <= qhi ? static_cast<uint32_t>(qhi) - static_cast<uint32_t>(qlo) : 0u;
+    const double pcut = qlo <= qhi ? pthr : __longlong_as_double(0x7FF0000000000000ll);
+    bool bad_value = false, bad_key = false;
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint64_t r0 = t * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
+        double pv[RPT];
+        int32_t qv[RPT];
+        if (r0 + RPT <= n) {
+#pragma unroll
+            for (int k = 0; k < RPT; k += 4) {
+                const double2* pp = reinterpret_cast<const double2*>(price + r0 + k);
+                const double2 a = __ldcs(pp), b = __ldcs(pp + 1);
+                const int4 q = __ldcs(reinterpret_cast<const int4*>(qty + r0 + k));
+                pv[k] = a.x; pv[k + 1] = a.y; pv[k + 2] = b.x; pv[k + 3] = b.y;
+                qv[k] = q.x; qv[k + 1] = q.y; qv[k + 2] = q.z; qv[k + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                const bool in = r0 + k < n;
+                pv[k] = in ? price[r0 + k] : __longlong_as_double(0x7FF8000000000000ll);  // NaN never passes
+                qv[k] = in ? qty[r0 + k] : 0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const double p = pv[k];
+            if (!(p > pcut && static_cast<uint32_t>(qv[k]) - static_cast<uint32_t>(qlo) <= qspan)) continue;
+            const uint32_t gi = key_bits(packed, r0 + k, width, mask);
+            if (gi >= card) {
+                bad_key = true;
+                continue;
+            }
+            const double v = __dmul_rn(p, static_cast<double>(qv[k]));  // one rounded multiply
+            const Fix3 f = fix_from_double_s<kFixScale>(v, &bad_value);
+            fix_atomic_add(&g.sum[3 * static_cast<uint64_t>(gi)], f);
+            atomicAdd(&g.cnt[gi], 1ull);
+            const uint64_t key = f64_order_key(p);
+            if (key < __ldcg(&g.mn[gi])) atomicMin(&g.mn[gi], static_cast<unsigned long long>(key));
+            if (key > __ldcg(&g.mx[gi])) atomicMax(&g.mx[gi], static_cast<unsigned long long>(key));
+        }
+    }
+    if (bad_value) atomicOr(status, 1);
+    if (bad_key) atomicOr(status, 2);
+}
+
+constexpr int kFinPer = 8;                        // groups per thread
+constexpr int kFinTile = kGbThreads * kFinPer;     // groups per tile
+
+__global__ void __launch_bounds__(kGbThreads) groupby_finalize_kernel(
+    GlobalGroups g, const int32_t* __restrict__ dict, uint32_t card, int32_t* out_keys, double* out_sum,
+    double* out_min, double* out_max, uint64_t* out_count, uint64_t* out_ngroups, unsigned long long* lb,
+    unsigned int* ctr, int* err) {
+    __shared__ uint64_t s_tile, s_base;
+    __shared__ uint64_t s_warp[kGbThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t ntiles = (card + kFinTile - 1) / kFinTile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+        __syncthreads();
+        const uint64_t tile = s_tile;
+        if (tile >= ntiles) break;
+        const uint64_t i0 = tile * kFinTile + static_cast<uint64_t>(threadIdx.x) * kFinPer;
+        uint32_t live = 0;
+#pragma unroll
+        for (int k = 0; k < kFinPer; ++k) {
+            const uint64_t i = i0 + k;
+            if (i < card && __ldcg(&g.cnt[i])) live |= 1u << k;
+        }
+        const uint64_t c = __popc(live);
+        uint64_t inc = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += y;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const uint64_t x = lane < kGbThreads / 32 ? s_warp[lane] : 0;
+            uint64_t t = x;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint64_t y = __shfl_up_sync(0xffffffffu, t, d);
+                if (lane >= d) t += y;
+            }
+            if (lane < kGbThreads / 32) s_warp[lane] = t - x;
+            const uint64_t total = __shfl_sync(0xffffffffu, t, kGbThreads / 32 - 1);
+            const uint64_t e = lookback_exclusive_warp(lb, tile, total, err);
+            if (lane == 0) {
+                s_base = e;
+                if (tile == ntiles - 1) *out_ngroups = e + total;
+            }
+        }
+        __syncthreads();
+        uint64_t pos = s_base + s_warp[warp] + (inc - c);
+#pragma unroll
+        for (int k = 0; k < kFinPer; ++k) {
+            const uint64_t i = i0 + k;
+            if (i >= card) break;
+            if (live >> k & 1u) {
+                const Fix3 f{__ldcg(&g.sum[3 * i]), __ldcg(&g.sum[3 * i + 1]), __ldcg(&g.sum[3 * i + 2])};
+                out_keys[pos] = dict[i];
+                out_sum[pos] = fix_to_double_s<kFixScale>(f);
+                out_min[pos] = f64_from_order_key(__ldcg(&g.mn[i]));
+                out_max[pos] = f64_from_order_key(__ldcg(&g.mx[i]));
+                out_count[pos] = __ldcg(&g.cnt[i]);
+                ++pos;
+            }
+            g.sum[3 * i] = 0;
+            g.sum[3 * i + 1] = 0;
+            g.sum[3 * i + 2] = 0;
+            g.cnt[i] = 0;
+            g.mn[i] = ~0ull;
+            g.mx[i] = 0;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* done) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < card; i += gridDim.x * blockDim.x) {
         g.sum[3 * i] = 0;
@@ -1313,13 +1452,47 @@ int launch_lean(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const in
     return kOk;
 }
 
+int launch_global(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+                  const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+                  int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
+    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * 4;
+    const int sms = sm_count() > 0 ? sm_count() : 148;
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    uint64_t grid = static_cast<uint64_t>(sms) * 4;
+    if (grid > ntiles) grid = ntiles;
+    if (grid < 1) grid = 1;
+    GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
+    if (n)
+        scan_groupby_global_kernel<4><<<static_cast<unsigned>(grid), kGbThreads, 0, s>>>(
+            packed, width, card, price, qty, n, pthr, qlo, qhi, g, static_cast<int*>(S.status.p));
+    VX_CUDA(cudaGetLastError());
+    const uint64_t ftiles = (card + kFinTile - 1) / kFinTile;
+    const size_t lb_bytes = (ftiles + 1) * 8 + 64;
+    if (S.lookback.n < lb_bytes) {
+        S.lookback = DevBuf(lb_bytes);
+        if (!S.lookback.p) return kErrOutOfMemory;
+    }
+    VX_CUDA(cudaMemsetAsync(S.lookback.p, 0, lb_bytes, s));
+    unsigned long long* lb = S.lookback.as<unsigned long long>();
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(lb + ftiles);
+    uint64_t fgrid = static_cast<uint64_t>(sms) * 4;
+    if (fgrid > ftiles) fgrid = ftiles;
+    // the status word's bit 4 is the look-back timeout, reported like the bulk-copy waits
+    groupby_finalize_kernel<<<static_cast<unsigned>(fgrid), kGbThreads, 0, s>>>(
+        g, dict, card, ok, os, omn, omx, oc, ong, lb, ctr, static_cast<int*>(S.status.p));
+    VX_CUDA(cudaGetLastError());
+    S.last_grid = static_cast<int>(grid);
+    S.last_kernel = 6;
+    return kOk;
+}
+
 }  // namespace
 
 size_t scan_groupby_smem_bytes(uint32_t card) { return static_cast<size_t>(card) * 5 * 8 + 16; }
 
 int ScanGroupBy::prepare(uint32_t card, cudaStream_t s) {
-    if (card == 0 || card > kMaxGroups) {
-        set_error(kErrInvalidArg, "dictionary cardinality %u outside 1..%u", card, kMaxGroups);
+    if (card == 0 || card > kMaxGlobalGroups) {
+        set_error(kErrInvalidArg, "dictionary cardinality %u outside 1..%u", card, kMaxGlobalGroups);
         return kErrInvalidArg;
     }
     if (card_ != card) {
@@ -1355,6 +1528,9 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
     }
     int st = prepare(card, s);
     if (st) return st;
+    if (card > kMaxGroups)  // the shared-memory tables do not fit: HBM atomics, multi-block finalize
+        return launch_global(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
+                             out_min, out_max, out_count, out_ngroups, s);
     if (use_tma && card <= kTmaMaxCard && tma_smem_bytes(card, width) <= kSmemOptIn && n >= kTmaRows &&
         ((reinterpret_cast<uintptr_t>(packed) & 15) == 0))
         return launch_tma(*this, packed, width, dict, card, price, qty, n, pthr, qlo, qhi, out_keys, out_sum,
@@ -1408,7 +1584,9 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
 int groupby_status_error(int h) {
     if (!h) return kOk;
     if (h & 4) {
-        set_error(kErrDeviceTimeout, "a bulk-copy wait in the fused scan ran out of its budget; the group rows are partial");
+        set_error(kErrDeviceTimeout,
+                  "a bounded wait in the fused scan (bulk copy or tile look-back) ran out of its budget; the group rows "
+                  "are partial");
         return kErrDeviceTimeout;
     }
     if (h & 2) {

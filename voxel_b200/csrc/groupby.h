@@ -11,11 +11,13 @@ namespace vx {
 
 // Largest dictionary the shared-memory group table holds.
 constexpr uint32_t kMaxGroups = 4096;
+// Largest dictionary of the fused scan (above kMaxGroups: the global-table path).
+constexpr uint32_t kMaxGlobalGroups = 1u << 26;
 
 size_t scan_groupby_smem_bytes(uint32_t card);
 
 struct ScanGroupBy {
-    DevBuf table, status;
+    DevBuf table, status, lookback;
     uint32_t card_ = 0;
     unsigned long long *g_sum = nullptr, *g_cnt = nullptr, *g_mn = nullptr, *g_mx = nullptr;
     unsigned int* g_done = nullptr;
@@ -27,7 +29,8 @@ struct ScanGroupBy {
     bool autotune = true;     // pick among the bit-identical word-table variants per shape (unless one was forced)
     int last_grid = 0;
     int last_kernel = 0;      // 0: merged 192-bit atomics, 1: TMA-fed, 2: word table + queue, 3: word table direct,
-                              // 4: bulk-copy-fed word table, 5: lean word table
+                              // 4: bulk-copy-fed word table, 5: lean word table,
+                              // 6: global table (dictionaries above kMaxGroups)
 
     int prepare(uint32_t card, cudaStream_t s);
     int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
