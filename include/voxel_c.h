@@ -306,7 +306,10 @@ int       voxel_dict_decode_dev(int dtype, const void* d_dict, size_t card, cons
 /* ================================================================
  * Additive: fused scan + group-by (decode key, two predicates, group SUM of a
  * product, COUNT, MIN, MAX).  Groups come out sorted by key; returns the
- * group count or (size_t)-1.
+ * group count or (size_t)-1.  Dictionaries of up to 4,096 entries aggregate
+ * in shared-memory tables; larger ones (up to 2^26 entries) add straight into
+ * the HBM table with atomics and compact the groups with a second kernel
+ * (the same exact integers: identical results).
  *   key = dict[unpack(packed_key)], WHERE price > price_gt AND
  *   qty BETWEEN qty_lo AND qty_hi, GROUP BY key:
  *   SUM(price*qty) (one rounded multiply), COUNT(*), MIN(price), MAX(price)
@@ -341,8 +344,9 @@ int       voxel_scan_groupby_last_variant(void);
 int       voxel_scan_groupby_tune_state(void);
 /* Errors of the device-pointer fused scan.  The kernels OR bits into a device
  * status word: 1 = a price*qty product not finite or beyond 2^63, 2 = a packed
- * key index outside the dictionary, 4 = a bounded bulk-copy wait ran out
- * (variants 0 and 6 only; the group rows are then partial).
+ * key index outside the dictionary, 4 = a bounded wait ran out (the bulk
+ * copies of variants 0 and 6, the tile look-back of the large-dictionary
+ * path; the group rows are then partial).
  * voxel_scan_groupby_check synchronises `stream`, reads and clears the calling
  * thread's status word of voxel_scan_groupby_dev and returns VOXEL_OK, or
  * VOXEL_ETIMEOUT (bit 4), VOXEL_EINVAL (bit 2), VOXEL_EOVERFLOW (bit 1), with
@@ -411,6 +415,14 @@ size_t    voxel_groupby_i32_f64(const int32_t* keys, const double* values, size_
 size_t    voxel_groupby_u32_f64(const uint32_t* keys, const double* values, size_t n,
                                 size_t expected_groups, uint32_t* out_keys, double* out_sum,
                                 double* out_min, double* out_max, uint64_t* out_count);
+/* GROUP BY over device columns with a chosen plan: method 0 = HashAggregator
+ * sized for expected_groups (grown if too small), 1 = sort-based
+ * (GroupedAggregator over radix-sorted keys).  Outputs are bit-identical
+ * either way (groups in key order); *ngroups (host) = the group count. */
+int       voxel_groupby_u32_f64_dev(const uint32_t* d_keys, const double* d_values, size_t n,
+                                    size_t expected_groups, int method, uint32_t* d_keys_out, double* d_sum,
+                                    double* d_min, double* d_max, uint64_t* d_count, uint64_t* ngroups,
+                                    void* stream);
 /* the voxel_agg_* object: device-pointer accumulate, and its groups sorted by key */
 int       voxel_agg_accumulate_dev(void* agg, const uint32_t* d_keys, const double* d_values, size_t count,
                                    void* stream);
@@ -451,6 +463,11 @@ size_t    voxel_merge_join(int dtype, const void* left, size_t nl, const void* r
 int       voxel_merge_join_dev(int dtype, const void* d_left, size_t nl, const void* d_right, size_t nr,
                                uint32_t* d_left_out, uint32_t* d_right_out, size_t max_matches, int unique,
                                uint64_t* d_count2, void* stream);
+/* the pairs of a join built on the left side (d_probe = right rows, d_build =
+ * left rows) in the order of the join built on the right: left rows
+ * ascending, each one's right rows descending (ProbeAllMatches order) */
+int       voxel_join_pairs_swap_order_dev(const uint32_t* d_probe, const uint32_t* d_build, size_t m,
+                                          uint32_t* d_left, uint32_t* d_right, void* stream);
 size_t    voxel_semi_join(int dtype, const void* left, size_t nl, const void* right, size_t nr, uint32_t* out,
                           int anti);
 int       voxel_semi_join_dev(int dtype, const void* d_left, size_t nl, const void* d_right, size_t nr,

@@ -133,6 +133,8 @@ _SIGS = {
     "voxel_time_window_sum": (sz, [C.c_int, vp, vp, sz, i64, i64, vp, sz]),
     "voxel_time_window_sum_dev": (C.c_int, [C.c_int, vp, vp, sz, i64, i64, vp, sz, C.POINTER(sz), vp]),
     "voxel_merge_join": (sz, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int]),
+    "voxel_join_pairs_swap_order_dev": (C.c_int, [vp, vp, sz, vp, vp, vp]),
+    "voxel_groupby_u32_f64_dev": (C.c_int, [vp, vp, sz, sz, C.c_int, vp, vp, vp, vp, vp, C.POINTER(u64), vp]),
     "voxel_merge_join_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
     "voxel_semi_join": (sz, [C.c_int, vp, sz, vp, sz, vp, C.c_int]),
     "voxel_semi_join_dev": (C.c_int, [C.c_int, vp, sz, vp, sz, vp, C.c_int, vp, vp]),

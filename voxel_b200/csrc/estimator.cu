@@ -173,8 +173,7 @@ __global__ void unique_runs_kernel(const T* __restrict__ col, const uint64_t* __
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         if (i > 0 && skey[i] == skey[i - 1]) continue;
-        uint64_t e = i + 1;
-        while (e < n && skey[e] == skey[i]) ++e;
+        const uint64_t e = sorted_run_end(skey, i, n);
         unsigned long long slot = atomicAdd(nu, 1ull);
         uval[slot] = col[sidx[i]];
         ucnt[slot] = static_cast<unsigned int>(e - i);

@@ -42,8 +42,7 @@ __global__ void insert_runs_kernel(const int64_t* __restrict__ skeys, const uint
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         if (!head[i]) continue;
         int64_t k = skeys[i];
-        uint64_t e = i + 1;
-        while (e < n && !head[e]) ++e;  // run length (runs are short; long runs are rare duplicates)
+        const uint64_t e = sorted_run_end(skeys, i, n);
         uint32_t len = static_cast<uint32_t>(e - i);
         uint64_t h = mix64(static_cast<uint64_t>(k)) & mask;
         uint64_t probes = 0;

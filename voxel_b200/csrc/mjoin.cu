@@ -181,6 +181,27 @@ __global__ void widen_kernel(const T* __restrict__ in, uint64_t n, int64_t* __re
         out[i] = static_cast<int64_t>(in[i]);
 }
 
+// (l << 32) | (2^32 - 1 - r): ascending order = left row ascending, then right
+// row descending (the order HashJoin::ProbeAllMatches emits with the right
+// side built: probe rows in order, each key's build rows newest first)
+__global__ void pair_key_kernel(const uint32_t* __restrict__ l, const uint32_t* __restrict__ r, uint64_t m,
+                                uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        key[i] = (static_cast<uint64_t>(l[i]) << 32) | (0xFFFFFFFFull - r[i]);
+        idx[i] = static_cast<uint32_t>(i);
+    }
+}
+
+__global__ void pair_split_kernel(const uint64_t* __restrict__ key, uint64_t m, uint32_t* __restrict__ l,
+                                  uint32_t* __restrict__ r) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        l[i] = static_cast<uint32_t>(key[i] >> 32);
+        r[i] = static_cast<uint32_t>(0xFFFFFFFFull - (key[i] & 0xFFFFFFFFull));
+    }
+}
+
 __global__ void total_kernel(const unsigned long long* status, uint64_t ntiles, uint64_t cap,
                              unsigned long long* out2) {
     const uint64_t total = ntiles ? (status[ntiles - 1] & kLbValMask) : 0;
@@ -335,6 +356,33 @@ int voxel_semi_join_dev(int dtype, const void* d_left, size_t nl, const void* d_
     }
     if (int st = finish(sc, nl ? ntiles : 0, ~0ull, nullptr, s)) return st;
     if (d_count) VX_CUDA(cudaMemcpyAsync(d_count, sc.out2, 8, cudaMemcpyDeviceToDevice, s));
+    if (int st = sync(s)) return st;
+    return radix_check(s);
+}
+
+// Pairs of a join built on the LEFT side and probed with the right (d_probe =
+// right row ids, d_build = left row ids) put into the order of the same join
+// built on the right and probed with the left: left rows ascending, each
+// left row's right rows descending.  Lets a planner build on the smaller side
+// and still return the reference's pair list.
+int voxel_join_pairs_swap_order_dev(const uint32_t* d_probe, const uint32_t* d_build, size_t m, uint32_t* d_left,
+                                    uint32_t* d_right, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    if (m == 0) return kOk;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevBuf key(m * 8), idx(m * 4);
+    if (!key.p || !idx.p) return kErrOutOfMemory;
+    const int sms = sm_count() > 0 ? sm_count() : 148;
+    const unsigned g = static_cast<unsigned>(m / 256 + 1 < static_cast<uint64_t>(sms) * 8 ? m / 256 + 1 : sms * 8);
+    pair_key_kernel<<<g, 256, 0, s>>>(d_build, d_probe, m, key.as<uint64_t>(), idx.as<uint32_t>());
+    VX_CUDA(cudaGetLastError());
+    const size_t tb = radix_tmp_bytes(U64, m);
+    DevBuf tmp(tb);
+    if (!tmp.p) return kErrOutOfMemory;
+    if (int st = launch_radix_sort(U64, key.p, idx.as<uint32_t>(), m, tmp.p, tb, radix_err(s), s, nullptr)) return st;
+    pair_split_kernel<<<g, 256, 0, s>>>(key.as<uint64_t>(), m, d_left, d_right);
+    VX_CUDA(cudaGetLastError());
     if (int st = sync(s)) return st;
     return radix_check(s);
 }

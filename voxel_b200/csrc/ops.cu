@@ -72,30 +72,73 @@ __global__ void table_init_kernel(Table t) {
     }
 }
 
-// phase 1: make sure every key has a slot; counts new groups; flags overflow
-__global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, uint64_t n,
-                                   unsigned long long* groups, uint64_t limit, int* overflow) {
-    unsigned int added = 0;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t k = keys[i];
-        unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
-        uint64_t h = home_slot(k, t.shift);
-        for (uint64_t p = 0;; ++p) {
-            unsigned long long cur = t.slot[h];
-            if (cur == want) break;
-            if (cur == 0) {
-                unsigned long long old = atomicCAS(&t.slot[h], 0ull, want);
-                if (old == 0) { ++added; break; }
-                if (old == want) break;
-            }
-            h = (h + 1) & t.mask;
-            if (p > t.mask) { atomicOr(overflow, 1); break; }
+// Phase 1 bookkeeping, once per warp and row batch: the new groups the warp
+// inserted are added to the table's group count at once, and a count past the
+// load limit raises the overflow flag, which every warp reads here and stops
+// on.  Returns true when the warp should stop.
+__device__ __forceinline__ bool warp_count_groups(unsigned added_now, unsigned long long* groups, uint64_t limit,
+                                                  int* overflow) {
+    const unsigned total = __reduce_add_sync(0xffffffffu, added_now);
+    int stop = 0;
+    if ((threadIdx.x & 31) == 0) {
+        if (total) {
+            const unsigned long long g = atomicAdd(groups, static_cast<unsigned long long>(total)) + total;
+            if (g > limit) atomicOr(overflow, 1);
+        }
+        stop = *reinterpret_cast<volatile int*>(overflow);
+    }
+    return __shfl_sync(0xffffffffu, stop, 0) != 0;
+}
+
+// Claims the key's slot in the global table (the slot word is published with
+// one CAS); returns 1 when this call inserted it, 0 when the key was there,
+// -1 when the probe ran past `probe_limit` slots (the overflow flag is then
+// raised).  Far more threads than slots run at once, so a table sized too
+// small is overfilled within the first row of every thread; the probe limit
+// makes each later probe of that full table give up after a few slots
+// instead of walking all of them.  The host tells a full table (grow) from a
+// long cluster in a lightly loaded one (retry with no limit) by the group
+// count the attempt left.
+__device__ __forceinline__ int claim_slot(const Table& t, uint32_t k, uint64_t probe_limit, int* overflow) {
+    const unsigned long long want = (static_cast<unsigned long long>(k) << 32) | 1ull;
+    uint64_t h = home_slot(k, t.shift);
+    for (uint64_t p = 0;; ++p) {
+        const unsigned long long cur = __ldcg(t.slot + h);
+        if (cur == want) return 0;
+        if (cur == 0) {
+            const unsigned long long old = atomicCAS(&t.slot[h], 0ull, want);
+            if (old == 0) return 1;
+            if (old == want) return 0;
+        }
+        h = (h + 1) & t.mask;
+        if (p >= probe_limit || p > t.mask) {
+            atomicOr(overflow, 1);
+            return -1;
         }
     }
-    if (added) {
-        unsigned long long g = atomicAdd(groups, static_cast<unsigned long long>(added)) + added;
-        if (g > limit) atomicOr(overflow, 1);
+}
+
+// phase 1: make sure every key has a slot; counts new groups; flags overflow.
+// The row loop is warp-uniform (whole warps step together) so the group count
+// can be kept per warp; a block stops claiming as soon as one of its threads
+// met a full table.
+__global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, uint64_t n,
+                                   unsigned long long* groups, uint64_t limit, uint64_t probe_limit, int* overflow) {
+    __shared__ int s_stop;
+    if (threadIdx.x == 0) s_stop = 0;
+    __syncthreads();
+    const uint64_t lane = threadIdx.x & 31;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane); base < n;
+         base += stride) {
+        const uint64_t i = base + lane;
+        unsigned added = 0;
+        if (i < n && !*reinterpret_cast<volatile int*>(&s_stop)) {
+            const int r = claim_slot(t, keys[i], probe_limit, overflow);
+            if (r > 0) added = 1;
+            if (r < 0) s_stop = 1;
+        }
+        if (warp_count_groups(added, groups, limit, overflow)) break;
     }
 }
 
@@ -104,17 +147,22 @@ __global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, u
 // keys another block inserted after the copy) take the global CAS path above.
 __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const uint32_t* __restrict__ keys,
                                                                uint64_t n, unsigned long long* groups, uint64_t limit,
-                                                               int* overflow) {
+                                                               uint64_t probe_limit, int* overflow) {
     extern __shared__ __align__(16) unsigned long long i_slot[];
+    __shared__ int s_stop;
     const uint32_t cap = static_cast<uint32_t>(t.mask + 1), mask = cap - 1;
     for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) i_slot[i] = __ldcg(t.slot + i);
+    if (threadIdx.x == 0) s_stop = 0;
     __syncthreads();
-    unsigned int added = 0;
+    const uint64_t lane = threadIdx.x & 31;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane); base < n;
+         base += 4 * stride) {
+        const uint64_t i0 = base + lane;
         uint32_t kk[4];  // four keys in flight per thread
 #pragma unroll
         for (int u = 0; u < 4; ++u) kk[u] = i0 + u * stride < n ? __ldcs(keys + i0 + u * stride) : 0u;
+        unsigned added = 0;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (i0 + u * stride >= n) break;
@@ -125,29 +173,15 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
             unsigned long long cur;
             while ((cur = i_slot[h]) != want && cur != 0 && probes++ < mask) h = (h + 1) & mask;
             if (cur == want) continue;
-            uint64_t g = home_slot(k, t.shift);
-            for (uint64_t p = 0;; ++p) {
-                const unsigned long long c = __ldcg(t.slot + g);
-                if (c == want) break;
-                if (c == 0) {
-                    const unsigned long long old = atomicCAS(&t.slot[g], 0ull, want);
-                    if (old == 0) {
-                        ++added;
-                        break;
-                    }
-                    if (old == want) break;
-                }
-                g = (g + 1) & t.mask;
-                if (p > t.mask) {
-                    atomicOr(overflow, 1);
-                    break;
-                }
+            if (*reinterpret_cast<volatile int*>(&s_stop)) break;
+            const int r = claim_slot(t, k, probe_limit, overflow);
+            if (r > 0) ++added;
+            if (r < 0) {
+                s_stop = 1;
+                break;
             }
         }
-    }
-    if (added) {
-        const unsigned long long gsum = atomicAdd(groups, static_cast<unsigned long long>(added)) + added;
-        if (gsum > limit) atomicOr(overflow, 1);
+        if (warp_count_groups(added, groups, limit, overflow)) break;
     }
 }
 
@@ -189,6 +223,7 @@ __global__ void accumulate_kernel(Table t, const uint32_t* __restrict__ keys, co
 // word's wrap, read from the atomic's returned old value, ripples upward, so
 // concurrent rows compose to the exact sum in any order.
 constexpr uint32_t kSmemSlots = 2048;
+constexpr uint64_t kProbeLimit = 128;  // slots a phase-1 probe walks before it reports a full table
 constexpr int kAccWords = 6;
 
 struct Words96 {
@@ -603,6 +638,19 @@ int run_ids(const int32_t* keys, uint64_t n, DevBuf& run, cudaStream_t s, uint64
 
 }  // namespace
 
+__global__ void iota_u32_kernel(uint32_t* out, uint64_t n) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<uint32_t>(i);
+}
+
+__global__ void gather_rows_f64_kernel(const double* __restrict__ v, const uint32_t* __restrict__ idx,
+                                       uint64_t n, double* __restrict__ out) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = __ldg(v + __ldg(idx + i));
+}
+
 // ---- device hash aggregator object ------------------------------------------------
 
 class HashAgg {
@@ -647,23 +695,28 @@ public:
         return alloc_table(c, t, mem, s);
     }
 
-    int grow(cudaStream_t s) {
+    int grow(cudaStream_t s, uint64_t factor) {
         Table nt{};
         DevBuf nm;
-        if (int st = alloc_table(cap * 2, nt, nm, s)) return st;
+        if (int st = alloc_table(cap * factor, nt, nm, s)) return st;
         rehash_kernel<<<ogrid(cap), kOThreads, 0, s>>>(t, nt);
         VX_CUDA(cudaGetLastError());
         mem = std::move(nm);
         t = nt;
-        cap *= 2;
+        cap *= factor;
         return kOk;
     }
 
     int accumulate(const uint32_t* dk, const double* dv, uint64_t n, cudaStream_t s) {
         if (!mem.p) if (int st = init(16, s)) return st;
         if (!n) return kOk;
-        // phase 1: insert keys, growing until every key fits under load 0.75
-        for (int attempt = 0; attempt < 40; ++attempt) {
+        // phase 1: insert keys, growing until every key fits under load 0.75.
+        // An attempt that overflowed leaves the exact count of the groups it
+        // inserted: a table (nearly) full grows 8x (a far-too-small size
+        // hint), one past its load limit 2x, and one that gave up on a long
+        // probe at a low load is retried with unbounded probes.
+        uint64_t probe_limit = kProbeLimit;
+        for (int attempt = 0; attempt < 64; ++attempt) {
             VX_CUDA(cudaMemsetAsync(flag_d.p, 0, 4, s));
             uint64_t limit = cap * 3 / 4;
             if (cap <= kSmemSlots) {
@@ -671,10 +724,10 @@ public:
                 uint64_t blocks = (n + 511) / 512;
                 if (blocks > static_cast<uint64_t>(sms) * 4) blocks = static_cast<uint64_t>(sms) * 4;
                 insert_keys_smem_kernel<<<static_cast<unsigned>(blocks), 512, cap * 8, s>>>(
-                    t, dk, n, groups_d.as<unsigned long long>(), limit, flag_d.as<int>());
+                    t, dk, n, groups_d.as<unsigned long long>(), limit, probe_limit, flag_d.as<int>());
             } else {
                 insert_keys_kernel<<<ogrid(n), kOThreads, 0, s>>>(t, dk, n, groups_d.as<unsigned long long>(), limit,
-                                                                  flag_d.as<int>());
+                                                                  probe_limit, flag_d.as<int>());
             }
             VX_CUDA(cudaGetLastError());
             int ovf = 0;
@@ -684,7 +737,13 @@ public:
             if (int st = sync(s)) return st;
             groups = g;
             if (!ovf) break;
-            if (int st = grow(s)) return st;
+            if (g >= cap - cap / 16) {
+                if (int st = grow(s, 8)) return st;
+            } else if (g > limit || g >= cap / 2) {
+                if (int st = grow(s, 2)) return st;
+            } else {
+                probe_limit = ~0ull;
+            }
         }
         if (cap <= kSmemSlots) {  // per-block shared-memory state, one flush per block
             const size_t smem = smem_table_bytes(cap);
@@ -708,9 +767,10 @@ public:
         return ocheck(s, "group-by");
     }
 
-    // groups sorted by key (key_signed: order as i32)
+    // groups sorted by key (key_signed: order as i32); dev_out: the outputs are
+    // device pointers (copied on the stream instead of read back)
     int results(int key_signed, void* okeys, double* osum, double* omin, double* omax, uint64_t* ocount,
-                cudaStream_t s) {
+                cudaStream_t s, bool dev_out = false) {
         if (!groups) return kOk;
         DevBuf k(groups * 4 + 4), sl(groups * 4 + 4), n(8);
         DevBuf ok(groups * 4), os(groups * 8), omn(groups * 8), omx(groups * 8), oc(groups * 8);
@@ -729,11 +789,20 @@ public:
                                                               ok.as<uint32_t>(), os.as<double>(), omn.as<double>(),
                                                               omx.as<double>(), oc.as<uint64_t>());
         VX_CUDA(cudaGetLastError());
-        if (int st = d2h(okeys, ok.p, groups * 4, s)) return st;
-        if (osum) if (int st = d2h(osum, os.p, groups * 8, s)) return st;
-        if (omin) if (int st = d2h(omin, omn.p, groups * 8, s)) return st;
-        if (omax) if (int st = d2h(omax, omx.p, groups * 8, s)) return st;
-        if (ocount) if (int st = d2h(ocount, oc.p, groups * 8, s)) return st;
+        auto out = [&](void* dst, const void* src, size_t bytes) -> int {
+            if (!dst) return kOk;
+            if (dev_out) {
+                VX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+                return kOk;
+            }
+            return d2h(dst, src, bytes, s);
+        };
+        if (int st = out(okeys, ok.p, groups * 4)) return st;
+        if (int st = out(osum, os.p, groups * 8)) return st;
+        if (int st = out(omin, omn.p, groups * 8)) return st;
+        if (int st = out(omax, omx.p, groups * 8)) return st;
+        if (int st = out(ocount, oc.p, groups * 8)) return st;
+        if (dev_out) if (int st = sync(s)) return st;  // the staging buffers are released on return
         return radix_check(s);
     }
 };
@@ -840,6 +909,72 @@ size_t voxel_grouped_sorted_i32_f64(const int32_t* sorted_keys, const double* va
         return static_cast<size_t>(-1);
     if (ocheck(s, "sorted group-by")) return static_cast<size_t>(-1);
     return g;
+}
+
+// ---- group-by over device columns with a chosen plan -----------------------------------
+// method 0: HashAggregator (table sized for expected_groups, grown by doubling
+// if that was too small); 1: sort-based (stable radix sort of the keys with row
+// ids, values gathered, GroupedAggregator over the runs).  Both sum the same
+// fixed-point integers, so the outputs (groups in key order) are bit-identical;
+// the plan only changes the time.  *ngroups (host) gets the group count.
+int voxel_groupby_u32_f64_dev(const uint32_t* d_keys, const double* d_values, size_t n, size_t expected_groups,
+                              int method, uint32_t* d_okeys, double* d_osum, double* d_omin, double* d_omax,
+                              uint64_t* d_ocount, uint64_t* ngroups, void* stream) {
+    clear_error();
+    if (int st = ensure_device()) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (ngroups) *ngroups = 0;
+    if (method != 0 && method != 1) {
+        set_error(kErrInvalidArg, "group-by method %d is neither 0 (hash) nor 1 (sort)", method);
+        return kErrInvalidArg;
+    }
+    if (n == 0) return kOk;
+    if (method == 0) {
+        HashAgg h;
+        if (int st = h.init(expected_groups, s)) return st;
+        if (int st = h.accumulate(d_keys, d_values, n, s)) return st;
+        if (int st = h.results(0, d_okeys, d_osum, d_omin, d_omax, d_ocount, s, true)) return st;
+        if (ngroups) *ngroups = h.groups;
+        return kOk;
+    }
+    if (n >= (1ull << 32)) {
+        set_error(kErrInvalidArg, "sort-based group-by limited to 2^32 rows");
+        return kErrInvalidArg;
+    }
+    DevBuf sk(n * 4), idx(n * 4), sv(n * 8);
+    if (!sk.p || !idx.p || !sv.p) return kErrOutOfMemory;
+    VX_CUDA(cudaMemcpyAsync(sk.p, d_keys, n * 4, cudaMemcpyDeviceToDevice, s));
+    iota_u32_kernel<<<ogrid(n), kOThreads, 0, s>>>(idx.as<uint32_t>(), n);
+    VX_CUDA(cudaGetLastError());
+    {
+        const size_t tb = radix_tmp_bytes(U32, n);
+        DevBuf tmp(tb);
+        if (!tmp.p) return kErrOutOfMemory;
+        if (int st = launch_radix_sort(U32, sk.p, idx.as<uint32_t>(), n, tmp.p, tb, radix_err(s), s, nullptr))
+            return st;
+        gather_rows_f64_kernel<<<ogrid(n), kOThreads, 0, s>>>(d_values, idx.as<uint32_t>(), n, sv.as<double>());
+        VX_CUDA(cudaGetLastError());
+        if (int st = sync(s)) return st;  // tmp is released here
+    }
+    DevBuf run;
+    uint64_t g = 0;
+    // runs only compare keys for equality, so the u32 keys are read as i32 bits
+    if (int st = run_ids(sk.as<int32_t>(), n, run, s, &g)) return st;
+    DevBuf stt(g * 48);
+    if (!stt.p) return kErrOutOfMemory;
+    unsigned long long* sum = stt.as<unsigned long long>();
+    unsigned long long *cnt = sum + 3 * g, *mn = cnt + g, *mx = mn + g;
+    init_runs_kernel<<<ogrid(g), kOThreads, 0, s>>>(sum, cnt, mn, mx, g);
+    grouped_sorted_kernel<<<ogrid(n), kOThreads, 0, s>>>(sk.as<int32_t>(), sv.as<double>(), n, run.as<uint32_t>(),
+                                                         sum, cnt, mn, mx, oerr(s));
+    emit_runs_kernel<<<ogrid(n), kOThreads, 0, s>>>(sk.as<int32_t>(), run.as<uint32_t>(), n, sum, cnt, mn, mx,
+                                                    reinterpret_cast<int32_t*>(d_okeys), d_osum, d_omin, d_omax,
+                                                    d_ocount);
+    VX_CUDA(cudaGetLastError());
+    if (int st = ocheck(s, "sorted group-by")) return st;
+    if (int st = radix_check(s)) return st;
+    if (ngroups) *ngroups = g;
+    return kOk;
 }
 
 // ---- SortOperator / TopK (reference bindings/voxel_c.cpp:187-203) ---------------------

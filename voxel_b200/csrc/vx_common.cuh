@@ -109,4 +109,29 @@ __device__ __forceinline__ bool budget_left(long long start, long long budget) {
     return (clock64() - start) < budget;
 }
 
+// End of the run of keys equal to keys[i] in an ascending array: the first
+// index e > i with keys[e] != keys[i], or n.  Galloping (steps 1, 2, 4, ...)
+// then bisection, so a run of length L costs O(log L) loads -- one load for
+// the common run of one -- rather than a walk of L rows by one thread.
+template <typename K>
+__device__ __forceinline__ uint64_t sorted_run_end(const K* __restrict__ keys, uint64_t i, uint64_t n) {
+    const K k = keys[i];
+    uint64_t good = i, bad = n, step = 1;  // keys[good] == k; bad == n or keys[bad] != k
+    for (;;) {
+        const uint64_t probe = good + step;
+        if (probe >= n) break;
+        if (keys[probe] != k) {
+            bad = probe;
+            break;
+        }
+        good = probe;
+        step <<= 1;
+    }
+    while (bad - good > 1) {
+        const uint64_t mid = good + (bad - good) / 2;
+        if (keys[mid] == k) good = mid; else bad = mid;
+    }
+    return bad;
+}
+
 }  // namespace vx
