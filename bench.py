@@ -940,8 +940,126 @@ def workload_ops(args, L, rank, world, local, dist, dev):
         roof, cpu, e2e, clk.summary(), nl, "mixed")
 
 
+def workload_ops2(args, L, rank, world, local, dist, dev):
+    """Delta / frame-of-reference codecs, merge and semi joins and window
+    functions on device-resident columns, each timed alone with CUDA events on
+    its stream, L2 flushed before every timed launch."""
+    import torch
+
+    n = args.rows if args.rows != ROWS else 1 << 28
+    g = torch.Generator(device=dev)
+    g.manual_seed(6001 + rank)
+    stream = torch.cuda.Stream(dev)
+    sh = stream.cuda_stream
+    nj = min(n, 1 << 24)
+    nw_ = min(n, 1 << 26)
+    with torch.cuda.stream(stream):
+        vals = torch.randint(-(1 << 40), 1 << 40, (n,), generator=g, device=dev, dtype=torch.int64)
+        deltas = torch.empty_like(vals)
+        dec = torch.empty_like(vals)
+        code = torch.randint(-(1 << 31), (1 << 31) - 1, (n,), generator=g, device=dev, dtype=torch.int32)
+        fout = torch.empty(n, dtype=torch.float64, device=dev)
+        # merge join: unique sorted keys, 90% shared
+        lk = torch.sort(torch.randperm(nj * 2, generator=g, device=dev)[: nj].to(torch.int64)).values
+        rk = torch.sort(torch.cat([lk[: nj * 9 // 10], torch.randint(nj * 2, nj * 3, (nj - nj * 9 // 10,),
+                                                                     generator=g, device=dev)]).to(torch.int64)).values
+        lo = torch.empty(nj, dtype=torch.int32, device=dev)
+        ro = torch.empty(nj, dtype=torch.int32, device=dev)
+        c2 = torch.zeros(2, dtype=torch.int64, device=dev)
+        probe = torch.randint(0, nj * 3, (nw_,), generator=g, device=dev, dtype=torch.int64)
+        semi_out = torch.empty(nw_, dtype=torch.int32, device=dev)
+        c1 = torch.zeros(1, dtype=torch.int64, device=dev)
+        x = torch.rand(nw_, generator=g, device=dev, dtype=torch.float64) * 100.0
+        wout = torch.empty(nw_, dtype=torch.float64, device=dev)
+        ts = torch.cumsum(torch.randint(0, 3, (n,), generator=g, device=dev, dtype=torch.int64), 0)
+        tv = torch.rand(n, generator=g, device=dev, dtype=torch.float64)
+        nb = int(ts[-1].item()) // 60 + 1
+        tout = torch.zeros(nb, dtype=torch.float64, device=dev)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream.synchronize()
+    nout = C.c_size_t(0)
+
+    def ok(st):
+        if st:
+            raise RuntimeError(capi.last_error())
+
+    W = 16
+    ops = {
+        "delta_encode_i64": (lambda: ok(L.voxel_delta_encode_dev(2, vals.data_ptr(), n, deltas.data_ptr(), sh)),
+                             n * 16),
+        "delta_decode_i64": (lambda: ok(L.voxel_delta_decode_dev(2, deltas.data_ptr(), n, 0, 0, n, dec.data_ptr(), sh)),
+                             n * 16),
+        "for_decode_f64": (lambda: ok(L.voxel_for_decode_f64_dev(code.data_ptr(), n, -12.5, 3e-7, 0, n,
+                                                                 fout.data_ptr(), sh)), n * 12),
+        "merge_join_i64": (lambda: ok(L.voxel_merge_join_dev(2, lk.data_ptr(), nj, rk.data_ptr(), nj, lo.data_ptr(),
+                                                             ro.data_ptr(), nj, 0, c2.data_ptr(), sh)), None),
+        "semi_join_i64": (lambda: ok(L.voxel_semi_join_dev(2, probe.data_ptr(), nw_, rk.data_ptr(), nj,
+                                                           semi_out.data_ptr(), 0, c1.data_ptr(), sh)), None),
+        "window_sum_f64_w16": (lambda: ok(L.voxel_window_dev(0, 1, x.data_ptr(), nw_, wout.data_ptr(), nw_, W, 0.0,
+                                                             C.byref(nout), sh)), nw_ * 16),
+        "window_stddev_f64_w16": (lambda: ok(L.voxel_window_dev(0, 3, x.data_ptr(), nw_, wout.data_ptr(), nw_, W, 0.0,
+                                                                C.byref(nout), sh)), nw_ * 16),
+        "window_quantile_f64_w16": (lambda: ok(L.voxel_window_dev(0, 5, x.data_ptr(), nw_, wout.data_ptr(), nw_, W,
+                                                                  0.5, C.byref(nout), sh)), nw_ * 16),
+        "time_window_sum_f64": (lambda: ok(L.voxel_time_window_sum_dev(0, ts.data_ptr(), tv.data_ptr(), n, 0, 60,
+                                                                       tout.data_ptr(), nb, C.byref(nout), sh)),
+                                n * 16),
+    }
+    res = {}
+    total_bytes, total_ms, nl = 0, 0.0, 0
+    peak, kind = measured_peak()
+    with ClockSampler(local) as clk:
+        for name, (fn, nbytes) in ops.items():
+            for _ in range(args.warmup):
+                fn()
+            stream.synchronize()
+            ms = []
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.current_stream().synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                stream.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            if name == "merge_join_i64":
+                nbytes = 2 * nj * 8 + int(c2[0].item()) * 8
+            if name == "semi_join_i64":
+                nbytes = nw_ * 8 + nj * 16 + int(c1[0].item()) * 4
+            m = _max_over_ranks(dist, dev, statistics.mean(ms))
+            gbs = nbytes / (m * 1e-3) / 1e9
+            res[name] = {"ms": m, "GB/s": gbs, "frac": gbs / peak, "bytes": nbytes}
+            total_bytes += nbytes
+            total_ms += m
+            nl += args.steps
+    d2 = torch.diff(torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), vals]))
+    checks = {
+        "delta_encode": bool(torch.equal(deltas, d2)),
+        "delta_decode": bool(torch.equal(dec, vals)),
+        "for_decode": bool(torch.equal(fout[:1 << 20], -12.5 + code[:1 << 20].double() * 3e-7)),
+        "merge_join_pairs": bool(torch.equal(lk[lo[:int(c2[0].item())].long()], rk[ro[:int(c2[0].item())].long()])),
+        "merge_join_count": int(c2[0].item()) == int(torch.isin(lk, rk).sum().item()),
+        "semi_join_count": int(c1[0].item()) == int(torch.isin(probe, rk).sum().item()),
+    }
+    value = world * total_bytes / (total_ms * 1e-3) / 1e9
+    roof = _roofline("ops2_kernels", total_bytes, total_ms)
+    roof["note"] = "aggregate of all kernels (sum of algorithmic bytes / sum of launch times); per kernel in config.ops"
+    return _common_line(
+        "codec / join / window kernels GB/s (sum of bytes / sum of times)", UNIT, value, world, args, total_ms,
+        {"workload": f"delta encode / decode and FOR decode of {n} rows, merge join of two {nj}-key sorted unique "
+                     f"i64 columns (90% shared), semi join of {nw_} probe keys against {nj} keys, sliding-window "
+                     f"sum / stddev / quantile (w = {W}) over {nw_} f64, TimeWindowSum of {n} rows into 60-unit "
+                     "buckets; L2 flushed before every launch",
+         "ops": res, "checks": checks, "parallelism": f"replicas x{world}", "peak_source": kind},
+        roof, None,
+        {"value": None, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+         "note": "device-resident inputs only for this workload"},
+        clk.summary(), nl, "i64/f64")
+
+
 WORKLOADS = {"scan": workload_scan, "sort": workload_sort, "join": workload_join, "batch": workload_batch,
-             "ops": workload_ops,
+             "ops": workload_ops, "ops2": workload_ops2,
              "serve": workload_serve}
 
 
@@ -975,7 +1093,7 @@ def main() -> None:
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve", "ops"],
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve", "ops", "ops2"],
                     help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
                          "2^28 f64; sort: radix sort of 2^28 u64; join: hash join 2^24 x 2^29; batch: 4096 "
                          "programs, batched + learned sizing against plain two-pass kernels; serve: serving loop, "
