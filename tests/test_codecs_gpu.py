@@ -106,3 +106,32 @@ def test_codecs_full_size_round_trip_on_device():
     c = code[sample].cpu().numpy().astype(np.float64)
     want = base + (c * scale)  # numpy: one rounding per operation
     assert (out[sample].cpu().numpy() == want).all()
+
+
+def test_delta_decode_device_alignments():
+    """The streaming decode (16-byte aligned deltas) and the plain one
+    (misaligned deltas) against numpy's wrapping cumsum, with outputs at
+    aligned and misaligned addresses and offsets that do and do not fall on a
+    16-byte boundary, across tile boundaries (32 KB tiles) and ragged tails."""
+    L = capi.lib()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(93)
+    for dt, tdt in ((2, torch.int64), (3, torch.int32)):
+        es = 8 if dt == 2 else 4
+        for n in (1, 5, 4095, 4096, 4097, 8193, 1_000_003):
+            host = rng.integers(np.iinfo(NP[dt]).min, np.iinfo(NP[dt]).max, size=n + 4, dtype=NP[dt])
+            buf = torch.from_numpy(host).to(dev)
+            base = int(rng.integers(0, 1 << 30))
+            for shift in (0, 1):  # deltas at the buffer start (aligned) or one element in (misaligned)
+                src = host[shift:shift + n]
+                want = (np.cumsum(src.astype(NP[dt]), dtype=NP[dt]) + NP[dt](base)).astype(NP[dt])
+                for off in (0, 1, 2, 3):
+                    if off >= n:
+                        continue
+                    for oshift in (0, 1):
+                        out = torch.zeros(n + 4, dtype=tdt, device=dev)
+                        st = L.voxel_delta_decode_dev(dt, buf.data_ptr() + shift * es, n, base, off, n - off,
+                                                      out.data_ptr() + oshift * es, None)
+                        assert st == 0, capi.last_error()
+                        got = out.cpu().numpy()[oshift:oshift + n - off]
+                        assert (got == want[off:]).all(), (dt, n, shift, off, oshift)

@@ -61,12 +61,14 @@ def test_windows_against_live_reference_large():
     n = (1 << 22) + 13
     for dt in (0, 2, 3):
         x = inputs.window_values(dt, n, 300 + dt)
-        for kind, w, q in ((1, 16, 0), (2, 5, 0), (3, 32, 0), (4, 7, 0), (5, 21, 0.37), (0, 2, 0)):
+        # windows of at most 16 inputs take the register-tiled kernels, longer ones the shared-memory ones
+        for kind, w, q in ((1, 16, 0), (1, 17, 0), (2, 5, 0), (3, 32, 0), (3, 16, 0), (4, 7, 0), (4, 2, 0),
+                           (5, 21, 0.37), (5, 16, 0.5), (5, 9, 0.0), (5, 2, 1.0), (5, 13, 0.81), (0, 2, 0)):
             want = np.zeros(n, x.dtype)
             m = getattr(R, f"vref_window_{NAME[dt]}")(kind, x.ctypes.data, n, want.ctypes.data, n, w, q)
             got = np.zeros(n, x.dtype)
             g = L.voxel_window(dt, kind, x.ctypes.data, n, got.ctypes.data, n, w, q)
-            assert g == m and (got[:m].view(np.uint8) == want[:m].view(np.uint8)).all(), (dt, kind)
+            assert g == m and (got[:m].view(np.uint8) == want[:m].view(np.uint8)).all(), (dt, kind, w, q)
 
 
 def test_time_window_sum_device_full_size():

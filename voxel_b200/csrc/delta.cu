@@ -13,9 +13,9 @@
 //     (f64) code[offset + i] * Scale, one rounding per operation (no fused
 //     multiply-add), for offset + i < size.
 //
-// B200 design: the delta decode is one single-pass prefix sum (tiles of 2048
-// values per 256-thread block, tile prefixes by decoupled look-back with a
-// 64-bit value beside each flag, since the wrapping sums use all 64 bits),
+// B200 design: the delta decode is one single-pass prefix sum (tiles of 4096
+// values per 256-thread block, tile prefixes by decoupled look-back over
+// fence-free two-word statuses, since the wrapping sums use all 64 bits),
 // outputs staged in shared memory and written coalesced.  The FOR codecs are
 // elementwise streams (the encode adds one min/max reduction).  Everything is
 // HBM-bound integer / FP64 work; nothing uses tensor cores.
@@ -34,27 +34,28 @@ namespace vx {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPer = 8;                        // values per thread
-constexpr int kTile = kThreads * kPer;         // 2048 values per tile
+constexpr int kPer = 16;                       // values per thread
+constexpr int kTile = kThreads * kPer;         // 4096 values per tile
+// shared-memory index of tile value j: one pad slot per 16 values, so a
+// thread's own 16 consecutive values and the warp's coalesced store order
+// both fall in distinct banks
+__device__ __forceinline__ uint32_t pad16(uint32_t j) { return j + (j >> 4); }
 constexpr long long kSpinBudget = 1ll << 31;   // clock cycles (about 1 s)
 
-// Tile status: flag 0 empty, 1 aggregate published, 2 inclusive prefix
-// published; the value is written before its flag (release), read after it
-// (acquire).
+// Tile status: the tile's aggregate and its inclusive prefix, each a 64-bit
+// value published as two words (low half, high half), each word the half
+// shifted up 32 bits with bit 0 set -- zero means not yet written.  A word is
+// written with one single-copy-atomic 64-bit store and a reader takes a
+// value only once both of its words are set, so no fence is needed to order
+// a value against its flag (a release store would wait for the tile's
+// earlier output stores to drain, on the critical path of every tile).
 struct Status64 {
-    uint32_t* flag;
-    unsigned long long* agg;
-    unsigned long long* inc;
+    unsigned long long* agg;  // 2 words per tile
+    unsigned long long* inc;  // 2 words per tile
 };
 
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
@@ -63,34 +64,47 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
     return v;
 }
 
+__device__ __forceinline__ void publish64(unsigned long long* w, uint64_t tile, uint64_t v) {
+    st_relaxed64(w + 2 * tile, (v << 32) | 1ull);
+    st_relaxed64(w + 2 * tile + 1, (v & 0xffffffff00000000ull) | 1ull);
+}
+
+// 0 empty, 1 aggregate, 2 inclusive prefix; *v the value
+__device__ __forceinline__ uint32_t read_status64(Status64 st, int64_t idx, uint64_t* v) {
+    // all four words in one round trip
+    const unsigned long long i0 = ld_relaxed64(st.inc + 2 * idx), i1 = ld_relaxed64(st.inc + 2 * idx + 1);
+    const unsigned long long a0 = ld_relaxed64(st.agg + 2 * idx), a1 = ld_relaxed64(st.agg + 2 * idx + 1);
+    if ((i0 & i1 & 1ull) != 0) {
+        *v = (i0 >> 32) | (i1 & 0xffffffff00000000ull);
+        return 2;
+    }
+    if ((a0 & a1 & 1ull) != 0) {
+        *v = (a0 >> 32) | (a1 & 0xffffffff00000000ull);
+        return 1;
+    }
+    return 0;
+}
+
 // Exclusive prefix (mod 2^64) of `tile` from its predecessors; all 32 lanes of
-// one warp call it and get the same value.  Bounded: when the budget runs out
-// it sets bit 4 of *err and returns what it has.
+// one warp call it and get the same value.  Each step reads 32 predecessors
+// (lane l reads p - l), finds the nearest inclusive prefix with a ballot and
+// adds the aggregates back to it; it spins only while an entry inside that
+// window is still empty.  Bounded: when the budget runs out it sets bit 4 of
+// *err and returns what it has.
 __device__ uint64_t lookback64_warp(Status64 st, uint64_t tile, uint64_t agg, int* err) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
-        if (lane == 0) {
-            st.inc[0] = agg;
-            st_release(&st.flag[0], 2u);
-        }
+        if (lane == 0) publish64(st.inc, 0, agg);
         return 0;
     }
-    if (lane == 0) {
-        st.agg[tile] = agg;
-        st_release(&st.flag[tile], 1u);
-    }
+    if (lane == 0) publish64(st.agg, tile, agg);
     uint64_t excl = 0;
     int64_t p = static_cast<int64_t>(tile) - 1;
     const long long t0 = clock64();
     while (p >= 0) {
         const int64_t idx = p - lane;
-        uint32_t f = 2;  // before tile 0: an inclusive prefix of 0
         uint64_t v = 0;
-        if (idx >= 0) {
-            f = ld_acquire(&st.flag[idx]);
-            if (f == 1) v = ld_relaxed64(&st.agg[idx]);
-            else if (f == 2) v = ld_relaxed64(&st.inc[idx]);
-        }
+        const uint32_t f = idx >= 0 ? read_status64(st, idx, &v) : 2u;  // before tile 0: an inclusive 0
         const unsigned incl = __ballot_sync(0xffffffffu, f == 2);
         const int stop = incl ? __ffs(incl) - 1 : 31;
         const unsigned empty = __ballot_sync(0xffffffffu, f == 0) & (stop == 31 ? 0xffffffffu : ((2u << stop) - 1));
@@ -108,10 +122,7 @@ __device__ uint64_t lookback64_warp(Status64 st, uint64_t tile, uint64_t agg, in
         if (incl) break;
         p -= 32;
     }
-    if (lane == 0) {
-        st.inc[tile] = excl + agg;
-        st_release(&st.flag[tile], 2u);
-    }
+    if (lane == 0) publish64(st.inc, tile, excl + agg);
     return excl;
 }
 
@@ -119,13 +130,13 @@ __device__ uint64_t lookback64_warp(Status64 st, uint64_t tile, uint64_t agg, in
 // unsigned type of T's width), base added; outputs for rows [offset, limit)
 // go to out[row - offset].  Tiles are claimed in launch order from *ctr.
 template <typename U>
-__global__ void __launch_bounds__(kThreads) delta_decode_kernel(const U* __restrict__ deltas, uint64_t limit,
+__global__ void __launch_bounds__(kThreads, 4) delta_decode_kernel(const U* __restrict__ deltas, uint64_t limit,
                                                                 U base, uint64_t offset, U* __restrict__ out,
                                                                 Status64 st, unsigned int* ctr, int vec, int* err) {
     __shared__ uint64_t s_tile;
     __shared__ uint64_t s_warp[kThreads / 32];
     __shared__ uint64_t s_base;
-    __shared__ U s_out[kTile];
+    __shared__ U s_out[kTile + kTile / 16];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t ntiles = (limit + kTile - 1) / kTile;
     for (;;) {
@@ -175,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) delta_decode_kernel(const U* __restr
         const U pre = static_cast<U>(base + static_cast<U>(s_base + s_warp[warp] + incl -
                                                           static_cast<uint64_t>(v[kPer - 1])));
 #pragma unroll
-        for (int k = 0; k < kPer; ++k) s_out[threadIdx.x * kPer + k] = static_cast<U>(pre + v[k]);
+        for (int k = 0; k < kPer; ++k) s_out[pad16(threadIdx.x * kPer + k)] = static_cast<U>(pre + v[k]);
         __syncthreads();
         // coalesced stores of the tile's rows that lie in [offset, limit)
         const uint64_t t0 = tile * kTile;
@@ -183,7 +194,7 @@ __global__ void __launch_bounds__(kThreads) delta_decode_kernel(const U* __restr
         for (int k = 0; k < kPer; ++k) {
             const uint32_t j = threadIdx.x + k * kThreads;
             const uint64_t r = t0 + j;
-            if (r >= offset && r < limit) out[r - offset] = s_out[j];
+            if (r >= offset && r < limit) out[r - offset] = s_out[pad16(j)];
         }
         __syncthreads();
     }
@@ -267,7 +278,7 @@ bool delta_type(int dtype) { return dtype == I64 || dtype == I32 || dtype == U64
 
 size_t delta_scratch_bytes(uint64_t limit) {
     const uint64_t ntiles = (limit + kTile - 1) / kTile;
-    return ntiles * (4 + 8 + 8) + 64;
+    return ntiles * 32 + 64;  // two 2-word statuses per tile + the tile counter
 }
 
 int launch_delta_decode(int dtype, const void* deltas, uint64_t n, uint64_t base_bits, uint64_t offset,
@@ -275,16 +286,14 @@ int launch_delta_decode(int dtype, const void* deltas, uint64_t n, uint64_t base
     if (offset >= n || count == 0) return kOk;
     const uint64_t limit = offset + (count < n - offset ? count : n - offset);
     const uint64_t ntiles = (limit + kTile - 1) / kTile;
-    char* b = static_cast<char*>(scratch);
     Status64 st;
-    st.agg = reinterpret_cast<unsigned long long*>(b);
-    st.inc = st.agg + ntiles;
-    st.flag = reinterpret_cast<uint32_t*>(st.inc + ntiles);
-    unsigned int* ctr = st.flag + ntiles;
-    VX_CUDA(cudaMemsetAsync(st.flag, 0, ntiles * 4 + 4, s));
+    st.agg = static_cast<unsigned long long*>(scratch);
+    st.inc = st.agg + 2 * ntiles;
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(st.inc + 2 * ntiles);
+    VX_CUDA(cudaMemsetAsync(scratch, 0, ntiles * 32 + 4, s));
     const int sms = sm_count() > 0 ? sm_count() : 148;
-    const uint64_t grid = ntiles < static_cast<uint64_t>(sms) * 6 ? ntiles : static_cast<uint64_t>(sms) * 6;
     const int vec = (reinterpret_cast<uintptr_t>(deltas) & 15) == 0 ? 1 : 0;
+    const uint64_t grid = ntiles < static_cast<uint64_t>(sms) * 4 ? ntiles : static_cast<uint64_t>(sms) * 4;
     if (dtype_size(dtype) == 8)
         delta_decode_kernel<uint64_t><<<static_cast<unsigned>(grid), kThreads, 0, s>>>(
             static_cast<const uint64_t*>(deltas), limit, base_bits, offset, static_cast<uint64_t*>(out), st, ctr,

@@ -74,18 +74,23 @@ __global__ void table_init_kernel(Table t) {
 
 // Phase 1 bookkeeping, once per warp and row batch: the new groups the warp
 // inserted are added to the table's group count at once, and a count past the
-// load limit raises the overflow flag, which every warp reads here and stops
-// on.  Returns true when the warp should stop.
+// load limit raises the overflow flag.  `seen` is lane 0's read of the flag,
+// issued at the start of the batch so its latency hides behind the batch's
+// probes.  Returns true when the warp should stop.
+__device__ __forceinline__ int overflow_peek(const int* overflow) {
+    return (threadIdx.x & 31) == 0 ? *reinterpret_cast<const volatile int*>(overflow) : 0;
+}
+
 __device__ __forceinline__ bool warp_count_groups(unsigned added_now, unsigned long long* groups, uint64_t limit,
-                                                  int* overflow) {
+                                                  int* overflow, int seen) {
     const unsigned total = __reduce_add_sync(0xffffffffu, added_now);
-    int stop = 0;
-    if ((threadIdx.x & 31) == 0) {
-        if (total) {
-            const unsigned long long g = atomicAdd(groups, static_cast<unsigned long long>(total)) + total;
-            if (g > limit) atomicOr(overflow, 1);
+    int stop = seen;
+    if ((threadIdx.x & 31) == 0 && total) {
+        const unsigned long long g = atomicAdd(groups, static_cast<unsigned long long>(total)) + total;
+        if (g > limit) {
+            atomicOr(overflow, 1);
+            stop = 1;
         }
-        stop = *reinterpret_cast<volatile int*>(overflow);
     }
     return __shfl_sync(0xffffffffu, stop, 0) != 0;
 }
@@ -131,6 +136,7 @@ __global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, u
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane); base < n;
          base += stride) {
+        const int seen = overflow_peek(overflow);
         const uint64_t i = base + lane;
         unsigned added = 0;
         if (i < n && !*reinterpret_cast<volatile int*>(&s_stop)) {
@@ -138,7 +144,7 @@ __global__ void insert_keys_kernel(Table t, const uint32_t* __restrict__ keys, u
             if (r > 0) added = 1;
             if (r < 0) s_stop = 1;
         }
-        if (warp_count_groups(added, groups, limit, overflow)) break;
+        if (warp_count_groups(added, groups, limit, overflow, seen)) break;
     }
 }
 
@@ -158,6 +164,7 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane); base < n;
          base += 4 * stride) {
+        const int seen = overflow_peek(overflow);
         const uint64_t i0 = base + lane;
         uint32_t kk[4];  // four keys in flight per thread
 #pragma unroll
@@ -181,7 +188,7 @@ __global__ void __launch_bounds__(512) insert_keys_smem_kernel(Table t, const ui
                 break;
             }
         }
-        if (warp_count_groups(added, groups, limit, overflow)) break;
+        if (warp_count_groups(added, groups, limit, overflow, seen)) break;
     }
 }
 

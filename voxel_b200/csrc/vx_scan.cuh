@@ -8,6 +8,11 @@
 // Every wait is bounded: when the budget runs out the kernel records an error
 // in *err and the tile proceeds with what it has (the host reports
 // VOXEL_ETIMEOUT; no spin is unbounded).
+//
+// A status is one 64-bit word (flag and value together), written with one
+// atomic exchange and read with one load, so no fence orders a value against
+// its flag; the look-back communicates nothing else, and a publication never
+// waits for the tile's earlier output stores to drain.
 #pragma once
 
 #include <stdint.h>
@@ -45,7 +50,6 @@ __device__ __forceinline__ uint64_t lookback_exclusive(unsigned long long* statu
         if (flag == kLbInc) break;
         --p;
     }
-    __threadfence();
     atomicExch(&status[tile], kLbInc | ((excl + agg) & kLbValMask));
     return excl;
 }
@@ -91,7 +95,6 @@ __device__ __forceinline__ uint64_t lookback_exclusive_warp(unsigned long long* 
         if (inc) break;
         p -= 32;
     }
-    __threadfence();
     if (lane == 0) atomicExch(&status[tile], kLbInc | ((excl + agg) & kLbValMask));
     return excl;
 }

@@ -27,6 +27,7 @@
 // and adds them to the output with global atomics.
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <type_traits>
 
 #include "voxel_c.h"
@@ -71,6 +72,26 @@ __device__ __forceinline__ T w_sqrt(T a) {
     else return static_cast<T>(__dsqrt_rn(static_cast<double>(a)));  // std::sqrt of an integer, back to T
 }
 
+// Copies src[0, m) into shared memory with every load of the thread issued
+// before its first store (a rolled copy loop waits for each load in turn),
+// between two block barriers.  LOADS * kWThreads >= m.
+template <typename T, int LOADS>
+__device__ __forceinline__ void stage_tile(const T* __restrict__ src, uint32_t m, T* s) {
+    T v[LOADS];
+#pragma unroll
+    for (int q = 0; q < LOADS; ++q) {
+        const uint32_t i = threadIdx.x + q * kWThreads;
+        v[q] = i < m ? __ldg(src + i) : T(0);
+    }
+    __syncthreads();  // the previous tile's readers are done
+#pragma unroll
+    for (int q = 0; q < LOADS; ++q) {
+        const uint32_t i = threadIdx.x + q * kWThreads;
+        if (i < m) s[i] = v[q];
+    }
+    __syncthreads();
+}
+
 template <typename T, int KIND>
 __global__ void __launch_bounds__(kWThreads) window_kernel(const T* __restrict__ data, uint64_t nout, uint32_t w,
                                                            T* __restrict__ out) {
@@ -80,9 +101,7 @@ __global__ void __launch_bounds__(kWThreads) window_kernel(const T* __restrict__
     for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kWTile; t0 < nout;
          t0 += static_cast<uint64_t>(gridDim.x) * kWTile) {
         const uint32_t nt = static_cast<uint32_t>(nout - t0 < kWTile ? nout - t0 : kWTile);
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < nt + halo; i += blockDim.x) s[i] = __ldg(data + t0 + i);
-        __syncthreads();
+        stage_tile<T, (kWTile + kWMaxWin + kWThreads - 1) / kWThreads>(data + t0, nt + halo, s);
         for (uint32_t j = threadIdx.x; j < nt; j += blockDim.x) {
             T r;
             if constexpr (KIND == kDelta) {
@@ -105,6 +124,126 @@ __global__ void __launch_bounds__(kWThreads) window_kernel(const T* __restrict__
                 }
             }
             out[t0 + j] = r;
+        }
+    }
+}
+
+// Register-tiled form of window_kernel (WindowSum, WindowMean) for windows of
+// at most kRW inputs: each thread evaluates kRR consecutive outputs from
+// kRR + w - 1 inputs held in registers (read once from shared memory instead of w times per output),
+// each output still summed left to right from T(0) as the definition is.
+// kRR is odd, so the threads' strided shared-memory reads fall in distinct
+// banks; outputs are staged in shared memory and stored coalesced.
+constexpr int kRW = 16;                 // largest window of the register form
+constexpr int kRR = 9;                  // consecutive outputs per thread
+constexpr int kRTile = kWThreads * kRR; // 2304 outputs per block step
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kWThreads) window_reg_kernel(const T* __restrict__ data, uint64_t nout, uint32_t w,
+                                                               T* __restrict__ out) {
+    __shared__ T s[kRTile + kRW];
+    __shared__ T so[kRTile];
+    const T tw = static_cast<T>(w);
+    const uint32_t halo = w - 1u;
+    for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kRTile; t0 < nout;
+         t0 += static_cast<uint64_t>(gridDim.x) * kRTile) {
+        const uint32_t nt = static_cast<uint32_t>(nout - t0 < kRTile ? nout - t0 : kRTile);
+        stage_tile<T, (kRTile + kRW + kWThreads - 1) / kWThreads>(data + t0, nt + halo, s);
+        const uint32_t j0 = threadIdx.x * kRR;
+        T x[kRR + kRW - 1];
+#pragma unroll
+        for (int k = 0; k < kRR + kRW - 1; ++k) x[k] = j0 + k < nt + halo ? s[j0 + k] : T(0);
+#pragma unroll
+        for (int r = 0; r < kRR; ++r) {
+            T sum = T(0);
+#pragma unroll
+            for (int k = 0; k < kRW; ++k)
+                if (k < static_cast<int>(w)) sum = w_add<T>(sum, x[r + k]);
+            const T res = KIND == kSum ? sum : w_div<T>(sum, tw);
+            if (j0 + r < nt) so[j0 + r] = res;
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nt; j += blockDim.x) out[t0 + j] = so[j];
+    }
+}
+
+// WindowQuantile for windows of at most kRW inputs: the sorted window lives in
+// registers (every index below is a compile-time constant).  The first window
+// is sorted by odd-even transposition; each slide drops data[j] and takes
+// data[j + wq] in one pass that builds every entry from its old neighbours.
+template <typename T>
+__device__ __forceinline__ T pick_entry(const T (&a)[kRW], int idx) {
+    // a[idx] as an OR of masked entries, so the array stays in registers (a
+    // plain select on idx is turned into an indexed local-memory load)
+    using B = typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned int>::type;
+    B acc = 0;
+#pragma unroll
+    for (int i = 0; i < kRW; ++i) {
+        B bits;
+        memcpy(&bits, &a[i], sizeof(T));
+        acc |= bits & (B(0) - B(i == idx));
+    }
+    T r;
+    memcpy(&r, &acc, sizeof(T));
+    return r;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWThreads) quantile_reg_kernel(const T* __restrict__ data, uint64_t nout, int wq,
+                                                                 int lo, int hi, double frac, T* __restrict__ out) {
+    const uint64_t nruns = (nout + kQRun - 1) / kQRun;
+    for (uint64_t run = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; run < nruns;
+         run += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t j0 = run * kQRun;
+        const uint64_t j1 = j0 + kQRun < nout ? j0 + kQRun : nout;
+        T a[kRW];
+#pragma unroll
+        for (int i = 0; i < kRW; ++i) a[i] = i < wq ? __ldg(data + j0 + i) : T(0);
+#pragma unroll
+        for (int round = 0; round < kRW; ++round) {
+#pragma unroll
+            for (int i = round & 1; i + 1 < kRW; i += 2) {
+                if (i + 1 < wq && a[i + 1] < a[i]) {
+                    const T t = a[i];
+                    a[i] = a[i + 1];
+                    a[i + 1] = t;
+                }
+            }
+        }
+        for (uint64_t j = j0; j < j1; ++j) {
+            const T vlo = pick_entry<T>(a, lo), vhi = pick_entry<T>(a, hi);
+            T r = vlo;
+            if (lo != hi) {
+                if constexpr (std::is_same<T, double>::value) {
+                    r = __dadd_rn(vlo, __dmul_rn(__dsub_rn(vhi, vlo), frac));
+                } else {
+                    const double d = static_cast<double>(static_cast<T>(vhi - vlo));
+                    r = static_cast<T>(vlo + static_cast<T>(__dmul_rn(d, frac)));
+                }
+            }
+            out[j] = r;
+            if (j + 1 < j1) {  // slide: drop data[j], take data[j + wq]
+                const T gone = __ldg(data + j), come = __ldg(data + j + wq);
+                int p = 0, ins = 0;  // p: the dropped entry; ins: where `come` goes once it is gone
+#pragma unroll
+                for (int i = 0; i < kRW; ++i)
+                    if (i < wq && a[i] < gone) ++p;
+                if (p >= wq) p = wq - 1;  // NaN-free input always finds it
+#pragma unroll
+                for (int i = 0; i < kRW; ++i)
+                    if (i < wq && i != p && a[i] < come) ++ins;
+                T b[kRW];
+#pragma unroll
+                for (int i = 0; i < kRW; ++i) {
+                    const T dn = i + 1 < kRW ? a[i + 1] : a[i];  // entries left of the drop shift down
+                    const T up = i > 0 ? a[i - 1] : a[i];        // entries right of the insert shift up
+                    const T left = i < p ? a[i] : dn;            // the array without the dropped entry, at i
+                    const T right = i - 1 < p ? up : a[i];       // ... at i - 1
+                    b[i] = i < ins ? left : (i == ins ? come : right);
+                }
+#pragma unroll
+                for (int i = 0; i < kRW; ++i) a[i] = b[i];
+            }
         }
     }
 }
@@ -241,6 +380,105 @@ __global__ void __launch_bounds__(kWThreads) time_window_kernel(const int64_t* _
     if (lane == 0 && m) atomicMax(maxb, m);
 }
 
+// trunc(x / d) for d > 0 (C++ division): for |x| < 2^50 from the double
+// product x * (1/d), whose error is below 1/4, corrected by one step on the
+// integer remainder; other x take the integer division.
+__device__ __forceinline__ int64_t div_trunc(int64_t x, int64_t d, double inv) {
+    if (x > -(1ll << 50) && x < (1ll << 50)) {
+        int64_t q = static_cast<int64_t>(__dmul_rn(static_cast<double>(x), inv));
+        int64_t r = x - q * d;
+        if (x >= 0) {
+            if (r < 0) --q;
+            else if (r >= d) ++q;
+        } else {
+            if (r > 0) ++q;
+            else if (r <= -d) --q;
+        }
+        return q;
+    }
+    return x / d;
+}
+
+// Warp form of the time-bucketed sum: a warp takes chunks of 1024 rows and
+// steps through them 32 consecutive rows at a time (coalesced loads), sums
+// each run of equal buckets with a segmented warp scan, adds every finished
+// run to the output once and carries the run that reaches lane 31 into the
+// next step.  Integer sums are exact; f64 sums group the additions by run
+// instead of the reference's row order.
+constexpr uint64_t kTChunk = 1024;
+constexpr int kTUnroll = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(kWThreads) time_window_warp_kernel(const int64_t* __restrict__ ts,
+                                                                     const T* __restrict__ vals, uint64_t n,
+                                                                     int64_t start, int64_t dur, double inv,
+                                                                     uint64_t nout, T* __restrict__ out,
+                                                                     unsigned long long* maxb) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t wid = static_cast<uint64_t>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    unsigned long long mymax = 0;
+    for (uint64_t c0 = wid * kTChunk; c0 < n; c0 += nwarps * kTChunk) {
+        const uint64_t c1 = c0 + kTChunk < n ? c0 + kTChunk : n;
+        long long cb = -1;  // the carried run's bucket (warp-uniform), -1 none
+        T cacc = T(0);
+        for (uint64_t r0 = c0; r0 < c1; r0 += 32 * kTUnroll) {
+            int64_t tv[kTUnroll];
+            T vv[kTUnroll];
+#pragma unroll
+            for (int u = 0; u < kTUnroll; ++u) {
+                const uint64_t i = r0 + u * 32 + lane;
+                tv[u] = i < c1 ? __ldcs(ts + i) : 0;
+                vv[u] = i < c1 ? __ldcs(vals + i) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < kTUnroll; ++u) {
+                const uint64_t i = r0 + u * 32 + lane;
+                long long b = -1;
+                T v = T(0);
+                if (i < c1) {
+                    const int64_t q = div_trunc(tv[u] - start, dur, inv);
+                    if (q >= 0 && static_cast<uint64_t>(q) < nout) {
+                        b = q;
+                        v = vv[u];
+                        if (static_cast<unsigned long long>(q) > mymax) mymax = static_cast<unsigned long long>(q);
+                    }
+                }
+                const long long bprev = __shfl_up_sync(full, b, 1);
+                const unsigned heads = __ballot_sync(full, lane == 0 || bprev != b);
+                const int sstart = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+                T sv = v;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T y = __shfl_up_sync(full, sv, d);
+                    if (lane - d >= sstart) sv = w_add<T>(sv, y);
+                }
+                const long long b0 = __shfl_sync(full, b, 0);
+                if (cb >= 0) {
+                    if (b0 == cb) {
+                        if (sstart == 0) sv = w_add<T>(sv, cacc);  // the first run continues the carried one
+                    } else if (lane == 0) {
+                        add_out<T>(out, static_cast<uint64_t>(cb), cacc);
+                    }
+                }
+                const long long bnext = __shfl_down_sync(full, b, 1);
+                if (lane != 31 && bnext != b && b >= 0) add_out<T>(out, static_cast<uint64_t>(b), sv);
+                cb = __shfl_sync(full, b, 31);
+                cacc = __shfl_sync(full, sv, 31);
+            }
+        }
+        if (cb >= 0 && lane == 0) add_out<T>(out, static_cast<uint64_t>(cb), cacc);
+    }
+    unsigned long long m = mymax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(full, m, o);
+        m = y > m ? y : m;
+    }
+    if (lane == 0 && m) atomicMax(maxb, m);
+}
+
 int w_grid(uint64_t work, int per_sm = 8) {
     const int sms = sm_count() > 0 ? sm_count() : 148;
     const uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
@@ -264,6 +502,16 @@ int launch_t(int kind, const void* d_data, uint64_t nout, uint32_t w, double q, 
     const T* in = static_cast<const T*>(d_data);
     T* o = static_cast<T*>(d_out);
     const uint64_t tiles = (nout + kWTile - 1) / kWTile;
+    const uint64_t rtiles = (nout + kRTile - 1) / kRTile;
+    // sums and means of short windows from registers; the statistics stay on
+    // the shared-memory kernel, where more resident warps hide the latency of
+    // their FP64 chains (measured faster)
+    if (w <= static_cast<uint32_t>(kRW) && (kind == kSum || kind == kMean)) {
+        if (kind == kSum) window_reg_kernel<T, kSum><<<w_grid(rtiles), kWThreads, 0, s>>>(in, nout, w, o);
+        else window_reg_kernel<T, kMean><<<w_grid(rtiles), kWThreads, 0, s>>>(in, nout, w, o);
+        VX_CUDA(cudaGetLastError());
+        return kOk;
+    }
     switch (kind) {
     case kDelta: window_kernel<T, kDelta><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
     case kSum: window_kernel<T, kSum><<<w_grid(tiles), kWThreads, 0, s>>>(in, nout, w, o); break;
@@ -279,8 +527,12 @@ int launch_t(int kind, const void* d_data, uint64_t nout, uint32_t w, double q, 
         if (hi >= wq) hi = lo;
         const double frac = pos - static_cast<double>(lo);
         const uint64_t runs = (nout + kQRun - 1) / kQRun;
-        quantile_kernel<T><<<w_grid((runs + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(in, nout, wq, lo, hi,
-                                                                                            frac, o);
+        if (wq <= kRW)
+            quantile_reg_kernel<T><<<w_grid((runs + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(in, nout, wq, lo,
+                                                                                                    hi, frac, o);
+        else
+            quantile_kernel<T><<<w_grid((runs + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(in, nout, wq, lo, hi,
+                                                                                                frac, o);
         break;
     }
     }
@@ -315,9 +567,10 @@ int check_args(int dtype, int kind) {
 template <typename T>
 int launch_time_t(const int64_t* ts, const void* vals, uint64_t n, int64_t start, int64_t dur, void* out,
                   uint64_t nout, unsigned long long* maxb, cudaStream_t s) {
-    const uint64_t chunks = (n + kTRows - 1) / kTRows;
-    time_window_kernel<T><<<w_grid((chunks + kWThreads - 1) / kWThreads), kWThreads, 0, s>>>(
-        ts, static_cast<const T*>(vals), n, start, dur, nout, static_cast<T*>(out), maxb);
+    const uint64_t chunks = (n + kTChunk - 1) / kTChunk;  // one warp per chunk
+    const double inv = 1.0 / static_cast<double>(dur);
+    time_window_warp_kernel<T><<<w_grid((chunks + kWThreads / 32 - 1) / (kWThreads / 32)), kWThreads, 0, s>>>(
+        ts, static_cast<const T*>(vals), n, start, dur, inv, nout, static_cast<T*>(out), maxb);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
