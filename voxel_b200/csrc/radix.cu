@@ -39,6 +39,7 @@ constexpr uint32_t kStAgg = 1u << 30;
 constexpr uint32_t kStInc = 2u << 30;
 constexpr uint32_t kStMask = (1u << 30) - 1;
 constexpr long long kSpinBudget = 1ll << 31;
+constexpr int kLbBatch = 4;  // look-back statuses loaded per round trip
 
 template <typename K>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
@@ -180,20 +181,35 @@ __global__ void __launch_bounds__(kRThreads, ITEMS >= 16 ? 1 : 2) onesweep_kerne
                 atomicExch(st, kStInc | (tcount & kStMask));
             } else {
                 atomicExch(st, kStAgg | (tcount & kStMask));
+                // walk back kLbBatch predecessors per round trip (all loads
+                // issued, then consumed newest first)
                 int64_t p = static_cast<int64_t>(tile) - 1;
                 long long t0 = clock64();
-                while (p >= 0) {
-                    unsigned int s = *reinterpret_cast<volatile unsigned int*>(status + p * kRadix + d);
-                    unsigned int flag = s & ~kStMask;
-                    if (flag == 0) {
-                        if (clock64() - t0 > kSpinBudget) { atomicOr(err, 4); break; }
-                        continue;
+                bool done = false;
+                while (!done && p >= 0) {
+                    unsigned int sv[kLbBatch];
+#pragma unroll
+                    for (int j = 0; j < kLbBatch; ++j)
+                        sv[j] = p - j >= 0 ? static_cast<unsigned int>(*reinterpret_cast<volatile unsigned int*>(
+                                                 status + (p - j) * kRadix + d))
+                                           : static_cast<unsigned int>(kStInc);  // before tile 0: an inclusive 0
+                    int used = 0;
+#pragma unroll
+                    for (int j = 0; j < kLbBatch; ++j) {
+                        if (done || used < j) continue;  // stopped at an empty entry or the inclusive one
+                        const unsigned int flag = sv[j] & ~kStMask;
+                        if (flag == 0) continue;
+                        if (p - j >= 0) excl += sv[j] & kStMask;
+                        used = j + 1;
+                        if (flag == kStInc) done = true;
                     }
-                    excl += s & kStMask;
-                    if (flag == kStInc) break;
-                    --p;
+                    p -= used;
+                    if (!done && used == 0 && clock64() - t0 > kSpinBudget) {
+                        atomicOr(err, 4);
+                        break;
+                    }
                 }
-                __threadfence();
+                // one status word carries flag and value: no fence needed
                 atomicExch(st, kStInc | static_cast<unsigned int>((excl + tcount) & kStMask));
             }
             uint64_t g = static_cast<uint64_t>(digit_offs[d]) + excl;
