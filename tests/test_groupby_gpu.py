@@ -78,7 +78,7 @@ def test_full_size_properties():
 def test_every_variant_gives_identical_bits():
     """The exact kernel variants (merged 192-bit atomics at 4/8/16 rows per
     thread, 32-bit word table with and without the warp queue at 4/8, the
-    lean word table) sum the same integers, so every output bit agrees; the
+    lean word table, the prefetching word table) sum the same integers, so every output bit agrees; the
     TMA-fed variant (compensated f64 per warp) and all of them match the
     oracle."""
     L = capi.lib()
@@ -90,7 +90,7 @@ def test_every_variant_gives_identical_bits():
             for pthr, qlo, qhi in preds:
                 w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], pthr, qlo, qhi)
                 base = None
-                for v in (4, 8, 16, 1, 2, 3, 5, 6, 7, 0):
+                for v in (4, 8, 16, 1, 2, 3, 5, 6, 7, 9, 0):
                     assert L.voxel_scan_groupby_tune(v) == 0
                     got = gpu_scan_groupby(d, pthr, qlo, qhi)
                     k, s, mn, mx, c = got
@@ -169,7 +169,7 @@ def test_lean_word_table_extremes_and_negative_products():
         for pthr, qlo, qhi in ((-1e9, -100, 100), (36.99, -50, 50), (-1e9, -1, -1)):
             w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], pthr, qlo, qhi)
             outs = []
-            for v in (1, 7):
+            for v in (1, 7, 9):
                 assert L.voxel_scan_groupby_tune(v) == 0
                 got = gpu_scan_groupby(d, pthr, qlo, qhi)
                 k, s, mn, mx, c = got
@@ -178,8 +178,9 @@ def test_lean_word_table_extremes_and_negative_products():
                 assert (mx.view(np.uint64) == w[3].view(np.uint64)).all()
                 np.testing.assert_allclose(s, w[1], rtol=1e-12, atol=1e-300)
                 outs.append(got)
-            for a, b in zip(*outs):
-                assert a.size == b.size and (a.view(np.uint8) == b.view(np.uint8)).all()
+            for other in outs[1:]:
+                for a, b in zip(outs[0], other):
+                    assert a.size == b.size and (a.view(np.uint8) == b.view(np.uint8)).all()
     finally:
         L.voxel_scan_groupby_tune(-1)
 

@@ -183,8 +183,8 @@ def test_autotuner_times_and_caches_radix_and_scan(tmp_path):
             assert g == w[0].size, capi.last_error()
             assert (ok[:g] == w[0]).all() and (c[:g] == w[4]).all() and (mn[:g] == w[2]).all()
             np.testing.assert_allclose(s[:g], w[1], rtol=1e-12, atol=0)
-        fam = "scan_groupby_v2_card%d" % (card.bit_length() - 1)
-        assert L.voxel_tune_lookup(fam.encode(), T.F64, d["price"].size) in (0, 1, 2, 3, 4)
+        fam = "scan_groupby_v3_card%d" % (card.bit_length() - 1)
+        assert L.voxel_tune_lookup(fam.encode(), T.F64, d["price"].size) in (0, 1, 2, 3, 4, 5)
         entries = json.loads(path.read_text())
         assert {e.split("|")[1] for e in entries} == {"radix_onesweep", fam}
         # tuning off: nothing new is timed or cached

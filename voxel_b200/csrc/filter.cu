@@ -10,6 +10,7 @@
 // atomic per block, and compaction is a single pass whose block offsets come
 // from a decoupled look-back over per-tile popcounts.
 #include "filter.h"
+#include "tune.h"
 #include "voxel_c.h"
 #include "vx_common.cuh"
 #include "vx_runtime.h"
@@ -253,8 +254,11 @@ size_t selection_scratch_bytes(uint64_t rows) {
     return (ntiles + 1) * 8 + 64;
 }
 
-int launch_selection(const uint64_t* bm, uint64_t rows, uint32_t* out, unsigned long long* count, void* scratch,
-                     int* err, cudaStream_t s) {
+namespace {
+// one selection pass with `per_sm` resident blocks per SM (tiles are claimed
+// dynamically, so any grid gives the same rows)
+int selection_pass(const uint64_t* bm, uint64_t rows, uint32_t* out, unsigned long long* count, void* scratch,
+                   int* err, cudaStream_t s, int per_sm) {
     uint64_t nwords = (rows + 63) / 64;
     uint64_t ntiles = (nwords + kSelWords - 1) / kSelWords;
     VX_CUDA(cudaMemsetAsync(scratch, 0, selection_scratch_bytes(rows), s));
@@ -263,11 +267,31 @@ int launch_selection(const uint64_t* bm, uint64_t rows, uint32_t* out, unsigned 
     unsigned long long* status = static_cast<unsigned long long*>(scratch);
     unsigned int* ctr = reinterpret_cast<unsigned int*>(status + ntiles);
     int sms = sm_count() > 0 ? sm_count() : 148;
-    uint64_t blocks = ntiles < static_cast<uint64_t>(sms) * 8 ? ntiles : static_cast<uint64_t>(sms) * 8;
+    const uint64_t cap = static_cast<uint64_t>(sms) * per_sm;
+    uint64_t blocks = ntiles < cap ? ntiles : cap;
     selection_kernel<<<static_cast<unsigned>(blocks), kSelThreads, 0, s>>>(bm, nwords, rows, out, count, status, ctr,
                                                                           err);
     VX_CUDA(cudaGetLastError());
     return kOk;
+}
+}  // namespace
+
+// Fewer resident tiles shorten every tile's look-back walk (the walk passes
+// over the tiles still in flight) but keep fewer loads in flight: the
+// autotuner times 1, 2, 4 and 8 blocks per SM once per (GPU, log2 rows) on the
+// call's own bitmap (every choice writes the same rows) and keeps the fastest.
+int launch_selection(const uint64_t* bm, uint64_t rows, uint32_t* out, unsigned long long* count, void* scratch,
+                     int* err, cudaStream_t s) {
+    static const int kPerSm[4] = {1, 2, 4, 8};
+    int c = 3;  // 8 blocks per SM unless tuned
+    if (rows >= (1ull << 22)) {
+        const std::string key = tune_key("selection_grid", U32, rows);
+        if (!tune_lookup(key, &c))
+            c = tune_pick(key, 4, 3, s, [&](int k) { return selection_pass(bm, rows, out, count, scratch, err, s,
+                                                                           kPerSm[k]); });
+        if (c < 0 || c > 3) c = 3;
+    }
+    return selection_pass(bm, rows, out, count, scratch, err, s, kPerSm[c]);
 }
 
 int launch_bitmap_and(const uint64_t* const* d_bms, int nbm, uint64_t rows, uint64_t* out, unsigned long long* count,

@@ -202,8 +202,12 @@ struct WarpQueue {
 //         a 32-bit count, and min/max keys; rows reach the lanes through the
 //         warp queue (all 32 lanes busy);
 // MODE 2: as MODE 1, rows added where they are read (no queue).
+// MODE 3: MODE 1 with the block's next tile of price and qty loaded into
+//         registers before the current tile is filtered and its queue
+//         consumed, so each warp keeps a tile of loads in flight while it
+//         aggregates (two blocks per SM: the second register set).
 template <int RPT, int MODE>
-__global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
+__device__ __forceinline__ void scan_groupby_body(
     const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
     const double* __restrict__ price, const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo,
     int32_t qhi, GlobalGroups g, unsigned int* done, int32_t* out_keys, double* out_sum, double* out_min,
@@ -347,6 +351,30 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
         }
     };
 
+    constexpr bool PF = MODE == 3;
+    auto load_tile = [&](uint64_t tt, double (&lp)[RPT], int32_t (&lq)[RPT]) {
+        const uint64_t l0 = tt * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
+        if (l0 + RPT <= n) {
+#pragma unroll
+            for (int k = 0; k < RPT; k += 4) {
+                const double2* pp = reinterpret_cast<const double2*>(price + l0 + k);
+                double2 a = __ldcs(pp), b = __ldcs(pp + 1);
+                int4 q = __ldcs(reinterpret_cast<const int4*>(qty + l0 + k));
+                lp[k] = a.x; lp[k + 1] = a.y; lp[k + 2] = b.x; lp[k + 3] = b.y;
+                lq[k] = q.x; lq[k + 1] = q.y; lq[k + 2] = q.z; lq[k + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                bool in = l0 + k < n;
+                lp[k] = in ? price[l0 + k] : __longlong_as_double(0x7FF8000000000000ll);
+                lq[k] = in ? qty[l0 + k] : 0;
+            }
+        }
+    };
+    double nextp[RPT];  // PF: the block's next tile, in flight while this one is processed
+    int32_t nextq[RPT];
+    if (PF && blockIdx.x < ntiles) load_tile(blockIdx.x, nextp, nextq);
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         if (since_flush == tiles_per_flush) {
             __syncwarp();
@@ -363,22 +391,15 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
         const uint64_t r0 = t * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
         double pv[RPT];
         int32_t qv[RPT];
-        if (r0 + RPT <= n) {
-#pragma unroll
-            for (int k = 0; k < RPT; k += 4) {
-                const double2* pp = reinterpret_cast<const double2*>(price + r0 + k);
-                double2 a = __ldcs(pp), b = __ldcs(pp + 1);
-                int4 q = __ldcs(reinterpret_cast<const int4*>(qty + r0 + k));
-                pv[k] = a.x; pv[k + 1] = a.y; pv[k + 2] = b.x; pv[k + 3] = b.y;
-                qv[k] = q.x; qv[k + 1] = q.y; qv[k + 2] = q.z; qv[k + 3] = q.w;
-            }
-        } else {
+        if (PF) {
 #pragma unroll
             for (int k = 0; k < RPT; ++k) {
-                bool in = r0 + k < n;
-                pv[k] = in ? price[r0 + k] : __longlong_as_double(0x7FF8000000000000ll);
-                qv[k] = in ? qty[r0 + k] : 0;
+                pv[k] = nextp[k];
+                qv[k] = nextq[k];
             }
+            if (t + gridDim.x < ntiles) load_tile(t + gridDim.x, nextp, nextq);
+        } else {
+            load_tile(t, pv, qv);
         }
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
@@ -460,6 +481,28 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(
         *done = 0;
     }
 }
+
+#define VX_GB_PARAMS                                                                                             \
+    const uint64_t *__restrict__ packed, uint32_t width, const int32_t *__restrict__ dict, uint32_t card,         \
+        const double *__restrict__ price, const int32_t *__restrict__ qty, uint64_t n, double pthr, int32_t qlo,  \
+        int32_t qhi, GlobalGroups g, unsigned int *done, int32_t *out_keys, double *out_sum, double *out_min,     \
+        double *out_max, uint64_t *out_count, uint64_t *out_ngroups, int *status
+#define VX_GB_ARGS \
+    packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, done, out_keys, out_sum, out_min, out_max, \
+        out_count, out_ngroups, status
+
+template <int RPT, int MODE>
+__global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(VX_GB_PARAMS) {
+    scan_groupby_body<RPT, MODE>(VX_GB_ARGS);
+}
+
+// MODE 3 holds a second tile in registers: sized for two blocks per SM
+template <int RPT>
+__global__ void __launch_bounds__(kGbThreads, 2) scan_groupby_pf_kernel(VX_GB_PARAMS) {
+    scan_groupby_body<RPT, 3>(VX_GB_ARGS);
+}
+#undef VX_GB_PARAMS
+#undef VX_GB_ARGS
 
 // ---------------------------------------------------------------------------
 // TMA-fed variant for dictionaries up to kTmaMaxCard entries.
@@ -1390,6 +1433,12 @@ int launch_tw(ScanGroupBy& S, int nstages, const uint64_t* packed, uint32_t widt
     return kOk;
 }
 
+template <int RPT, int MODE>
+auto fused_kernel_of() {
+    if constexpr (MODE == 3) return scan_groupby_pf_kernel<RPT>;
+    else return scan_groupby_kernel<RPT, MODE>;
+}
+
 // dynamic shared memory of the MODE 1, 2 table: min, max (8 bytes each), five
 // accumulator words and a count (4 bytes each) per group -- the MODE 0 size
 template <int RPT, int MODE>
@@ -1397,15 +1446,16 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
                const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
                int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
     constexpr int kTile = kGbThreads * RPT;
+    auto* const kern = fused_kernel_of<RPT, MODE>();
     size_t smem = scan_groupby_smem_bytes(card);
     static thread_local uint32_t attr_set_for = 0;
     if (attr_set_for < card) {
-        VX_CUDA(cudaFuncSetAttribute(scan_groupby_kernel<RPT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
         attr_set_for = kMaxGroups;
     }
     int per_sm = 0;
-    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_groupby_kernel<RPT, MODE>, kGbThreads, smem));
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGbThreads, smem));
     if (per_sm < 1) per_sm = 1;
     int sms = sm_count() > 0 ? sm_count() : 148;
     uint64_t ntiles = (n + kTile - 1) / kTile;
@@ -1413,12 +1463,12 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
     GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
-    scan_groupby_kernel<RPT, MODE><<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
-        packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, S.g_done, ok, os, omn, omx, oc, ong,
-        static_cast<int*>(S.status.p));
+    kern<<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(packed, width, dict, card, price, qty, n, pthr, qlo,
+                                                               qhi, g, S.g_done, ok, os, omn, omx, oc, ong,
+                                                               static_cast<int*>(S.status.p));
     VX_CUDA(cudaGetLastError());
     S.last_grid = static_cast<int>(grid);
-    S.last_kernel = MODE == 0 ? 0 : MODE + 1;
+    S.last_kernel = MODE == 0 ? 0 : MODE == 3 ? 7 : MODE + 1;
     return kOk;
 }
 
@@ -1556,17 +1606,19 @@ int ScanGroupBy::launch(const uint64_t* packed, uint32_t width, const int32_t* d
             case 2: return VX_LAUNCH_RPT(4, 2);
             case 3: return VX_LAUNCH_RPT(8, 2);
             case 4: return lean_ok ? VX_LAUNCH_LEAN() : VX_LAUNCH_RPT(4, 1);
+            case 5: return VX_LAUNCH_RPT(4, 3);
             default: return VX_LAUNCH_RPT(4, 1);
             }
         };
         int cl = 0;
         while (cl < 31 && (2u << cl) <= card) ++cl;
-        const std::string family = "scan_groupby_v2_card" + std::to_string(cl);
+        const std::string family = "scan_groupby_v3_card" + std::to_string(cl);
         const std::string key = tune_key(family.c_str(), F64, n);
         int c = 0;
-        if (!tune_lookup(key, &c)) c = tune_pick(key, 5, 0, s, variant);
+        if (!tune_lookup(key, &c)) c = tune_pick(key, 6, 0, s, variant);
         return variant(c);
     }
+    if (mode == 3) return VX_LAUNCH_RPT(4, 3);
     if (mode == 1) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 1) : VX_LAUNCH_RPT(4, 1);
     if (mode == 2) return rows_per_thread == 8 ? VX_LAUNCH_RPT(8, 2) : VX_LAUNCH_RPT(4, 2);
     switch (rows_per_thread) {
@@ -1697,7 +1749,7 @@ int voxel_scan_groupby_dev(const uint64_t* d_packed, size_t nwords, uint32_t wid
 int voxel_scan_groupby_tune(int variant) {
     clear_error();
     // validate before touching the state: a rejected id leaves the previous choice in place
-    const bool known = variant == -1 || (variant >= 0 && variant <= 7) || variant == 8 || variant == 16;
+    const bool known = variant == -1 || (variant >= 0 && variant <= 9) || variant == 16;
     if (!known) {
         set_error(kErrInvalidArg, "unknown fused-scan variant %d", variant);
         return kErrInvalidArg;
@@ -1716,6 +1768,12 @@ int voxel_scan_groupby_tune(int variant) {
     }
     if (variant == 0) {
         S.use_tma = true;
+        return kOk;
+    }
+    if (variant == 9) {  // word table + queue with the next tile prefetched into registers
+        S.use_tma = false;
+        S.mode = 3;
+        S.rows_per_thread = 4;
         return kOk;
     }
     if (variant == 6) {  // bulk-copy-fed word table where the shape allows, else variant 1
@@ -1751,6 +1809,7 @@ int voxel_scan_groupby_tune_state(void) {
     if (S.use_tw) return 6;
     if (S.mode == 1) return S.rows_per_thread == 8 ? 2 : 1;
     if (S.mode == 2) return S.rows_per_thread == 8 ? 5 : 3;
+    if (S.mode == 3) return 9;
     return S.rows_per_thread;
 }
 

@@ -9,7 +9,7 @@
 //     launch of the batched executor; programs that arrive while a batch runs
 //     form the next batch, prepared on the host while the device works on the
 //     previous one (two batches in flight, alternating streams);
-//   - operator workers (kOpWorkers threads, one stream each) run group-by
+//   - operator workers (kOpWorkers = 8 threads, one stream each) run group-by
 //     and join requests, several at once.
 // Both workers admit work by device-memory footprint: a request reserves its
 // estimated working memory from a shared budget before it starts and returns
@@ -48,7 +48,7 @@ struct Request {
     uint64_t id = 0;
     int kind = kProgram;
     size_t footprint = 0;
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_start, t_done;  // t_start: admitted to a worker
     int status = kOk;
     bool done = false;
     std::string error;
@@ -203,9 +203,24 @@ public:
         return kOk;
     }
 
+    // mean time in the arrival queue and in service, per request kind
+    int breakdown(int kind, double* queue_ms, double* service_ms, uint64_t* n) {
+        if (kind < 0 || kind > 2) {
+            set_error(kErrInvalidArg, "request kind %d outside 0..2", kind);
+            return kErrInvalidArg;
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        const Breakdown& b = by_kind_[kind];
+        if (queue_ms) *queue_ms = b.n ? b.queue_ms / b.n : 0.0;
+        if (service_ms) *service_ms = b.n ? b.service_ms / b.n : 0.0;
+        if (n) *n = b.n;
+        return kOk;
+    }
+
     void reset_stats() {
         std::lock_guard<std::mutex> lk(mu_);
         lat_.clear();
+        for (auto& b : by_kind_) b = Breakdown{};
         peak_ = in_use_;
     }
 
@@ -218,6 +233,7 @@ private:
             if (in_use_ + r->footprint > budget_) break;  // head of line waits for memory
             in_use_ += r->footprint;
             peak_ = std::max(peak_, in_use_);
+            r->t_start = Clock::now();
             out.push_back(r);
             q.pop_front();
         }
@@ -232,6 +248,10 @@ private:
             r->done = true;
             in_use_ -= r->footprint;
             lat_.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+            Breakdown& b = by_kind_[r->kind];
+            b.queue_ms += std::chrono::duration<double, std::milli>(r->t_start - r->t_submit).count();
+            b.service_ms += std::chrono::duration<double, std::milli>(r->t_done - r->t_start).count();
+            ++b.n;
         }
         cv_done_.notify_all();
         cv_work_.notify_all();  // memory came back: the other worker may admit now
@@ -404,10 +424,15 @@ private:
     std::deque<Request*> prog_q_, op_q_;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs_;
     std::vector<double> lat_;
+    struct Breakdown {
+        double queue_ms = 0, service_ms = 0;
+        uint64_t n = 0;
+    };
+    Breakdown by_kind_[3];
     uint64_t next_id_ = 0;
     size_t in_use_ = 0, peak_ = 0;
     bool stop_ = false;
-    static constexpr int kOpWorkers = 4;
+    static constexpr int kOpWorkers = 8;
     std::thread prog_thread_;
     std::vector<std::thread> op_threads_;
 };
@@ -499,5 +524,10 @@ int voxel_server_stats(void* s, uint64_t* completed, double* p50_ms, double* p99
 }
 
 void voxel_server_reset_stats(void* s) { static_cast<Server*>(s)->reset_stats(); }
+
+int voxel_server_breakdown(void* s, int kind, double* queue_ms, double* service_ms, uint64_t* completed) {
+    clear_error();
+    return static_cast<Server*>(s)->breakdown(kind, queue_ms, service_ms, completed);
+}
 
 }  // extern "C"

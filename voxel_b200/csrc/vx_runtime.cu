@@ -188,16 +188,110 @@ cudaStream_t thread_stream() {
     return g_stream;
 }
 
+// Copies between the device and pageable host memory go through two pinned
+// chunks of this thread's own (the host-side memcpy of one chunk overlaps the
+// DMA of the other).  Left to the driver, a pageable copy passes through its
+// shared staging path, and one thread's large pageable copy then holds up
+// every other thread's -- the serving loop's workers copy results out
+// concurrently.  Pinned host memory and small copies go straight.
+namespace {
+constexpr size_t kStageChunk = 8u << 20;
+constexpr size_t kStageMin = 64u << 10;
+struct CopyStage {
+    char* p = nullptr;  // 2 x kStageChunk, pinned
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool used[2] = {false, false};
+    bool failed = false;
+    ~CopyStage() {
+        if (p) cudaFreeHost(p);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+thread_local CopyStage g_copy;
+
+bool stage_ready() {
+    if (g_copy.p) return true;
+    if (g_copy.failed) return false;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, 2 * kStageChunk, cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g_copy.ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g_copy.ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (p) cudaFreeHost(p);
+        g_copy.failed = true;  // the driver's own path then
+        return false;
+    }
+    g_copy.p = static_cast<char*>(p);
+    return true;
+}
+
+bool pageable(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// waits until this thread's staging chunk k is no longer read or written by a copy
+int stage_wait(int k) {
+    if (g_copy.used[k]) {
+        VX_CUDA(cudaEventSynchronize(g_copy.ev[k]));
+        g_copy.used[k] = false;
+    }
+    return kOk;
+}
+}  // namespace
+
 int h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (bytes == 0) return kOk;
-    VX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
-    return kOk;
+    if (bytes < kStageMin || !pageable(src) || !stage_ready()) {
+        VX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return kOk;
+    }
+    const char* in = static_cast<const char*>(src);
+    char* out = static_cast<char*>(dst);
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += kStageChunk, k ^= 1) {
+        const size_t c = bytes - off < kStageChunk ? bytes - off : kStageChunk;
+        if (int st = stage_wait(k)) return st;
+        char* chunk = g_copy.p + k * kStageChunk;
+        std::memcpy(chunk, in + off, c);
+        VX_CUDA(cudaMemcpyAsync(out + off, chunk, c, cudaMemcpyHostToDevice, s));
+        VX_CUDA(cudaEventRecord(g_copy.ev[k], s));
+        g_copy.used[k] = true;
+    }
+    return kOk;  // the source may be reused: every byte is in a staging chunk or on the device
 }
 
 int d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (bytes == 0) return kOk;
-    VX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
-    return kOk;
+    if (bytes < kStageMin || !pageable(dst) || !stage_ready()) {
+        VX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        return kOk;
+    }
+    const char* in = static_cast<const char*>(src);
+    char* out = static_cast<char*>(dst);
+    size_t pend_off = 0, pend_len = 0;  // the chunk in flight in the other half
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += kStageChunk, k ^= 1) {
+        const size_t c = bytes - off < kStageChunk ? bytes - off : kStageChunk;
+        if (int st = stage_wait(k)) return st;
+        VX_CUDA(cudaMemcpyAsync(g_copy.p + k * kStageChunk, in + off, c, cudaMemcpyDeviceToHost, s));
+        VX_CUDA(cudaEventRecord(g_copy.ev[k], s));
+        g_copy.used[k] = true;
+        if (pend_len) {  // drain the previous chunk while this one is copied
+            if (int st = stage_wait(k ^ 1)) return st;
+            std::memcpy(out + pend_off, g_copy.p + (k ^ 1) * kStageChunk, pend_len);
+        }
+        pend_off = off;
+        pend_len = c;
+    }
+    if (int st = stage_wait(k ^ 1)) return st;
+    std::memcpy(out + pend_off, g_copy.p + (k ^ 1) * kStageChunk, pend_len);
+    return kOk;  // like a pageable copy, complete on return
 }
 
 int sync(cudaStream_t s) {

@@ -25,6 +25,7 @@ class Server:
         if not self.h:
             raise ServerError(capi.last_error())
         self._host = {}
+        self._outbufs = {}
 
     def close(self):
         if self.h:
@@ -49,24 +50,47 @@ class Server:
             raise ServerError(capi.last_error())
         return rid
 
-    def submit_program(self, prog, dcol, n: int | None = None, want_selection: bool = False, capacity: int = 0,
-                       dsel=None) -> int:
+    def prepare_program(self, prog, dcol, n: int | None = None, want_selection: bool = False, capacity: int = 0,
+                        dsel=None) -> tuple:
+        """The submission arguments of a program over a device column, built
+        once (a prepared statement): `submit_prepared` then costs one C call."""
         n = dcol.numel() if n is None else n
         regs = np.array(prog.registers(n), np.uint64)
         code = np.asarray(prog.code, np.uint32)
-        rid = self.L.voxel_server_submit_program(self.h, prog.dtype, code.ctypes.data, code.size, regs.ctypes.data,
-                                                 dcol.data_ptr(), n, int(want_selection), capacity,
-                                                 dsel.data_ptr() if dsel is not None else None)
-        return self._check(rid)
+        return (prog.dtype, code, regs, dcol.data_ptr(), n, int(want_selection), capacity,
+                dsel.data_ptr() if dsel is not None else None)
+
+    def submit_prepared(self, p: tuple) -> int:
+        dtype, code, regs, col, n, want, cap, sel = p
+        return self._check(self.L.voxel_server_submit_program(self.h, dtype, code.ctypes.data, code.size,
+                                                              regs.ctypes.data, col, n, want, cap, sel))
+
+    def submit_program(self, prog, dcol, n: int | None = None, want_selection: bool = False, capacity: int = 0,
+                       dsel=None) -> int:
+        return self.submit_prepared(self.prepare_program(prog, dcol, n, want_selection, capacity, dsel))
+
+    # group-by outputs go to host buffers reused across requests: a fresh
+    # array faults its pages in during the device-to-host copy, which then
+    # runs at a fraction of the link rate
+    def _take_outputs(self, cap: int) -> dict:
+        cls = 1 << max(cap - 1, 0).bit_length()
+        free = self._outbufs.setdefault(cls, [])
+        if free:
+            return free.pop()
+        out = dict(keys=np.ones(cls, np.uint32), sum=np.ones(cls), min=np.ones(cls), max=np.ones(cls),
+                   count=np.ones(cls, np.uint64))  # written once here, so every page is resident
+        out["_cls"] = cls
+        return out
 
     def submit_groupby(self, dkeys, dvals, expected_groups: int, capacity: int | None = None) -> int:
         cap = capacity if capacity is not None else max(expected_groups, 1)
-        out = dict(keys=np.zeros(cap, np.uint32), sum=np.zeros(cap), min=np.zeros(cap), max=np.zeros(cap),
-                   count=np.zeros(cap, np.uint64))
+        out = self._take_outputs(cap)
         rid = self.L.voxel_server_submit_groupby(self.h, dkeys.data_ptr(), dvals.data_ptr(), dkeys.numel(),
                                                  expected_groups, cap, out["keys"].ctypes.data,
                                                  out["sum"].ctypes.data, out["min"].ctypes.data,
                                                  out["max"].ctypes.data, out["count"].ctypes.data)
+        if not rid:
+            self._outbufs[out["_cls"]].append(out)
         self._check(rid)
         self._host[rid] = out
         return rid
@@ -100,7 +124,8 @@ class Server:
         if host is not None:  # group-by: `count` becomes the per-group counts
             g = r["count"]
             r["groups"] = g
-            r.update({k: v[:g].copy() for k, v in host.items()})
+            r.update({k: v[:g].copy() for k, v in host.items() if k != "_cls"})
+            self._outbufs[host["_cls"]].append(host)
         return r
 
     def stats(self) -> dict:
@@ -110,6 +135,17 @@ class Server:
         self.L.voxel_server_stats(self.h, C.byref(n), C.byref(p50), C.byref(p99), C.byref(mean), C.byref(peak))
         return {"completed": n.value, "p50_ms": p50.value, "p99_ms": p99.value, "mean_ms": mean.value,
                 "peak_reserved_bytes": peak.value}
+
+    def breakdown(self) -> dict:
+        """Mean queue and service milliseconds per request kind."""
+        out = {}
+        for k, name in enumerate(("program", "groupby", "join")):
+            q, sv, n = C.c_double(0), C.c_double(0), C.c_uint64(0)
+            if self.L.voxel_server_breakdown(self.h, k, C.byref(q), C.byref(sv), C.byref(n)):
+                raise ServerError(capi.last_error())
+            if n.value:
+                out[name] = {"queue_ms": q.value, "service_ms": sv.value, "n": n.value}
+        return out
 
     def reset_stats(self) -> None:
         self.L.voxel_server_reset_stats(self.h)
