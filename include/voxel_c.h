@@ -581,6 +581,11 @@ void      voxel_server_reset_stats(void* server);
  * 2 join) spent in the arrival queue and in service since the last reset. */
 int       voxel_server_breakdown(void* server, int kind, double* queue_ms, double* service_ms,
                                  uint64_t* completed);
+/* Program batches since the last reset: how many, their programs, the largest,
+ * the host milliseconds spent lowering + uploading + launching them (total and
+ * the longest) and waiting for their results. */
+int       voxel_server_batch_stats(void* server, uint64_t* batches, uint64_t* programs, uint64_t* max_batch,
+                                   double* build_ms, double* max_build_ms, double* wait_ms);
 
 /* ================================================================
  * Additive: learned cardinality / selectivity estimator.

@@ -61,6 +61,38 @@ def test_vfilter_full_size():
         assert (got == want).all()
 
 
+def test_vfilter_four_byte_types_ragged_and_misaligned():
+    """4-byte columns against numpy's predicate for every comparison, at ragged
+    sizes around the 256-row warp step, with device pointers at and off the
+    16-byte boundary; nothing is written past the last bitmap word."""
+    import torch
+
+    L = capi.lib()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(23)
+    ops = {0: np.equal, 1: np.not_equal, 2: np.less, 3: np.less_equal, 4: np.greater, 5: np.greater_equal}
+    for dt, npt, tt in ((T.I32, np.int32, torch.int32), (T.U32, np.uint32, torch.int32), (T.F32, np.float32, torch.float32)):
+        for n in (1, 3, 63, 64, 65, 511, 512, 513, 4097, 100_003):
+            host = rng.integers(0, 40, n + 4).astype(npt)
+            buf = torch.from_numpy(host.view(np.int32) if npt is np.uint32 else host).to(dev)
+            for shift in (0, 1, 3):
+                col = host[shift:shift + n]
+                for op in range(7):
+                    a, b = npt(12), npt(30)
+                    m = (col >= a) & (col <= b) if op == 6 else ops[op](col, a)
+                    words = (n + 63) // 64
+                    bm = torch.zeros(words + 1, dtype=torch.int64, device=dev)
+                    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+                    st = L.voxel_vfilter_dev(dt, op, buf.data_ptr() + 4 * shift, n, bits(dt, a), bits(dt, b), bm.data_ptr(),
+                                             cnt.data_ptr(), None)
+                    assert st == 0, capi.last_error()
+                    torch.cuda.synchronize()
+                    want = np.packbits(m, bitorder="little")
+                    got = bm.cpu().numpy().view(np.uint8)[: want.size]
+                    assert (got == want).all() and int(cnt.item()) == int(m.sum()), (dt, n, shift, op)
+                    assert int(bm[words].item()) == 0  # nothing written past the last word
+
+
 def test_selection_and_bitmap_and(golden):
     L = capi.lib()
     for case in golden["ops"]["selection"]:

@@ -197,6 +197,7 @@ _SIGS = {
     "voxel_server_stats": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "voxel_server_reset_stats": (None, [vp]),
     "voxel_server_breakdown": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "voxel_server_batch_stats": (C.c_int, [vp, vp, vp, vp, vp, vp, vp]),
     "voxel_hashjoin_i64": (sz, [vp, sz, vp, sz, vp, vp, sz, C.c_int]),
     "voxel_hashjoin_i64_dev": (C.c_int, [vp, vp, sz, vp, sz, vp, vp, sz, C.c_int, vp, vp]),
 }

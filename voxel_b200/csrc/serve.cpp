@@ -217,10 +217,23 @@ public:
         return kOk;
     }
 
+    int batch_stats(uint64_t* batches, uint64_t* programs, uint64_t* max_batch, double* build_ms,
+                    double* max_build_ms, double* wait_ms) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (batches) *batches = bstat_.batches;
+        if (programs) *programs = bstat_.programs;
+        if (max_batch) *max_batch = bstat_.max_batch;
+        if (build_ms) *build_ms = bstat_.build_ms;
+        if (max_build_ms) *max_build_ms = bstat_.max_build_ms;
+        if (wait_ms) *wait_ms = bstat_.wait_ms;
+        return kOk;
+    }
+
     void reset_stats() {
         std::lock_guard<std::mutex> lk(mu_);
         lat_.clear();
         for (auto& b : by_kind_) b = Breakdown{};
+        bstat_ = BatchStats{};
         peak_ = in_use_;
     }
 
@@ -263,8 +276,25 @@ private:
         cudaStream_t stream = nullptr;
     };
 
+    // host time to lower, upload and launch a batch, and its size
+    void note_batch(size_t n, Clock::time_point t0) {
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        std::lock_guard<std::mutex> lk(mu_);
+        ++bstat_.batches;
+        bstat_.programs += n;
+        bstat_.max_batch = std::max<uint64_t>(bstat_.max_batch, n);
+        bstat_.build_ms += ms;
+        bstat_.max_build_ms = std::max(bstat_.max_build_ms, ms);
+    }
+
     void complete_batch(InFlight& f) {
+        const auto t_wait = Clock::now();
         int st = f.batch->fetch(f.stream);
+        {
+            const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t_wait).count();
+            std::lock_guard<std::mutex> lk(mu_);
+            bstat_.wait_ms += ms;
+        }
         std::string err = st ? last_error() : "";
         for (size_t i = 0; i < f.reqs.size(); ++i) {
             Request* r = f.reqs[i];
@@ -302,6 +332,7 @@ private:
                 take = admit(prog_q_, max_batch_);
             }
             if (!take.empty()) {
+                const auto t_build = Clock::now();
                 InFlight& f = slot[cur];
                 f.stream = streams[cur];
                 f.batch = std::make_unique<Batch>();
@@ -332,6 +363,7 @@ private:
                     f.batch.reset();
                 } else {
                     int st = f.batch->launch(f.stream, false);
+                    note_batch(f.reqs.size(), t_build);
                     if (st) {
                         std::string err = last_error();
                         for (Request* r : f.reqs) {
@@ -429,6 +461,11 @@ private:
         uint64_t n = 0;
     };
     Breakdown by_kind_[3];
+    struct BatchStats {
+        uint64_t batches = 0, programs = 0, max_batch = 0;
+        double build_ms = 0, max_build_ms = 0, wait_ms = 0;
+    };
+    BatchStats bstat_;
     uint64_t next_id_ = 0;
     size_t in_use_ = 0, peak_ = 0;
     bool stop_ = false;
@@ -524,6 +561,12 @@ int voxel_server_stats(void* s, uint64_t* completed, double* p50_ms, double* p99
 }
 
 void voxel_server_reset_stats(void* s) { static_cast<Server*>(s)->reset_stats(); }
+
+int voxel_server_batch_stats(void* s, uint64_t* batches, uint64_t* programs, uint64_t* max_batch,
+                             double* build_ms, double* max_build_ms, double* wait_ms) {
+    clear_error();
+    return static_cast<Server*>(s)->batch_stats(batches, programs, max_batch, build_ms, max_build_ms, wait_ms);
+}
 
 int voxel_server_breakdown(void* s, int kind, double* queue_ms, double* service_ms, uint64_t* completed) {
     clear_error();

@@ -147,5 +147,14 @@ class Server:
                 out[name] = {"queue_ms": q.value, "service_ms": sv.value, "n": n.value}
         return out
 
+    def batch_stats(self) -> dict:
+        """Program batches: count, programs, largest, host build / wait ms."""
+        b, p, m = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        bm, mb, wm = C.c_double(0), C.c_double(0), C.c_double(0)
+        self.L.voxel_server_batch_stats(self.h, C.byref(b), C.byref(p), C.byref(m), C.byref(bm), C.byref(mb),
+                                        C.byref(wm))
+        return {"batches": b.value, "programs": p.value, "max_batch": m.value, "build_ms": bm.value,
+                "max_build_ms": mb.value, "wait_ms": wm.value}
+
     def reset_stats(self) -> None:
         self.L.voxel_server_reset_stats(self.h)
