@@ -120,6 +120,44 @@ def test_selection_and_bitmap_and(golden):
         del C_ptrs
 
 
+def test_bitpack_decode_device_alignments():
+    """Whole 4096-value tiles decode four values per thread into 16-byte
+    stores when the output is 16-byte aligned, the per-value path otherwise:
+    both equal the input for widths 1..32, with offsets and ragged tails, and
+    through a dictionary."""
+    import torch
+
+    L = capi.lib()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(24)
+    for w in (1, 3, 10, 17, 31, 32):
+        for n in (4096, 3 * 4096 + 77, 40_001):
+            v = rng.integers(0, (1 << w) - 1, n, dtype=np.uint64, endpoint=True).astype(np.uint32)
+            words = encode.bitpack(v, w)
+            dw = torch.from_numpy(words.view(np.int64)).to(dev)
+            for off in (0, 4096, 5):
+                if off >= n:
+                    continue
+                for oshift in (0, 1):
+                    out = torch.zeros(n + 8, dtype=torch.int32, device=dev)
+                    st = L.voxel_bitpack_decode_dev(dw.data_ptr(), words.size, w, n, off, n - off,
+                                                    out.data_ptr() + 4 * oshift, None)
+                    assert st == 0, capi.last_error()
+                    got = out.cpu().numpy().view(np.uint32)[oshift:oshift + n - off]
+                    assert (got == v[off:]).all(), (w, n, off, oshift)
+    dct = np.arange(1000, dtype=np.int32) * 7 - 3000
+    v = rng.integers(0, 1000, 9000).astype(np.uint32)
+    words = encode.bitpack(v, 10)
+    dw = torch.from_numpy(words.view(np.int64)).to(dev)
+    dd = torch.from_numpy(dct).to(dev)
+    for oshift in (0, 1):
+        out = torch.zeros(9000 + 8, dtype=torch.int32, device=dev)
+        st = L.voxel_dict_bitpack_decode_i32_dev(dw.data_ptr(), words.size, 10, dd.data_ptr(), dct.size, v.size, 0,
+                                                 v.size, out.data_ptr() + 4 * oshift, None)
+        assert st == 0, capi.last_error()
+        assert (out.cpu().numpy()[oshift:oshift + 9000] == dct[v]).all()
+
+
 def test_decoders_golden_and_round_trip(golden):
     L = capi.lib()
     for case in golden["ops"]["bitpack"]:

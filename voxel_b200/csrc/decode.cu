@@ -33,7 +33,7 @@ template <bool DICT>
 __global__ void __launch_bounds__(kDThreads) unpack_tile_kernel(const uint64_t* __restrict__ words, uint64_t nwords,
                                                                 uint32_t w, const int32_t* __restrict__ dict,
                                                                 uint32_t card, uint64_t offset, uint64_t count,
-                                                                uint32_t* __restrict__ out, int* err) {
+                                                                uint32_t* __restrict__ out, int vec_out, int* err) {
     __shared__ uint64_t s_w[kUnpackWords + 1];  // + one word read (masked off) past the last value
     extern __shared__ __align__(16) int32_t s_dict[];
     const bool dict_smem = DICT && card <= 8192;
@@ -57,6 +57,37 @@ __global__ void __launch_bounds__(kDThreads) unpack_tile_kernel(const uint64_t* 
         if (threadIdx.x == 0) s_w[nwl] = 0;  // words past nwords read as zero
         __syncthreads();
         const uint32_t b0 = static_cast<uint32_t>(r0 * w - wi0 * 64);  // the tile's first bit in s_w (< 64)
+        if (vec_out && nb == kUnpackRows) {
+            // a whole tile: each thread decodes groups of 4 consecutive values (one
+            // 16-byte store; lanes store consecutive groups), bit positions stepped
+            // by w, no per-value bounds (the staged words cover the tile, and the
+            // zero word after them covers the second word of the last value)
+            uint4* out4 = reinterpret_cast<uint4*>(out + tile * kUnpackRows);
+#pragma unroll
+            for (int e = 0; e < kUnpackRows / (4 * kDThreads); ++e) {
+                const uint32_t g = threadIdx.x + e * kDThreads;
+                uint32_t bit = b0 + g * 4 * w;
+                uint32_t o[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const uint32_t q = bit >> 5;
+                    uint32_t k = __funnelshift_r(s_w32[q], s_w32[q + 1], bit & 31) & mask;
+                    bit += w;
+                    if constexpr (DICT) {
+                        if (k >= card) {
+                            bad = true;
+                            k = 0;
+                        } else {
+                            k = static_cast<uint32_t>(dict_smem ? s_dict[k] : __ldg(dict + k));
+                        }
+                    }
+                    o[i] = k;
+                }
+                out4[g] = make_uint4(o[0], o[1], o[2], o[3]);
+            }
+            __syncthreads();
+            continue;
+        }
 #pragma unroll 4
         for (int e = 0; e < kUnpackRows / kDThreads; ++e) {
             const uint32_t j = threadIdx.x + e * kDThreads;
@@ -301,8 +332,9 @@ int launch_bitunpack(const uint64_t* words, uint64_t nwords, uint32_t w, uint64_
     if (offset >= value_count) return kOk;
     if (count > value_count - offset) count = value_count - offset;  // reference stops at ValueCount
     if (!count) return kOk;
+    const int vec_out = (reinterpret_cast<uintptr_t>(out) & 15) == 0 ? 1 : 0;
     unpack_tile_kernel<false><<<unpack_grid(count), kDThreads, 0, s>>>(words, nwords, w, nullptr, 0, offset, count,
-                                                                      out, nullptr);
+                                                                      out, vec_out, nullptr);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -318,8 +350,10 @@ int launch_dict_bitunpack_i32(const uint64_t* words, uint64_t nwords, uint32_t w
     if (count > value_count - offset) count = value_count - offset;
     if (!count) return kOk;
     size_t smem = card <= 8192 ? card * sizeof(int32_t) : 0;
+    const int vec_out = (reinterpret_cast<uintptr_t>(out) & 15) == 0 ? 1 : 0;
     unpack_tile_kernel<true><<<unpack_grid(count), kDThreads, smem, s>>>(words, nwords, w, dict, card, offset, count,
-                                                                        reinterpret_cast<uint32_t*>(out), err);
+                                                                        reinterpret_cast<uint32_t*>(out), vec_out,
+                                                                        err);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
