@@ -121,8 +121,8 @@ __global__ void bitmap_and_kernel(const uint64_t* const* bms, int nbm, uint64_t 
 // reads word round*32 + l, coalesced); a round's rows are gathered in the
 // warp's shared-memory stage and stored as one contiguous run.
 constexpr int kSelThreads = 128;
-constexpr int kSelRounds = 16;
-constexpr int kSelWords = kSelThreads * kSelRounds;  // 2048 words = 131072 rows per tile
+constexpr int kSelRounds = 8;
+constexpr int kSelWords = kSelThreads * kSelRounds;  // 1024 words = 65536 rows per tile
 
 __global__ void __launch_bounds__(kSelThreads) selection_kernel(const uint64_t* __restrict__ bitmap, uint64_t nwords,
                                                                 uint64_t rows, uint32_t* __restrict__ out,

@@ -22,6 +22,7 @@
 // to sorted output rows and resets it for the next launch.
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "fixedpoint.cuh"
 #include "groupby.h"
@@ -111,6 +112,17 @@ __device__ __forceinline__ uint32_t key_bits(const uint64_t* __restrict__ packed
     return static_cast<uint32_t>(v & mask);
 }
 
+// key_bits for scans whose bit offsets fit 32 bits (rows x width < 2^32): the
+// queue holds the row's bit offset, and the decode is two 32-bit loads and a
+// funnel shift (nw32: 32-bit words of the packed column that hold values)
+__device__ __forceinline__ uint32_t key_bits32(const uint32_t* __restrict__ p32, uint32_t bit, uint32_t nw32,
+                                               uint32_t mask32) {
+    const uint32_t q = bit >> 5;
+    const uint32_t lo = __ldg(p32 + q);
+    const uint32_t hi = q + 1 < nw32 ? __ldg(p32 + q + 1) : 0u;
+    return __funnelshift_r(lo, hi, bit & 31) & mask32;
+}
+
 // Word form of a row value for the 32-bit table (MODE 1, 2): the magnitude
 // trunc(|x| * 2^76) -- the integer fix_from_double_s<76> produces -- as three
 // 32-bit words c0..c2 placed at word k0 of a 160-bit group accumulator.
@@ -189,8 +201,11 @@ __device__ __forceinline__ Fix3 fix_from_words(const uint32_t* w) {
 constexpr int kQueue = 64;
 // Entries carry the row, its price and qty; the key decode and the price*qty
 // product happen when the queue is consumed, with all 32 lanes busy.
+// B32: the entry's position is the row's 32-bit bit offset in the packed
+// column, else the 64-bit row index.
+template <bool B32>
 struct WarpQueue {
-    uint64_t row[kQueue];
+    typename std::conditional<B32, uint32_t, uint64_t>::type pos[kQueue];
     double price[kQueue];
     int32_t qty[kQueue];
 };
@@ -206,7 +221,7 @@ struct WarpQueue {
 //         registers before the current tile is filtered and its queue
 //         consumed, so each warp keeps a tile of loads in flight while it
 //         aggregates (two blocks per SM: the second register set).
-template <int RPT, int MODE>
+template <int RPT, int MODE, bool B32 = false>
 __device__ __forceinline__ void scan_groupby_body(
     const uint64_t* __restrict__ packed, uint32_t width, const int32_t* __restrict__ dict, uint32_t card,
     const double* __restrict__ price, const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo,
@@ -268,10 +283,13 @@ __device__ __forceinline__ void scan_groupby_body(
     bool bad_value = false, bad_key = false;
     uint64_t since_flush = 0;
 
-    __shared__ WarpQueue s_queue[kGbThreads / 32];
+    __shared__ WarpQueue<B32> s_queue[kGbThreads / 32];
     const int lane = threadIdx.x & 31;
     const unsigned lanemask_lt = (1u << lane) - 1;
-    WarpQueue& Q = s_queue[threadIdx.x >> 5];
+    WarpQueue<B32>& Q = s_queue[threadIdx.x >> 5];
+    const uint32_t* const p32 = reinterpret_cast<const uint32_t*>(packed);
+    const uint32_t nw32 = B32 ? static_cast<uint32_t>((n * width + 63) / 64 * 2) : 0u;
+    const uint32_t mask32 = static_cast<uint32_t>(mask);
     int qn = 0;  // warp-uniform fill of Q (a ring of kQueue entries from qh)
     int qh = 0;
     // qty in [qlo, qhi] as one unsigned compare; an empty range passes nothing
@@ -305,7 +323,8 @@ __device__ __forceinline__ void scan_groupby_body(
         if (valid) {
             const int e = (qh + lane) & (kQueue - 1);
             p = Q.price[e];
-            gi = key_bits(packed, Q.row[e], width, mask);
+            if constexpr (B32) gi = key_bits32(p32, Q.pos[e], nw32, mask32);
+            else gi = key_bits(packed, Q.pos[e], width, mask);
             // one rounded multiply, as the reference materialises price*qty
             v = __dmul_rn(p, static_cast<double>(Q.qty[e]));
         }
@@ -414,7 +433,8 @@ __device__ __forceinline__ void scan_groupby_body(
             unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
                 const int pos = (qh + qn + __popc(m & lanemask_lt)) & (kQueue - 1);
-                Q.row[pos] = r;
+                if constexpr (B32) Q.pos[pos] = static_cast<uint32_t>(r) * width;  // < 2^32 by the launch check
+                else Q.pos[pos] = r;
                 Q.price[pos] = p;
                 Q.qty[pos] = q;
             }
@@ -491,15 +511,15 @@ __device__ __forceinline__ void scan_groupby_body(
     packed, width, dict, card, price, qty, n, pthr, qlo, qhi, g, done, out_keys, out_sum, out_min, out_max, \
         out_count, out_ngroups, status
 
-template <int RPT, int MODE>
+template <int RPT, int MODE, bool B32 = false>
 __global__ void __launch_bounds__(kGbThreads) scan_groupby_kernel(VX_GB_PARAMS) {
-    scan_groupby_body<RPT, MODE>(VX_GB_ARGS);
+    scan_groupby_body<RPT, MODE, B32>(VX_GB_ARGS);
 }
 
 // MODE 3 holds a second tile in registers: sized for two blocks per SM
-template <int RPT>
+template <int RPT, bool B32 = false>
 __global__ void __launch_bounds__(kGbThreads, 2) scan_groupby_pf_kernel(VX_GB_PARAMS) {
-    scan_groupby_body<RPT, 3>(VX_GB_ARGS);
+    scan_groupby_body<RPT, 3, B32>(VX_GB_ARGS);
 }
 #undef VX_GB_PARAMS
 #undef VX_GB_ARGS
@@ -1433,10 +1453,10 @@ int launch_tw(ScanGroupBy& S, int nstages, const uint64_t* packed, uint32_t widt
     return kOk;
 }
 
-template <int RPT, int MODE>
+template <int RPT, int MODE, bool B32>
 auto fused_kernel_of() {
-    if constexpr (MODE == 3) return scan_groupby_pf_kernel<RPT>;
-    else return scan_groupby_kernel<RPT, MODE>;
+    if constexpr (MODE == 3) return scan_groupby_pf_kernel<RPT, B32>;
+    else return scan_groupby_kernel<RPT, MODE, B32>;
 }
 
 // dynamic shared memory of the MODE 1, 2 table: min, max (8 bytes each), five
@@ -1446,13 +1466,16 @@ int launch_rpt(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int
                const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
                int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
     constexpr int kTile = kGbThreads * RPT;
-    auto* const kern = fused_kernel_of<RPT, MODE>();
+    // the queue modes keep 32-bit bit offsets when rows x width < 2^32
+    constexpr bool kQueued = MODE == 1 || MODE == 3;
+    const bool b32 = kQueued && n * static_cast<uint64_t>(width) < (1ull << 32);
+    auto* const kern = b32 ? fused_kernel_of<RPT, MODE, kQueued>() : fused_kernel_of<RPT, MODE, false>();
     size_t smem = scan_groupby_smem_bytes(card);
-    static thread_local uint32_t attr_set_for = 0;
-    if (attr_set_for < card) {
+    static thread_local uint32_t attr_set_for[2] = {0, 0};  // per B32 instance
+    if (attr_set_for[b32] < card) {
         VX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(scan_groupby_smem_bytes(kMaxGroups))));
-        attr_set_for = kMaxGroups;
+        attr_set_for[b32] = kMaxGroups;
     }
     int per_sm = 0;
     VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGbThreads, smem));
