@@ -109,6 +109,14 @@ class Server:
 
     def result(self, rid: int) -> dict:
         """Waits for the request and returns its outputs (the request is then forgotten)."""
+        try:
+            return self._result(rid)
+        finally:  # a group-by's host buffers go back to the pool, also after an error
+            host = self._host.pop(rid, None)
+            if host is not None:
+                self._outbufs[host["_cls"]].append(host)
+
+    def _result(self, rid: int) -> dict:
         self.wait(rid)
         regs = np.zeros(64, np.uint64)
         cnt = np.zeros(1, np.uint64)
@@ -120,12 +128,11 @@ class Server:
             raise ServerError(capi.last_error())
         r = {"registers": [int(x) for x in regs], "count": int(cnt[0]), "aux": int(aux[0]),
              "latency_ms": lat.value}
-        host = self._host.pop(rid, None)
+        host = self._host.get(rid)
         if host is not None:  # group-by: `count` becomes the per-group counts
             g = r["count"]
             r["groups"] = g
             r.update({k: v[:g].copy() for k, v in host.items() if k != "_cls"})
-            self._outbufs[host["_cls"]].append(host)
         return r
 
     def stats(self) -> dict:
