@@ -217,6 +217,31 @@ def test_radix_sort_golden_and_properties(golden):
         assert (idx == order).all() and (k == k0[order]).all()
 
 
+def test_radix_sort_skips_constant_digit_passes():
+    """Keys narrower than their type (row ids in u64, small signed values,
+    constant high bytes) skip the passes whose digit is the same for every key;
+    odd and even numbers of remaining passes, and no pass at all, still give
+    numpy's stable permutation."""
+    L = capi.lib()
+    rng = np.random.default_rng(29)
+    n = (1 << 20) + 9
+    cases = [
+        (T.U64, rng.integers(0, 1 << 20, n, dtype=np.uint64)),                # 3 passes of 8
+        (T.U64, rng.integers(0, 1 << 16, n, dtype=np.uint64) << np.uint64(8)),  # 2 passes, digit 0 constant
+        (T.I64, rng.integers(-1000, 1000, n).astype(np.int64)),               # sign byte and low bytes
+        (T.I64, rng.integers(5, 300, n).astype(np.int64)),                    # non-negative only
+        (T.U32, (rng.integers(0, 1 << 8, n, dtype=np.uint32) << np.uint32(24)) | np.uint32(0x00ABCD00)),  # 1 pass
+        (T.I32, np.full(n, -7, np.int32)),                                    # every pass skipped
+        (T.U32, rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)),  # all passes
+    ]
+    for dt, k0 in cases:
+        k = k0.copy()
+        idx = np.arange(n, dtype=np.uint32)
+        assert L.voxel_radix_sort(dt, k.ctypes.data, idx.ctypes.data, n) == 0, capi.last_error()
+        order = np.argsort(k0, kind="stable")
+        assert (idx == order).all() and (k == k0[order]).all(), (dt, k0[:4])
+
+
 def test_autotuner_times_and_caches_radix_and_scan(tmp_path):
     """First calls of a shape time the candidate configurations, cache the
     fastest per (GPU, family, element type, log2 size) and still return the

@@ -40,6 +40,7 @@ constexpr uint32_t kStInc = 2u << 30;
 constexpr uint32_t kStMask = (1u << 30) - 1;
 constexpr long long kSpinBudget = 1ll << 31;
 constexpr int kLbBatch = 4;  // look-back statuses loaded per round trip
+constexpr uint64_t kSkipMinKeys = 1ull << 16;  // smaller sorts run every pass (no histogram read-back)
 
 template <typename K>
 __device__ __forceinline__ uint32_t digit_of(K k, int shift) {
@@ -291,25 +292,57 @@ int sort_run(K* keys, uint32_t* idx, uint64_t n, bool is_signed, void* tmp, int*
     const uint64_t per_sm = ITEMS >= 16 ? 1 : 2;  // resident blocks per SM (shared memory)
     uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
     if (grid > ntiles) grid = ntiles;
+    // A pass whose digit is the same for every key is the identity (the sort is
+    // stable): its histogram holds n in one bin.  Such passes are skipped --
+    // keys of narrower range than their type (row ids in u64, small signed
+    // values) sort in fewer passes -- unless the stream is being captured into
+    // a graph, which the histogram read-back would break.
+    bool run_pass[8];
+    int nrun = passes;
+    for (int p = 0; p < passes; ++p) run_pass[p] = true;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;
+    }
+    if (cap == cudaStreamCaptureStatusNone && n >= kSkipMinKeys) {
+        unsigned int h[8 * kRadix];
+        if (int st = d2h(h, hist, static_cast<size_t>(passes) * kRadix * 4, s)) return st;
+        if (int st = sync(s)) return st;
+        for (int p = 0; p < passes; ++p)
+            for (int d = 0; d < kRadix; ++d)
+                if (h[p * kRadix + d] == n) {
+                    run_pass[p] = false;
+                    --nrun;
+                }
+    }
     const K* kin = keys;
     const uint32_t* vin = idx;
     K* kout = ktmp;
     uint32_t* vout = vtmp;
+    int done = 0;
     for (int p = 0; p < passes; ++p) {
+        if (!run_pass[p]) continue;
         VX_CUDA(cudaMemsetAsync(status, 0, ntiles * kRadix * 4, s));
         VX_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
-        K fin = p == 0 ? flip : 0;
-        K fout = p == passes - 1 ? flip : 0;
+        // the sign flip goes on at the first pass run and off at the last
+        K fin = done == 0 ? flip : 0;
+        K fout = done == nrun - 1 ? flip : 0;
         onesweep_kernel<K, ITEMS><<<static_cast<unsigned>(grid), kRThreads, smem, s>>>(
             kin, kout, vin, vout, n, p * kRBits, fin, fout, offs + p * kRadix, status, ctr, err);
         VX_CUDA(cudaGetLastError());
-        // ping-pong; an even pass count leaves the result in the caller's buffers
+        ++done;
+        // ping-pong
         const K* nk = kout;
         const uint32_t* nv = vout;
         kout = const_cast<K*>(kin);
         vout = const_cast<uint32_t*>(vin);
         kin = nk;
         vin = nv;
+    }
+    if (done & 1) {  // an odd number of passes left the result in the scratch halves
+        VX_CUDA(cudaMemcpyAsync(keys, ktmp, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        VX_CUDA(cudaMemcpyAsync(idx, vtmp, n * 4, cudaMemcpyDeviceToDevice, s));
     }
     return kOk;
 }
