@@ -21,10 +21,13 @@
 // outputs are bit-identical for every element type.  B200 design: blocks stage a
 // tile of outputs plus its halo of w-1 inputs in shared memory with coalesced
 // loads, and each thread evaluates windows from there (O(w) shared reads per
-// output, as the definition is); the quantile keeps each thread's window sorted
-// in local memory and slides it (one removal and one insertion per output);
-// the time-bucketed sum reduces runs of equal buckets in registers and warps
-// and adds them to the output with global atomics.
+// output, as the definition is; sums and means of windows up to 16 inputs
+// evaluate 9 consecutive outputs per thread from registers); the quantile
+// keeps each thread's window sorted -- in registers up to 16 inputs, in local
+// memory above -- and slides it (one removal and one insertion per output);
+// the time-bucketed sum steps warps through 32 consecutive rows, sums runs of
+// one bucket with a segmented warp scan and adds each finished run to the
+// output once with a global atomic.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -305,79 +308,12 @@ __global__ void __launch_bounds__(kWThreads) quantile_kernel(const T* __restrict
     }
 }
 
-// out[bucket] += values[i]; *maxb = max bucket touched.  Each thread sums its
-// rows' runs of equal buckets (ts is meant to be non-decreasing, so runs are
-// long); a warp whose 32 threads all hold one run of one bucket adds it once.
-constexpr int kTRows = 16;
-
+// out[bucket] += v (integer buckets wrap like the reference's T additions)
 template <typename T>
 __device__ __forceinline__ void add_out(T* out, uint64_t b, T v) {
     if constexpr (std::is_same<T, double>::value) atomicAdd(out + b, v);
     else if constexpr (sizeof(T) == 8) atomicAdd(reinterpret_cast<unsigned long long*>(out + b), static_cast<unsigned long long>(v));
     else atomicAdd(reinterpret_cast<unsigned int*>(out + b), static_cast<unsigned int>(v));
-}
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = w_add<T>(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kWThreads) time_window_kernel(const int64_t* __restrict__ ts,
-                                                                const T* __restrict__ vals, uint64_t n,
-                                                                int64_t start, int64_t dur, uint64_t nout,
-                                                                T* __restrict__ out, unsigned long long* maxb) {
-    const uint64_t nchunks = (n + kTRows - 1) / kTRows;
-    uint64_t mymax = 0;
-    const int lane = threadIdx.x & 31;
-    const uint64_t nwarps_total = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
-    const uint64_t w0 = static_cast<uint64_t>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
-    for (uint64_t wb = w0; wb * 32 < nchunks; wb += nwarps_total) {  // warp-uniform loop
-        const uint64_t chunk = wb * 32 + lane;
-        const uint64_t r0 = chunk * kTRows;
-        int64_t cur = -1;
-        T acc = T(0);
-        bool single = true;  // this thread's rows: one valid bucket (or no rows)
-        int64_t first = -1;
-        for (int k = 0; k < kTRows; ++k) {
-            const uint64_t i = r0 + k;
-            if (i >= n) break;
-            const int64_t b = (ts[i] - start) / dur;
-            if (b < 0 || static_cast<uint64_t>(b) >= nout) {
-                single = false;
-                continue;
-            }
-            if (static_cast<uint64_t>(b) > mymax) mymax = static_cast<uint64_t>(b);
-            if (b != cur) {
-                if (cur >= 0) {
-                    add_out<T>(out, static_cast<uint64_t>(cur), acc);
-                    single = false;
-                }
-                if (first < 0) first = b;
-                cur = b;
-                acc = T(0);
-            }
-            acc = w_add<T>(acc, vals[i]);
-        }
-        // the whole warp on one bucket: one atomic
-        const int64_t b0 = __shfl_sync(0xffffffffu, cur, 0);
-        const bool same = single && cur == b0 && first == cur && cur >= 0;
-        if (__all_sync(0xffffffffu, same)) {
-            const T s = warp_sum<T>(acc);
-            if (lane == 0) add_out<T>(out, static_cast<uint64_t>(b0), s);
-        } else if (cur >= 0) {
-            add_out<T>(out, static_cast<uint64_t>(cur), acc);
-        }
-    }
-    unsigned long long m = mymax;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
-        m = y > m ? y : m;
-    }
-    if (lane == 0 && m) atomicMax(maxb, m);
 }
 
 // trunc(x / d) for d > 0 (C++ division): for |x| < 2^50 from the double
