@@ -123,17 +123,22 @@ class ClockSampler:
 
 def workload_config(d: dict, world: int) -> dict:
     """The `config` object both arms print."""
-    return {"workload": "scan+groupby 2^25 rows/GPU: key i32 zipf(1.1) over 1000, dict+bitpack 10-bit; "
+    card = d["dict"].size
+    keys = ("key i32 zipf(1.1) over 1000" if d.get("card_req", 1000) == 1000 else
+            f"key i32 over {d['card_req']} values ({card} present)")
+    return {"workload": f"scan+groupby {d['n']} rows/GPU: {keys}, dict+bitpack {d['width']}-bit; "
                         "price f64 lognormal(3,1); qty i32 U[1,100]; price>20 AND qty BETWEEN 10 AND 50; "
                         "GROUP BY key SUM(price*qty) COUNT MIN MAX",
             "rows_per_gpu": d["n"], "algorithmic_bytes_per_step": algorithmic_bytes(d),
             "l2": "inputs (444.6 MB) larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}"}
 
 
-def make_data(rank: int, rows: int) -> dict:
+def make_data(rank: int, rows: int, card: int = 1000) -> dict:
     import inputs
 
-    return inputs.config2(rows, 2001 + rank)
+    d = inputs.config2(rows, 2001 + rank) if card == 1000 else inputs.config2(rows, 2001 + rank, card=card)
+    d["card_req"] = card
+    return d
 
 
 def cpu_reference(d: dict, threads: int, reps: int, budget_s: float):
@@ -163,7 +168,7 @@ def cpu_reference(d: dict, threads: int, reps: int, budget_s: float):
 def run_reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    d = make_data(0, args.rows)
+    d = make_data(0, args.rows, getattr(args, "card", 1000))
     threads = os.cpu_count() or 1
     steps = []
     for _ in range(args.warmup):
@@ -1107,6 +1112,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="voxel", choices=["voxel", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--card", type=int, default=1000,
+                    help="groupby workload: dictionary size (1000 is the benchmark configuration; above 4096 the "
+                         "HBM group table runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="groupby", choices=["groupby", "scan", "sort", "join", "batch", "serve", "ops", "ops2"],
                     help="groupby (default): the headline fused scan + group-by; scan: fast-path filter+sum over "
@@ -1145,7 +1153,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     L = capi.lib()
-    d = make_data(rank, args.rows)
+    d = make_data(rank, args.rows, getattr(args, "card", 1000))
     dev = torch.device("cuda", local)
     t = {k: torch.from_numpy(d[k]).to(dev) for k in ("packed", "dict", "price", "qty")}
     card = d["dict"].size
@@ -1233,7 +1241,7 @@ def main() -> None:
 
     # the last timed step's groups against the reference's full-size output
     parity = None
-    want = _pinned("config2", d["n"], rank)
+    want = _pinned("config2", d["n"], rank) if d.get("card_req", 1000) == 1000 else None
     if want is not None:
         import fullsize
 
