@@ -1207,7 +1207,7 @@ def main() -> None:
     peak, peak_kind = measured_peak()
     # the committed capture is of the benchmark configuration's kernel
     default_card = d.get("card_req", 1000) == 1000
-    kernel_name = "scan_groupby_kernel" if d["dict"].size <= 4096 else "scan_groupby_global_kernel"
+    kernel_name = "scan_groupby_kernel" if d["dict"].size <= 4096 else "scan_groupby_spill_kernel"
     traffic = ncu_traffic("scan_groupby_kernel") if default_card else None
 
     # end to end through the public host entry point: pinned host buffers in,

@@ -185,9 +185,73 @@ def test_lean_word_table_extremes_and_negative_products():
         L.voxel_scan_groupby_tune(-1)
 
 
+def _exact_group_sums(idx, prod, card):
+    """Correctly rounded per-group sums (math.fsum over each group's rows)."""
+    order = np.argsort(idx, kind="stable")
+    cuts = np.searchsorted(idx[order], np.arange(card + 1))
+    vals = prod[order]
+    return np.array([math.fsum(vals[cuts[g]:cuts[g + 1]]) for g in range(card)])
+
+
+def test_spill_path_mixed_signs_and_hot_groups():
+    """Slot caches plus the HBM limb table: products of both signs over many
+    binades, a skewed key column (hot groups held in the block caches, the
+    tail spilled to HBM) and both cache sizes give the exact sums, and the
+    oracle's keys, counts, min and max."""
+    L = capi.lib()
+    rng = np.random.default_rng(61)
+    d = inputs.config2(1 << 20, 62, card=6000)
+    card = d["dict"].size
+    assert card > 4096
+    d["price"] = rng.standard_normal(d["n"]) * np.exp(rng.uniform(-25, 25, d["n"]))
+    d["qty"] = rng.integers(-100, 101, size=d["n"]).astype(np.int32)
+    w = oracle.scan_groupby_port(d["packed"], d["width"], d["dict"], d["price"], d["qty"], -np.inf, -1000, 1000)
+    prod = d["price"] * d["qty"].astype(np.float64)
+    exact = _exact_group_sums(d["idx"].astype(np.int64), prod, card)
+    exact = exact[np.bincount(d["idx"], minlength=card) > 0]
+    outs = []
+    for _ in range(2):  # the first call may time both cache sizes; the second runs the kept one
+        k, s, mn, mx, c = gpu_scan_groupby(d, -np.inf, -1000, 1000)
+        assert L.voxel_scan_groupby_last_variant() == 6
+        assert (k == w[0]).all() and (c == w[4]).all()
+        assert (mn.view(np.uint64) == w[2].view(np.uint64)).all() and (mx.view(np.uint64) == w[3].view(np.uint64)).all()
+        np.testing.assert_allclose(s, exact, rtol=1e-14, atol=1e-300)
+        outs.append(s)
+    assert (outs[0].view(np.uint64) == outs[1].view(np.uint64)).all()
+
+
+def test_spill_path_beyond_one_limb_chunk():
+    """More than 2^28 rows with a dictionary above 4,096 entries: the limbs
+    are normalised between scan chunks, and the exact sums of mixed-sign
+    half-integer products (exact in FP64, so numpy's sums are exact too),
+    counts, min and max match."""
+    L = capi.lib()
+    card = 5000
+    n = (1 << 28) + 4099
+    i = np.arange(n, dtype=np.int64)
+    idx = (i % card).astype(np.uint32)
+    price = (i % 7).astype(np.float64) + 19.5          # 19.5 fails price > 20
+    qty = ((i % 41) - 20).astype(np.int32)              # -20 fails qty >= -15
+    del i
+    from voxel_b200 import encode
+    width = encode.bit_width(idx)
+    packed = encode.bitpack(idx, width)
+    dict_ = (np.arange(card, dtype=np.int32) * 3 - 7000)
+    passing = (price > 20.0) & (qty >= -15) & (qty <= 20)
+    want_c = np.bincount(idx[passing], minlength=card).astype(np.uint64)
+    want_s = np.bincount(idx[passing], weights=(price * qty)[passing], minlength=card)
+    d = dict(n=n, dict=dict_, idx=idx, width=width, packed=packed, price=price, qty=qty)
+    k, s, mn, mx, c = gpu_scan_groupby(d, 20.0, -15, 20)
+    assert L.voxel_scan_groupby_last_variant() == 6
+    assert (k == dict_).all() and (c == want_c).all()
+    assert (s == want_s).all()
+    # every group sees every (price, qty) residue pair: min 20.5, max 25.5
+    assert (mn == 20.5).all() and (mx == 25.5).all()
+
+
 def test_large_dictionaries_against_reference():
     """Dictionaries beyond the 4,096-entry shared-memory tables (here up to
-    about a million distinct keys present) take the global-table path and
+    about a million distinct keys present) take the slot-cache + HBM path and
     give the reference HashAggregator's rows: keys, counts, min / max exact,
     sums within 1e-12."""
     if not oracle.have_ref():

@@ -188,6 +188,26 @@ __device__ __forceinline__ void words_add(uint32_t* acc, const RowWords& w, bool
     if (x2) words_ripple(acc, w.k0 + 4, step, wrap);
 }
 
+// five signed limbs (weights 2^0, 2^32, .., 2^128) -> 192-bit two's complement
+__device__ __forceinline__ Fix3 fix_from_limbs(const unsigned long long* l) {
+    Fix3 r{0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+        const uint64_t u = l[k];
+        const uint64_t e = static_cast<int64_t>(u) < 0 ? ~0ull : 0ull;  // sign extension
+        Fix3 t;
+        switch (k) {
+        case 0: t = Fix3{u, e, e}; break;
+        case 1: t = Fix3{u << 32, (u >> 32) | (e << 32), e}; break;
+        case 2: t = Fix3{0, u, e}; break;
+        case 3: t = Fix3{0, u << 32, (u >> 32) | (e << 32)}; break;
+        default: t = Fix3{0, 0, u}; break;
+        }
+        fix_add(r, t);
+    }
+    return r;
+}
+
 // 160-bit two's complement (5 words) -> 192-bit.
 __device__ __forceinline__ Fix3 fix_from_words(const uint32_t* w) {
     const uint64_t lo = w[0] | (static_cast<uint64_t>(w[1]) << 32);
@@ -231,12 +251,12 @@ __device__ __forceinline__ void scan_groupby_body(
     constexpr bool WORDS = MODE != 0;
     extern __shared__ __align__(128) unsigned char smem[];
     // MODE 0: 3 words per group (packed 192-bit sum + count), min, max.
-    // MODE 1, 2: min, max, then 5 32-bit words and a 32-bit count per group.
+    // MODE 1-3: min, max, then 5 32-bit words and a 32-bit count per group.
     unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem);
     unsigned long long* s_mn = WORDS ? s_acc : s_acc + 3 * card;
     unsigned long long* s_mx = s_mn + card;
-    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + card);  // MODE 1, 2
-    uint32_t* s_cnt = s_w + kWords * card;                      // MODE 1, 2
+    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + card);  // MODE 1-3
+    uint32_t* s_cnt = s_w + kWords * card;                      // MODE 1-3
 
     auto reset_table = [&]() {
         for (uint32_t i = threadIdx.x; i < card; i += blockDim.x) {
@@ -277,7 +297,7 @@ __device__ __forceinline__ void scan_groupby_body(
     __syncthreads();
     const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
     const uint64_t ntiles = (n + kTile - 1) / kTile;
-    // rows between flushes: MODE 0 embeds counts in 20 bits; MODES 1, 2 sum
+    // rows between flushes: MODE 0 embeds counts in 20 bits; MODES 1-3 sum
     // rows below 2^139 in 160 bits (and count in 32)
     const uint64_t tiles_per_flush = WORDS ? (1ull << 19) / kTile : ((1ull << kCountBits) - 1) / kTile;
     bool bad_value = false, bad_key = false;
@@ -462,8 +482,10 @@ __device__ __forceinline__ void scan_groupby_body(
     if (!is_last) return;
     __threadfence();
 
-    // last block: compact non-empty groups in key (= dictionary index) order
-    __shared__ unsigned int s_scan[kGbThreads];
+    // last block: compact non-empty groups in key (= dictionary index) order;
+    // the scan scratch reuses the warp queues, idle since the last consume
+    static_assert(sizeof(s_queue) >= kGbThreads * sizeof(unsigned int), "scan scratch");
+    unsigned int* const s_scan = reinterpret_cast<unsigned int*>(s_queue);
     uint32_t per = (card + blockDim.x - 1) / blockDim.x;
     uint32_t lo = threadIdx.x * per < card ? threadIdx.x * per : card;
     uint32_t hi = lo + per < card ? lo + per : card;
@@ -1206,31 +1228,166 @@ __global__ void __launch_bounds__(kGbThreads, 3) scan_groupby_lean_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Large dictionaries (more than kMaxGroups entries: the shared-memory tables
-// do not fit).  Passing rows are added straight into the global table in HBM:
-// the exact 192-bit sum with 64-bit atomics (carries from the returned old
-// values), the count, and MIN / MAX keys only when a plain read of the
-// current key shows the row can improve it.  A separate single-pass kernel
-// then compacts the non-empty groups in key order (tiles of groups claimed in
-// launch order, output offsets by decoupled look-back) and resets the table.
-// The sums are the same integers as the shared-table kernels', so the rows
-// are bit-identical to theirs.
+// Large dictionaries (more than kMaxGroups entries: a full shared-memory table
+// does not fit).  Each block keeps a shared-memory cache of 2^slots_log2 slots,
+// each a 32-bit word accumulator as in MODE 1 tagged with the group it holds.
+// A group takes the first free slot of its probe sequence the first time one
+// of its rows reaches the block and keeps it until the block flushes, so the
+// frequent groups of a skewed column settle in every block's cache.  Rows whose
+// group finds no slot go to the HBM table: per group five signed 64-bit limbs
+// (limb k weighs 2^(32k) units of 2^-76), the count and the MIN / MAX order
+// keys.  Every addition to the HBM table is a reduction whose result is never
+// read (no carry crosses a limb; each added piece is below 2^32), so no thread
+// waits on an HBM atomic.  A scan kernel covers at most kSpillChunk rows; the
+// limbs are normalised between chunks, which keeps each below 2^61.  A
+// separate kernel then compacts the non-empty groups in key order (tiles of
+// groups claimed in launch order, output offsets by decoupled look-back) and
+// resets the table.  The sums are the same integers as the shared-table
+// kernels', so the rows are bit-identical to theirs.
 // ---------------------------------------------------------------------------
-template <int RPT>
-__global__ void __launch_bounds__(kGbThreads) scan_groupby_global_kernel(
+constexpr int kLimbWords = 8;  // per group in HBM: limbs 0-4, count, min key, max key
+constexpr uint32_t kSlotEmpty = 0xFFFFFFFFu;
+constexpr int kSlotProbes = 4;
+constexpr uint64_t kSpillChunk = 1ull << 28;
+constexpr int kSpillMaxLog2 = 11;
+
+// shared memory of the slot cache: min, max keys, five words, count, tag per slot
+size_t spill_smem_bytes(int slots_log2) { return (static_cast<size_t>(1) << slots_log2) * 44; }
+
+template <int RPT, int MINB>
+__global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
     const uint64_t* __restrict__ packed, uint32_t width, uint32_t card, const double* __restrict__ price,
-    const int32_t* __restrict__ qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi, GlobalGroups g, int* status) {
-    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * RPT;
+    const int32_t* __restrict__ qty, uint64_t row0, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+    unsigned long long* __restrict__ hbm, int slots_log2, int* status) {
+    constexpr int kTile = kGbThreads * RPT;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const uint32_t nslots = 1u << slots_log2;
+    unsigned long long* s_mn = reinterpret_cast<unsigned long long*>(smem);
+    unsigned long long* s_mx = s_mn + nslots;
+    uint32_t* s_w = reinterpret_cast<uint32_t*>(s_mx + nslots);
+    uint32_t* s_cnt = s_w + kWords * nslots;
+    uint32_t* s_tag = s_cnt + nslots;
+    auto reset_slots = [&]() {
+        for (uint32_t i = threadIdx.x; i < nslots; i += blockDim.x) {
+#pragma unroll
+            for (int k = 0; k < kWords; ++k) s_w[kWords * i + k] = 0;
+            s_cnt[i] = 0;
+            s_mn[i] = ~0ull;
+            s_mx[i] = 0;
+            s_tag[i] = kSlotEmpty;
+        }
+    };
+    // slot -> HBM: words 0-3 as unsigned pieces, word 4 sign-extended (the
+    // 160-bit two's complement value), all as reductions
+    auto flush_slots = [&]() {
+        for (uint32_t i = threadIdx.x; i < nslots; i += blockDim.x) {
+            const uint32_t tag = s_tag[i], c = s_cnt[i];
+            if (tag == kSlotEmpty || !c) continue;
+            unsigned long long* e = hbm + static_cast<uint64_t>(kLimbWords) * tag;
+#pragma unroll
+            for (int k = 0; k < kWords - 1; ++k)
+                if (const uint32_t w = s_w[kWords * i + k]) atomicAdd(&e[k], static_cast<unsigned long long>(w));
+            if (const uint32_t w = s_w[kWords * i + kWords - 1])
+                atomicAdd(&e[kWords - 1], static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(w))));
+            atomicAdd(&e[5], static_cast<unsigned long long>(c));
+            atomicMin(&e[6], s_mn[i]);
+            atomicMax(&e[7], s_mx[i]);
+        }
+    };
+    reset_slots();
+    __syncthreads();
+
     const uint64_t mask = (width >= 64) ? ~0ull : ((1ull << width) - 1);
     const uint32_t qspan = qlo <= qhi ? static_cast<uint32_t>(qhi) - static_cast<uint32_t>(qlo) : 0u;
     const double pcut = qlo <= qhi ? pthr : __longlong_as_double(0x7FF0000000000000ll);
-    bool bad_value = false, bad_key = false;
     const uint64_t ntiles = (n + kTile - 1) / kTile;
+    const uint64_t tiles_per_flush = (1ull << 19) / kTile;  // 32-bit slot counts, 160-bit slot sums
+    bool bad_value = false, bad_key = false;
+    uint64_t since_flush = 0;
+
+    __shared__ WarpQueue<false> s_queue[kGbThreads / 32];
+    const int lane = threadIdx.x & 31;
+    const unsigned lanemask_lt = (1u << lane) - 1;
+    WarpQueue<false>& Q = s_queue[threadIdx.x >> 5];
+    int qn = 0, qh = 0;
+    volatile uint32_t* const v_tag = s_tag;
+
+    auto consume = [&](int cnt) {
+        const bool valid = lane < cnt;
+        const int e = (qh + lane) & (kQueue - 1);
+        const double p = valid ? Q.price[e] : 0.0;
+        const double v = valid ? __dmul_rn(p, static_cast<double>(Q.qty[e])) : 0.0;  // one rounded multiply
+        // one warp-uniform test picks the add-only path of the slot words
+        const bool mayneg = __any_sync(0xffffffffu, v < 0.0);
+        if (!valid) return;
+        const uint32_t gi = key_bits(packed, Q.pos[e], width, mask);
+        if (gi >= card) {
+            bad_key = true;
+            return;
+        }
+        RowWords w;
+        const bool ok = row_words(v, &w);
+        if (!ok) bad_value = true;
+        const bool neg = v < 0.0;
+        const unsigned long long key = f64_order_key(p);
+        // a slot is written once (empty -> tag) between flushes, so the first
+        // slot of the probe sequence that holds gi or is won for it is gi's own
+        uint32_t h = (gi * 0x9E3779B1u) >> (32 - slots_log2);
+        int slot = -1;
+#pragma unroll
+        for (int pr = 0; pr < kSlotProbes; ++pr) {
+            uint32_t t = v_tag[h];
+            if (t == kSlotEmpty) {
+                t = atomicCAS(&s_tag[h], kSlotEmpty, gi);
+                if (t == kSlotEmpty) t = gi;
+            }
+            if (t == gi) {
+                slot = static_cast<int>(h);
+                break;
+            }
+            h = (h + 1) & (nslots - 1);
+        }
+        if (slot >= 0) {
+            if (ok && mayneg) words_add<true>(s_w + kWords * slot, w, neg);
+            else if (ok) words_add<false>(s_w + kWords * slot, w, false);
+            atomicAdd(&s_cnt[slot], 1u);
+            if (key < s_mn[slot]) atomicMin(&s_mn[slot], key);
+            if (key > s_mx[slot]) atomicMax(&s_mx[slot], key);
+            return;
+        }
+        unsigned long long* eb = hbm + static_cast<uint64_t>(kLimbWords) * gi;
+        if (ok) {
+            const unsigned long long a0 = w.c0, a1 = w.c1, a2 = w.c2;
+            if (a0) atomicAdd(&eb[w.k0], neg ? 0ull - a0 : a0);
+            if (a1) atomicAdd(&eb[w.k0 + 1], neg ? 0ull - a1 : a1);
+            if (a2) atomicAdd(&eb[w.k0 + 2], neg ? 0ull - a2 : a2);
+        }
+        atomicAdd(&eb[5], 1ull);
+        // screen MIN / MAX with one read of both keys: a stale read only costs
+        // an atomic that changes nothing
+        const ulonglong2 mm = __ldcg(reinterpret_cast<const ulonglong2*>(eb + 6));
+        if (key < mm.x) atomicMin(&eb[6], key);
+        if (key > mm.y) atomicMax(&eb[7], key);
+    };
+
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const uint64_t r0 = t * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
+        if (since_flush == tiles_per_flush) {
+            __syncwarp();
+            consume(qn);
+            qn = 0;
+            __syncthreads();
+            flush_slots();
+            __syncthreads();
+            reset_slots();
+            __syncthreads();
+            since_flush = 0;
+        }
+        ++since_flush;
+        const uint64_t r0 = row0 + t * kTile + static_cast<uint64_t>(threadIdx.x) * RPT;
+        const uint64_t rend = row0 + n;
         double pv[RPT];
         int32_t qv[RPT];
-        if (r0 + RPT <= n) {
+        if (r0 + RPT <= rend) {
 #pragma unroll
             for (int k = 0; k < RPT; k += 4) {
                 const double2* pp = reinterpret_cast<const double2*>(price + r0 + k);
@@ -1242,7 +1399,7 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_global_kernel(
         } else {
 #pragma unroll
             for (int k = 0; k < RPT; ++k) {
-                const bool in = r0 + k < n;
+                const bool in = r0 + k < rend;
                 pv[k] = in ? price[r0 + k] : __longlong_as_double(0x7FF8000000000000ll);  // NaN never passes
                 qv[k] = in ? qty[r0 + k] : 0;
             }
@@ -1250,30 +1407,55 @@ __global__ void __launch_bounds__(kGbThreads) scan_groupby_global_kernel(
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
             const double p = pv[k];
-            if (!(p > pcut && static_cast<uint32_t>(qv[k]) - static_cast<uint32_t>(qlo) <= qspan)) continue;
-            const uint32_t gi = key_bits(packed, r0 + k, width, mask);
-            if (gi >= card) {
-                bad_key = true;
-                continue;
+            const int32_t q = qv[k];
+            const bool pass = p > pcut && static_cast<uint32_t>(q) - static_cast<uint32_t>(qlo) <= qspan;
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) {
+                const int pos = (qh + qn + __popc(m & lanemask_lt)) & (kQueue - 1);
+                Q.pos[pos] = r0 + k;
+                Q.price[pos] = p;
+                Q.qty[pos] = q;
             }
-            const double v = __dmul_rn(p, static_cast<double>(qv[k]));  // one rounded multiply
-            const Fix3 f = fix_from_double_s<kFixScale>(v, &bad_value);
-            fix_atomic_add(&g.sum[3 * static_cast<uint64_t>(gi)], f);
-            atomicAdd(&g.cnt[gi], 1ull);
-            const uint64_t key = f64_order_key(p);
-            if (key < __ldcg(&g.mn[gi])) atomicMin(&g.mn[gi], static_cast<unsigned long long>(key));
-            if (key > __ldcg(&g.mx[gi])) atomicMax(&g.mx[gi], static_cast<unsigned long long>(key));
+            qn += __popc(m);
+            if (qn >= 32) {
+                __syncwarp();
+                consume(32);
+                __syncwarp();  // the consumed entries are free for the next pushes
+                qh = (qh + 32) & (kQueue - 1);
+                qn -= 32;
+            }
         }
     }
+    __syncwarp();
+    consume(qn);
     if (bad_value) atomicOr(status, 1);
     if (bad_key) atomicOr(status, 2);
+    __syncthreads();
+    flush_slots();
 }
 
-constexpr int kFinPer = 8;                        // groups per thread
+// carries of limbs 0-3 into the next limb: afterwards limbs 0-3 lie in
+// [0, 2^32) and limb 4 holds the signed rest (between scan chunks)
+__global__ void normalize_limbs_kernel(unsigned long long* hbm, uint32_t card) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < card;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        unsigned long long* e = hbm + kLimbWords * i;
+        long long c = 0;
+#pragma unroll
+        for (int k = 0; k < kWords - 1; ++k) {
+            const long long v = static_cast<long long>(e[k]) + c;
+            e[k] = static_cast<unsigned long long>(v) & 0xFFFFFFFFull;
+            c = v >> 32;  // arithmetic: v = c * 2^32 + low word
+        }
+        e[kWords - 1] = static_cast<unsigned long long>(static_cast<long long>(e[kWords - 1]) + c);
+    }
+}
+
+constexpr int kFinPer = 2;                        // groups per thread
 constexpr int kFinTile = kGbThreads * kFinPer;     // groups per tile
 
 __global__ void __launch_bounds__(kGbThreads) groupby_finalize_kernel(
-    GlobalGroups g, const int32_t* __restrict__ dict, uint32_t card, int32_t* out_keys, double* out_sum,
+    unsigned long long* hbm, const int32_t* __restrict__ dict, uint32_t card, int32_t* out_keys, double* out_sum,
     double* out_min, double* out_max, uint64_t* out_count, uint64_t* out_ngroups, unsigned long long* lb,
     unsigned int* ctr, int* err) {
     __shared__ uint64_t s_tile, s_base;
@@ -1290,7 +1472,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_finalize_kernel(
 #pragma unroll
         for (int k = 0; k < kFinPer; ++k) {
             const uint64_t i = i0 + k;
-            if (i < card && __ldcg(&g.cnt[i])) live |= 1u << k;
+            if (i < card && __ldcg(&hbm[kLimbWords * i + 5])) live |= 1u << k;
         }
         const uint64_t c = __popc(live);
         uint64_t inc = c;
@@ -1323,21 +1505,22 @@ __global__ void __launch_bounds__(kGbThreads) groupby_finalize_kernel(
         for (int k = 0; k < kFinPer; ++k) {
             const uint64_t i = i0 + k;
             if (i >= card) break;
+            unsigned long long* e = hbm + kLimbWords * i;
             if (live >> k & 1u) {
-                const Fix3 f{__ldcg(&g.sum[3 * i]), __ldcg(&g.sum[3 * i + 1]), __ldcg(&g.sum[3 * i + 2])};
+                unsigned long long l[kWords];
+#pragma unroll
+                for (int j = 0; j < kWords; ++j) l[j] = __ldcg(&e[j]);
                 out_keys[pos] = dict[i];
-                out_sum[pos] = fix_to_double_s<kFixScale>(f);
-                out_min[pos] = f64_from_order_key(__ldcg(&g.mn[i]));
-                out_max[pos] = f64_from_order_key(__ldcg(&g.mx[i]));
-                out_count[pos] = __ldcg(&g.cnt[i]);
+                out_sum[pos] = fix_to_double_s<kFixScale>(fix_from_limbs(l));
+                out_min[pos] = f64_from_order_key(__ldcg(&e[6]));
+                out_max[pos] = f64_from_order_key(__ldcg(&e[7]));
+                out_count[pos] = __ldcg(&e[5]);
                 ++pos;
             }
-            g.sum[3 * i] = 0;
-            g.sum[3 * i + 1] = 0;
-            g.sum[3 * i + 2] = 0;
-            g.cnt[i] = 0;
-            g.mn[i] = ~0ull;
-            g.mx[i] = 0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) e[j] = 0;
+            e[6] = ~0ull;
+            e[7] = 0;
         }
         __syncthreads();
     }
@@ -1355,7 +1538,23 @@ __global__ void init_groups_kernel(GlobalGroups g, uint32_t card, unsigned int* 
     if (blockIdx.x == 0 && threadIdx.x == 0) *done = 0;
 }
 
-size_t table_bytes(uint32_t card) { return static_cast<size_t>(card) * 6 * 8 + 256; }
+__global__ void init_limbs_kernel(unsigned long long* hbm, uint32_t card, unsigned int* done) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < card;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        unsigned long long* e = hbm + kLimbWords * i;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) e[j] = 0;
+        e[6] = ~0ull;
+        e[7] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *done = 0;
+}
+
+// shared-table dictionaries: sums (3 words), count, min, max per group; larger
+// ones: the eight-word limb layout
+size_t table_bytes(uint32_t card) {
+    return static_cast<size_t>(card) * (card > kMaxGroups ? kLimbWords : 6) * 8 + 256;
+}
 
 size_t tma_smem_bytes(uint32_t card, uint32_t width) {
     return kTmaStages * (24576u + 256u * width) + static_cast<size_t>(kTmaConsumers) * card * 16 +
@@ -1525,20 +1724,44 @@ int launch_lean(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const in
     return kOk;
 }
 
-int launch_global(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
-                  const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
-                  int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
-    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * 4;
+int launch_spill(ScanGroupBy& S, int slots_log2, const uint64_t* packed, uint32_t width, const int32_t* dict,
+                 uint32_t card, const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo,
+                 int32_t qhi, int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong,
+                 cudaStream_t s) {
+    constexpr int kRpt = 4;
+    constexpr uint64_t kTile = static_cast<uint64_t>(kGbThreads) * kRpt;
     const int sms = sm_count() > 0 ? sm_count() : 148;
-    const uint64_t ntiles = (n + kTile - 1) / kTile;
-    uint64_t grid = static_cast<uint64_t>(sms) * 4;
-    if (grid > ntiles) grid = ntiles;
-    if (grid < 1) grid = 1;
-    GlobalGroups g{S.g_sum, S.g_cnt, S.g_mn, S.g_mx};
-    if (n)
-        scan_groupby_global_kernel<4><<<static_cast<unsigned>(grid), kGbThreads, 0, s>>>(
-            packed, width, card, price, qty, n, pthr, qlo, qhi, g, static_cast<int*>(S.status.p));
-    VX_CUDA(cudaGetLastError());
+    unsigned long long* const hbm = S.g_limb;
+    int* const status = static_cast<int*>(S.status.p);
+    const size_t smem = spill_smem_bytes(slots_log2);
+    // the smaller cache leaves room for a third block per SM: registers capped to match
+    auto* const kern =
+        slots_log2 < kSpillMaxLog2 ? scan_groupby_spill_kernel<kRpt, 3> : scan_groupby_spill_kernel<kRpt, 2>;
+    static thread_local bool attr_set = false;
+    if (!attr_set) {
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(spill_smem_bytes(kSpillMaxLog2))));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(spill_smem_bytes(kSpillMaxLog2))));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    VX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGbThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = 1;
+    for (uint64_t off = 0; off < n; off += kSpillChunk) {
+        const uint64_t m = n - off < kSpillChunk ? n - off : kSpillChunk;
+        if (off) {  // carries out of the limbs before the next chunk adds to them
+            normalize_limbs_kernel<<<static_cast<unsigned>(sms) * 4, 256, 0, s>>>(hbm, card);
+            VX_CUDA(cudaGetLastError());
+        }
+        const uint64_t ntiles = (m + kTile - 1) / kTile;
+        grid = static_cast<uint64_t>(sms) * per_sm;
+        if (grid > ntiles) grid = ntiles;
+        kern<<<static_cast<unsigned>(grid), kGbThreads, smem, s>>>(
+            packed, width, card, price, qty, off, m, pthr, qlo, qhi, hbm, slots_log2, status);
+        VX_CUDA(cudaGetLastError());
+    }
     const uint64_t ftiles = (card + kFinTile - 1) / kFinTile;
     const size_t lb_bytes = (ftiles + 1) * 8 + 64;
     if (S.lookback.n < lb_bytes) {
@@ -1551,12 +1774,31 @@ int launch_global(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const 
     uint64_t fgrid = static_cast<uint64_t>(sms) * 4;
     if (fgrid > ftiles) fgrid = ftiles;
     // the status word's bit 4 is the look-back timeout, reported like the bulk-copy waits
-    groupby_finalize_kernel<<<static_cast<unsigned>(fgrid), kGbThreads, 0, s>>>(
-        g, dict, card, ok, os, omn, omx, oc, ong, lb, ctr, static_cast<int*>(S.status.p));
+    groupby_finalize_kernel<<<static_cast<unsigned>(fgrid), kGbThreads, 0, s>>>(hbm, dict, card, ok, os, omn, omx,
+                                                                                oc, ong, lb, ctr, status);
     VX_CUDA(cudaGetLastError());
     S.last_grid = static_cast<int>(grid);
     S.last_kernel = 6;
     return kOk;
+}
+
+// the slot-cache size: 2048 slots (two blocks per SM) or 1024 (three), timed
+// per (dictionary size, rows) when tuning is on
+int launch_global(ScanGroupBy& S, const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card,
+                  const double* price, const int32_t* qty, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
+                  int32_t* ok, double* os, double* omn, double* omx, uint64_t* oc, uint64_t* ong, cudaStream_t s) {
+    auto variant = [&](int c) -> int {
+        return launch_spill(S, c == 1 ? kSpillMaxLog2 - 1 : kSpillMaxLog2, packed, width, dict, card, price, qty, n,
+                            pthr, qlo, qhi, ok, os, omn, omx, oc, ong, s);
+    };
+    if (!S.autotune || n < (1u << 16)) return variant(0);
+    int cl = 0;
+    while (cl < 31 && (2u << cl) <= card) ++cl;
+    const std::string family = "scan_groupby_spill_card" + std::to_string(cl);
+    const std::string key = tune_key(family.c_str(), F64, n);
+    int c = 0;
+    if (!tune_lookup(key, &c)) c = tune_pick(key, 2, 0, s, variant);
+    return variant(c);
 }
 
 }  // namespace
@@ -1574,13 +1816,21 @@ int ScanGroupBy::prepare(uint32_t card, cudaStream_t s) {
         if (!table.p || !status.p) return kErrOutOfMemory;
         card_ = card;
         char* b = static_cast<char*>(table.p);
-        g_sum = reinterpret_cast<unsigned long long*>(b);
-        g_cnt = g_sum + 3 * card;
-        g_mn = g_cnt + card;
-        g_mx = g_mn + card;
-        g_done = reinterpret_cast<unsigned int*>(g_mx + card);
-        GlobalGroups g{g_sum, g_cnt, g_mn, g_mx};
-        init_groups_kernel<<<(card + 255) / 256, 256, 0, s>>>(g, card, g_done);
+        if (card > kMaxGroups) {  // the HBM table of the slot-cache kernels: eight words per group
+            g_limb = reinterpret_cast<unsigned long long*>(b);
+            g_sum = g_cnt = g_mn = g_mx = nullptr;
+            g_done = reinterpret_cast<unsigned int*>(g_limb + static_cast<size_t>(kLimbWords) * card);
+            init_limbs_kernel<<<(card + 255) / 256, 256, 0, s>>>(g_limb, card, g_done);
+        } else {
+            g_limb = nullptr;
+            g_sum = reinterpret_cast<unsigned long long*>(b);
+            g_cnt = g_sum + 3 * card;
+            g_mn = g_cnt + card;
+            g_mx = g_mn + card;
+            g_done = reinterpret_cast<unsigned int*>(g_mx + card);
+            GlobalGroups g{g_sum, g_cnt, g_mn, g_mx};
+            init_groups_kernel<<<(card + 255) / 256, 256, 0, s>>>(g, card, g_done);
+        }
         VX_CUDA(cudaGetLastError());
         VX_CUDA(cudaMemsetAsync(status.p, 0, 16, s));
     }

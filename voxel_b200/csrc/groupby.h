@@ -20,6 +20,7 @@ struct ScanGroupBy {
     DevBuf table, status, lookback;
     uint32_t card_ = 0;
     unsigned long long *g_sum = nullptr, *g_cnt = nullptr, *g_mn = nullptr, *g_mx = nullptr;
+    unsigned long long* g_limb = nullptr;  // dictionaries above kMaxGroups: limbs 0-4, count, min, max per group
     unsigned int* g_done = nullptr;
     int rows_per_thread = 4;  // rows per thread of the shared-table variants: 4, 8 (16: merged only)
     bool use_tma = false;     // TMA-fed private-table variant when the dictionary fits
@@ -30,7 +31,8 @@ struct ScanGroupBy {
     int last_grid = 0;
     int last_kernel = 0;      // 0: merged 192-bit atomics, 1: TMA-fed, 2: word table + queue, 3: word table direct,
                               // 4: bulk-copy-fed word table, 5: lean word table,
-                              // 6: global table (dictionaries above kMaxGroups)
+                              // 6: slot caches spilling to the HBM table (dictionaries above kMaxGroups),
+                              // 7: word table with next-tile prefetch
 
     int prepare(uint32_t card, cudaStream_t s);
     int launch(const uint64_t* packed, uint32_t width, const int32_t* dict, uint32_t card, const double* price,
