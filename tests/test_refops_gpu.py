@@ -1,6 +1,8 @@
 """The remaining reference C ABI operators on the GPU: HashAggregator object,
 one-shot and sort-based group-by, SortOperator index sorts, TopK and the f64
 dictionary, each against the reference's known answers and the oracle."""
+import math
+
 import numpy as np
 import pytest
 
@@ -78,6 +80,35 @@ def test_groupby_high_cardinality():
     assert got == ng and (ok == want[0]).all() and (c == want[4]).all()
     assert (mn == want[2]).all() and (mx == want[3]).all()
     np.testing.assert_allclose(s, want[1], rtol=1e-12, atol=0)
+
+
+def test_groupby_large_table_mixed_signs_exact():
+    """Tables above 2,048 slots accumulate with 192-bit global atomics whose
+    returned old values carry into the next word: values of both signs over
+    many binades give the correctly rounded group sums, and the oracle's
+    keys, counts, min and max, whether the table grew from a small size hint
+    or was sized up front."""
+    L = capi.lib()
+    rng = np.random.default_rng(34)
+    n, card = 1_500_000, 200_000
+    keys = (rng.integers(0, card, n) * 7 - 700_000).astype(np.int32)
+    vals = rng.standard_normal(n) * np.exp(rng.uniform(-20, 20, n))
+    want = oracle.groupby_port(keys, vals)
+    ng = want[0].size
+    order = np.argsort(keys, kind="stable")
+    cuts = np.searchsorted(keys[order], want[0], side="left").tolist() + [n]
+    sv = vals[order]
+    exact = np.array([math.fsum(sv[cuts[g]:cuts[g + 1]]) for g in range(ng)])
+    for hint in (16, card):  # grown from a small table, and sized up front
+        ok = np.zeros(ng, np.int32)
+        s, mn, mx = (np.zeros(ng) for _ in range(3))
+        c = np.zeros(ng, np.uint64)
+        got = L.voxel_groupby_i32_f64(keys.ctypes.data, vals.ctypes.data, n, hint, ok.ctypes.data, s.ctypes.data,
+                                      mn.ctypes.data, mx.ctypes.data, c.ctypes.data)
+        assert got == ng, capi.last_error()
+        assert (ok == want[0]).all() and (c == want[4]).all()
+        assert (mn == want[2]).all() and (mx == want[3]).all()
+        np.testing.assert_allclose(s, exact, rtol=1e-14, atol=1e-300)
 
 
 def test_sort_and_topk(golden):
