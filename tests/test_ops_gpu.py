@@ -333,6 +333,41 @@ def test_hashjoin_golden_and_properties(golden):
     assert m == wm == 100 and (l == wl).all() and (r == wr).all()
 
 
+def test_bitmap_and_many_bitmaps():
+    """AND of 1 to 70 bitmaps: pointer lists passed by value (up to 16), held
+    in shared memory (up to 64) and read from the device table beyond, on the
+    host and device entry points, against the oracle."""
+    import ctypes
+
+    import torch
+
+    L = capi.lib()
+    rng = np.random.default_rng(23)
+    n = 100_003
+    words = (n + 63) // 64
+    dev = torch.device("cuda", 0)
+    for nbm in (1, 5, 16, 17, 64, 70):
+        bms = []
+        for _ in range(nbm):
+            bits = rng.random(n) < 0.985
+            raw = np.packbits(bits, bitorder="little")
+            raw = np.concatenate([raw, np.zeros(words * 8 - raw.size, np.uint8)])
+            bms.append(raw.view(np.uint64).copy())
+        hp = (ctypes.c_void_p * nbm)(*[b.ctypes.data for b in bms])
+        out = np.zeros(words, np.uint64)
+        c = L.voxel_bitmap_and(hp, nbm, n, out.ctypes.data)
+        want = np.zeros(words, np.uint64)
+        wc = oracle.port().vo_bitmap_and(hp, nbm, n, want.ctypes.data)
+        assert c == wc and (out == want).all(), nbm
+        dts = [torch.from_numpy(b.view(np.int64)).to(dev) for b in bms]
+        dp = (ctypes.c_void_p * nbm)(*[t.data_ptr() for t in dts])
+        dout = torch.zeros(words, dtype=torch.int64, device=dev)
+        dcnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        assert L.voxel_bitmap_and_dev(ctypes.addressof(dp), nbm, n, dout.data_ptr(), dcnt.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        assert int(dcnt.item()) == wc and (dout.cpu().numpy().view(np.uint64) == want).all(), nbm
+
+
 def test_device_entry_points_equal_host_ones():
     """The device-pointer variants (bitmap AND, dictionary decoders) give the
     host entry points' results; an index outside the dictionary is an error."""

@@ -81,11 +81,22 @@ __global__ void __launch_bounds__(kFThreads) vfilter_kernel(const T* __restrict_
 
 constexpr int kAndMax = 64;  // bitmaps whose pointers are held in shared memory
 
-__global__ void bitmap_and_kernel(const uint64_t* const* bms, int nbm, uint64_t rows, uint64_t* out,
+// inl.p[k] by a chain of selects over the parameter words (an indexed read
+// would copy the whole list to local memory first)
+__device__ __forceinline__ const uint64_t* list_at(const BitmapList& inl, int k) {
+    const uint64_t* r = nullptr;
+#pragma unroll
+    for (int j = 0; j < kAndInline; ++j) r = j == k ? inl.p[j] : r;
+    return r;
+}
+
+// bms: a device array of nbm bitmap pointers, or null with the pointers passed
+// by value in inl (nbm <= kAndInline: no pointer table to upload first)
+__global__ void bitmap_and_kernel(BitmapList inl, const uint64_t* const* bms, int nbm, uint64_t rows, uint64_t* out,
                                   unsigned long long* count) {
     __shared__ const uint64_t* s_bm[kAndMax];
     const int nsm = nbm < kAndMax ? nbm : kAndMax;
-    for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_bm[k] = bms[k];
+    for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_bm[k] = bms ? bms[k] : list_at(inl, k);
     __syncthreads();
     const uint64_t nwords = (rows + 63) / 64;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -294,17 +305,30 @@ int launch_selection(const uint64_t* bm, uint64_t rows, uint32_t* out, unsigned 
     return selection_pass(bm, rows, out, count, scratch, err, s, kPerSm[c]);
 }
 
-int launch_bitmap_and(const uint64_t* const* d_bms, int nbm, uint64_t rows, uint64_t* out, unsigned long long* count,
-                      cudaStream_t s) {
+int launch_bitmap_and_from(const BitmapList& inl, const uint64_t* const* d_bms, int nbm, uint64_t rows,
+                           uint64_t* out, unsigned long long* count, cudaStream_t s) {
     VX_CUDA(cudaMemsetAsync(count, 0, 8, s));
     uint64_t words = (rows + 63) / 64;
     if (!words) return kOk;
     int sms = sm_count() > 0 ? sm_count() : 148;
     uint64_t blocks = (words + 255) / 256;
     if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
-    bitmap_and_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(d_bms, nbm, rows, out, count);
+    bitmap_and_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(inl, d_bms, nbm, rows, out, count);
     VX_CUDA(cudaGetLastError());
     return kOk;
+}
+
+int launch_bitmap_and(const uint64_t* const* d_bms, int nbm, uint64_t rows, uint64_t* out, unsigned long long* count,
+                      cudaStream_t s) {
+    return launch_bitmap_and_from(BitmapList{}, d_bms, nbm, rows, out, count, s);
+}
+
+// host array of device bitmap pointers: passed by value when they fit
+int launch_bitmap_and_host_list(const uint64_t* const* h_bms, int nbm, uint64_t rows, uint64_t* out,
+                                unsigned long long* count, cudaStream_t s) {
+    BitmapList inl{};
+    for (int k = 0; k < nbm; ++k) inl.p[k] = h_bms[k];
+    return launch_bitmap_and_from(inl, nullptr, nbm, rows, out, count, s);
 }
 
 }  // namespace vx
@@ -409,6 +433,9 @@ int voxel_bitmap_and_dev(const uint64_t* const* d_bitmaps, size_t nbm, size_t ro
     clear_error();
     if (int st = ensure_device()) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
+    if (nbm <= static_cast<size_t>(kAndInline))
+        return launch_bitmap_and_host_list(d_bitmaps, static_cast<int>(nbm), rows, d_out,
+                                           reinterpret_cast<unsigned long long*>(d_count), s);
     static thread_local DevBuf table;  // the device copy of the pointer table
     if (table.n < nbm * sizeof(void*) + 8) {
         table = DevBuf(nbm * sizeof(void*) + 8);
@@ -435,10 +462,16 @@ size_t voxel_bitmap_and(const uint64_t* const* bitmaps, size_t nbm, size_t rows,
     }
     DevBuf dptrs(nbm * sizeof(void*) + 8), o(words * 8), c(8);
     if (!dptrs.p || !o.ok(words * 8) || !c.p) return static_cast<size_t>(-1);
-    if (nbm && h2d(dptrs.p, ptrs.data(), nbm * sizeof(void*), s)) return static_cast<size_t>(-1);
-    if (launch_bitmap_and(static_cast<const uint64_t* const*>(dptrs.p), static_cast<int>(nbm), rows, o.as<uint64_t>(),
-                          c.as<unsigned long long>(), s))
-        return static_cast<size_t>(-1);
+    if (nbm <= static_cast<size_t>(kAndInline)) {
+        if (launch_bitmap_and_host_list(ptrs.data(), static_cast<int>(nbm), rows, o.as<uint64_t>(),
+                                        c.as<unsigned long long>(), s))
+            return static_cast<size_t>(-1);
+    } else {
+        if (h2d(dptrs.p, ptrs.data(), nbm * sizeof(void*), s)) return static_cast<size_t>(-1);
+        if (launch_bitmap_and(static_cast<const uint64_t* const*>(dptrs.p), static_cast<int>(nbm), rows,
+                              o.as<uint64_t>(), c.as<unsigned long long>(), s))
+            return static_cast<size_t>(-1);
+    }
     uint64_t cnt = 0;
     if (d2h(out, o.p, words * 8, s) || d2h(&cnt, c.p, 8, s) || sync(s)) return static_cast<size_t>(-1);
     return cnt;

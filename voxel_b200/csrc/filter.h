@@ -19,5 +19,13 @@ int launch_selection(const uint64_t* bitmap, uint64_t rows, uint32_t* out, unsig
                      int* err, cudaStream_t s);
 int launch_bitmap_and(const uint64_t* const* d_bitmaps, int nbm, uint64_t rows, uint64_t* out,
                       unsigned long long* count, cudaStream_t s);
+// up to kAndInline bitmaps whose device pointers sit in a host array: passed
+// to the kernel by value (no pointer table is uploaded)
+constexpr int kAndInline = 16;
+struct BitmapList {
+    const uint64_t* p[kAndInline];
+};
+int launch_bitmap_and_host_list(const uint64_t* const* h_bitmaps, int nbm, uint64_t rows, uint64_t* out,
+                                unsigned long long* count, cudaStream_t s);
 
 }  // namespace vx
