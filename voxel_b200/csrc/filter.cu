@@ -94,6 +94,8 @@ __device__ __forceinline__ const uint64_t* list_at(const BitmapList& inl, int k)
 // by value in inl (nbm <= kAndInline: no pointer table to upload first)
 __global__ void bitmap_and_kernel(BitmapList inl, const uint64_t* const* bms, int nbm, uint64_t rows, uint64_t* out,
                                   unsigned long long* count) {
+    constexpr int kU = 4;   // words per thread per step
+    constexpr int kB = 4;   // bitmaps whose loads are issued together
     __shared__ const uint64_t* s_bm[kAndMax];
     const int nsm = nbm < kAndMax ? nbm : kAndMax;
     for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_bm[k] = bms ? bms[k] : list_at(inl, k);
@@ -101,22 +103,34 @@ __global__ void bitmap_and_kernel(BitmapList inl, const uint64_t* const* bms, in
     const uint64_t nwords = (rows + 63) / 64;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     unsigned int cnt = 0;
-    for (uint64_t w0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w0 < nwords; w0 += 2 * stride) {
-        uint64_t x[2];
+    for (uint64_t w0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w0 < nwords; w0 += kU * stride) {
+        uint64_t x[kU];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kU; ++u) {
             const uint64_t w = w0 + u * stride;
             x[u] = ~0ull;
             if (w == nwords - 1 && (rows & 63)) x[u] = (1ull << (rows & 63)) - 1;
         }
-        for (int k = 0; k < nbm; ++k) {
-            const uint64_t* b = k < kAndMax ? s_bm[k] : bms[k];
+        // kB bitmaps x kU words of loads in flight before any of them is used
+        for (int k = 0; k < nbm; k += kB) {
+            uint64_t v[kB][kU];
 #pragma unroll
-            for (int u = 0; u < 2; ++u)
-                if (w0 + u * stride < nwords) x[u] &= __ldcs(b + w0 + u * stride);
+            for (int j = 0; j < kB; ++j) {
+                const int kk = k + j;
+                const uint64_t* b = kk < nbm ? (kk < kAndMax ? s_bm[kk] : bms[kk]) : nullptr;
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const uint64_t w = w0 + u * stride;
+                    v[j][u] = b && w < nwords ? __ldcs(b + w) : ~0ull;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kB; ++j)
+#pragma unroll
+                for (int u = 0; u < kU; ++u) x[u] &= v[j][u];
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kU; ++u) {
             const uint64_t w = w0 + u * stride;
             if (w >= nwords) break;
             out[w] = x[u];
@@ -311,8 +325,8 @@ int launch_bitmap_and_from(const BitmapList& inl, const uint64_t* const* d_bms, 
     uint64_t words = (rows + 63) / 64;
     if (!words) return kOk;
     int sms = sm_count() > 0 ? sm_count() : 148;
-    uint64_t blocks = (words + 255) / 256;
-    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
+    uint64_t blocks = (words + 1023) / 1024;  // 256 threads x 4 words per step
+    if (blocks > static_cast<uint64_t>(sms) * 4) blocks = static_cast<uint64_t>(sms) * 4;  // resident at 64 registers
     bitmap_and_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(inl, d_bms, nbm, rows, out, count);
     VX_CUDA(cudaGetLastError());
     return kOk;
