@@ -6,9 +6,9 @@
 //   RLEEncoding<T>::DecodeBatch (231-257): (value, run length) pairs expanded
 //     from row `offset`; rows past the last run decode to T{}.
 // Outputs are written once, coalesced; the packed words are read through L1
-// (neighbouring threads share words); the RLE decode scans the run lengths
-// into row starts (decoupled look-back) and each block expands the runs that
-// cover its row range from shared memory.
+// (neighbouring threads share words); the RLE decode scans each tile of run
+// lengths into row starts in shared memory (tile offsets by decoupled
+// look-back) and expands the tile's runs from there in the same pass.
 #include "decode.h"
 #include "voxel_c.h"
 #include "vx_common.cuh"
@@ -148,158 +148,159 @@ __global__ void __launch_bounds__(kDThreads) dict_gather_kernel(const T* __restr
     if (bad) atomicOr(err, 2);
 }
 
-// exclusive prefix of u32 run lengths -> u64 row starts (single pass)
-constexpr int kRunsPer = 16;  // runs per thread
-constexpr int kRunsPerTile = kDThreads * kRunsPer;
+// RLE decode in one pass.  A block takes tiles of kRleTileRuns runs in launch
+// order: it loads their lengths and values, scans the lengths into the tile's
+// local row starts (shared memory), gets the tile's first row from a
+// decoupled look-back over the tiles before it, and writes the tile's rows
+// that fall in [offset, offset + count).  Each warp expands steps of
+// kRleStepRows rows: it finds the run covering the step's first row by a
+// binary search over the local starts, marks the row where each later
+// non-empty run of the step begins (two non-empty runs never share a first
+// row), takes an inclusive max-scan over the marks (each row's run is the last
+// one begun at or before it) and stores the rows' values coalesced.  The tile
+// holding the last run writes 0 to the requested rows past the data.
+constexpr int kRleRunsPerThread = 8;
+constexpr int kRleTileRuns = kDThreads * kRleRunsPerThread;  // 2048 runs per tile
+constexpr int kRleStepRows = 256;                             // rows per warp step, 8 per lane
+constexpr int kRleWarps = kDThreads / 32;
+__device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + (j >> 3); }  // lanes 9 words apart
+// runs' starts and values: one pad word per 8 runs, so a thread's 8 runs and
+// its neighbour's sit 9 words apart (conflict-free stores)
+__device__ __forceinline__ int run_pad(int r) { return r + (r >> 3); }
+constexpr int kRlePadRuns = kRleTileRuns + kRleTileRuns / 8 + 1;
 
-__global__ void __launch_bounds__(kDThreads) run_starts_kernel(const uint32_t* __restrict__ runs, uint64_t nruns,
-                                                               uint64_t* __restrict__ starts,
+template <typename T>
+__global__ void __launch_bounds__(kDThreads, 4) rle_decode_kernel(const T* __restrict__ values,
+                                                               const uint32_t* __restrict__ runs, uint64_t nruns,
+                                                               uint64_t offset, uint64_t count, T* __restrict__ out,
                                                                unsigned long long* status, unsigned int* ctr,
                                                                int* err) {
+    __shared__ uint64_t s_start[kRlePadRuns];  // local first row of each run (run_pad); run kRleTileRuns: tile rows
+    __shared__ T s_val[kRlePadRuns];
+    __shared__ uint32_t s_mark[kRleWarps][kRleStepRows + kRleStepRows / 8];
+    __shared__ uint64_t s_warp[kRleWarps];
     __shared__ uint64_t s_tile, s_base;
-    __shared__ uint64_t s_warp[kDThreads / 32];
-    const uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t ntiles = (nruns + kRleTileRuns - 1) / kRleTileRuns;
+    const uint64_t end = offset + count;
+    uint32_t* const mark = s_mark[warp];
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
         __syncthreads();
-        uint64_t tile = s_tile;
+        const uint64_t tile = s_tile;
         if (tile >= ntiles) break;
-        uint64_t r0 = tile * kRunsPerTile + threadIdx.x * kRunsPer;
-        uint32_t v[kRunsPer];
-        uint64_t c = 0;
-        if (r0 + kRunsPer <= nruns && (reinterpret_cast<uintptr_t>(runs + r0) & 15) == 0) {
+        const uint64_t t0 = tile * kRleTileRuns;
+        const int nin = static_cast<int>(nruns - t0 < kRleTileRuns ? nruns - t0 : kRleTileRuns);
+        const uint64_t r0 = t0 + static_cast<uint64_t>(threadIdx.x) * kRleRunsPerThread;
+        uint32_t len[kRleRunsPerThread];
+        T val[kRleRunsPerThread];
+        if (r0 + kRleRunsPerThread <= nruns && ((reinterpret_cast<uintptr_t>(runs + r0) |
+                                                  reinterpret_cast<uintptr_t>(values + r0)) & 15) == 0) {
+            const uint4* lp = reinterpret_cast<const uint4*>(runs + r0);
+            const uint4 a = __ldcs(lp), b = __ldcs(lp + 1);
+            len[0] = a.x; len[1] = a.y; len[2] = a.z; len[3] = a.w;
+            len[4] = b.x; len[5] = b.y; len[6] = b.z; len[7] = b.w;
 #pragma unroll
-            for (int k = 0; k < kRunsPer; k += 4) {
-                const uint4 q = __ldcs(reinterpret_cast<const uint4*>(runs + r0 + k));
-                v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
-            }
+            for (int k = 0; k < kRleRunsPerThread; ++k) val[k] = __ldcs(values + r0 + k);
         } else {
 #pragma unroll
-            for (int k = 0; k < kRunsPer; ++k) v[k] = r0 + k < nruns ? runs[r0 + k] : 0;
+            for (int k = 0; k < kRleRunsPerThread; ++k) {
+                const bool in = r0 + k < nruns;
+                len[k] = in ? runs[r0 + k] : 0u;
+                val[k] = in ? values[r0 + k] : T(0);
+            }
         }
+        uint64_t c = 0;
 #pragma unroll
-        for (int k = 0; k < kRunsPer; ++k) c += v[k];
-        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int k = 0; k < kRleRunsPerThread; ++k) c += len[k];
         uint64_t inc = c;
+#pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
             if (lane >= d) inc += y;
         }
         if (lane == 31) s_warp[warp] = inc;
         __syncthreads();
         if (warp == 0) {
-            uint64_t x = lane < kDThreads / 32 ? s_warp[lane] : 0, t = x;
+            const uint64_t x = lane < kRleWarps ? s_warp[lane] : 0;
+            uint64_t t = x;
+#pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
-                uint64_t y = __shfl_up_sync(0xffffffffu, t, d);
+                const uint64_t y = __shfl_up_sync(0xffffffffu, t, d);
                 if (lane >= d) t += y;
             }
-            if (lane < kDThreads / 32) s_warp[lane] = t - x;
-            const uint64_t tile_total = __shfl_sync(0xffffffffu, t, 31);
-            const uint64_t e = lookback_exclusive_warp(status, tile, tile_total, err);
+            if (lane < kRleWarps) s_warp[lane] = t - x;
+            const uint64_t total = __shfl_sync(0xffffffffu, t, 31);
+            const uint64_t e = lookback_exclusive_warp(status, tile, total, err);
             if (lane == 0) s_base = e;
         }
         __syncthreads();
-        uint64_t pos = s_base + s_warp[warp] + (inc - c);
+        {
+            uint64_t st = s_warp[warp] + (inc - c);
 #pragma unroll
-        for (int k = 0; k < kRunsPer; ++k) {
-            if (r0 + k < nruns) starts[r0 + k] = pos;
-            pos += v[k];
-        }
-        if (r0 < nruns && r0 + kRunsPer >= nruns) starts[nruns] = pos;  // the thread holding the last run: total rows
-        __syncthreads();
-    }
-}
-
-// rows [offset, offset+count): block b expands rows [b*R, (b+1)*R) of the
-// output.  The block knows the run covering its first row, marks each later
-// run's first row in shared memory with its run index (and stages the runs'
-// values there), takes an inclusive max-scan over the R rows (each row's
-// covering run is the last run starting at or before it), and writes the
-// rows' values coalesced.
-constexpr int kRleRows = 2048;
-constexpr int kRlePer = kRleRows / kDThreads;  // rows per thread in the scan
-__device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + (j >> 5); }  // bank-conflict padding
-
-template <typename T>
-__global__ void __launch_bounds__(kDThreads) rle_expand_kernel(const T* __restrict__ values,
-                                                               const uint64_t* __restrict__ starts, uint64_t nruns,
-                                                               uint64_t offset, uint64_t count, T* __restrict__ out) {
-    __shared__ uint32_t s_idx[kRleRows + kRleRows / 32];
-    __shared__ T s_val[kRleRows];  // values of runs k0 .. k0 + kRleRows - 1
-    __shared__ uint32_t s_wmax[kDThreads / 32];
-    __shared__ uint64_t s_k0;
-    const uint64_t total = starts[nruns];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // each block expands a contiguous range of tiles: one binary search for
-    // its first tile, then the covering run of each next tile's first row is
-    // found by walking forward from the previous tile's last run
-    const uint64_t ntiles = (count + kRleRows - 1) / kRleRows;
-    const uint64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
-    const uint64_t tb = blockIdx.x * per, te = min(ntiles, tb + per);
-    if (threadIdx.x == 0 && tb < te) {
-        const uint64_t key = offset + tb * kRleRows;
-        uint64_t lo = 0, hi = nruns;
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (starts[mid] <= key) lo = mid + 1;
-            else hi = mid;
-        }
-        s_k0 = lo ? lo - 1 : 0;
-    }
-    for (uint64_t blk = tb; blk < te; ++blk) {
-        const uint64_t row0 = offset + blk * kRleRows;
-        const uint32_t nb = static_cast<uint32_t>(min(static_cast<uint64_t>(kRleRows), count - blk * kRleRows));
-#pragma unroll
-        for (int e = 0; e < kRlePer; ++e) s_idx[rle_pad(threadIdx.x + e * kDThreads)] = 0;
-        __syncthreads();
-        const uint64_t k0 = s_k0;
-        if (threadIdx.x == 0) s_val[0] = __ldg(values + k0);
-        // runs after k0 start after row0 (starts are non-decreasing); each
-        // thread stops at its first run past the tile
-        for (uint64_t k = k0 + 1 + threadIdx.x; k < nruns; k += kDThreads) {
-            const uint64_t st = __ldg(starts + k);
-            if (st - row0 >= nb) break;
-            const uint32_t rel = static_cast<uint32_t>(k - k0);
-            atomicMax(&s_idx[rle_pad(static_cast<uint32_t>(st - row0))], rel);
-            if (rel < kRleRows) s_val[rel] = __ldg(values + k);
-        }
-        __syncthreads();
-        // inclusive max-scan: each thread a segment of kRlePer rows, then warps, then the block
-        uint32_t loc[kRlePer], m = 0;
-#pragma unroll
-        for (int e = 0; e < kRlePer; ++e) {
-            m = max(m, s_idx[rle_pad(threadIdx.x * kRlePer + e)]);
-            loc[e] = m;
-        }
-        uint32_t inc = m;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc = max(inc, y);
-        }
-        if (lane == 31) s_wmax[warp] = inc;
-        __syncthreads();
-        uint32_t pre = __shfl_up_sync(0xffffffffu, inc, 1);
-        if (lane == 0) pre = 0;
-        for (int w = 0; w < warp; ++w) pre = max(pre, s_wmax[w]);
-#pragma unroll
-        for (int e = 0; e < kRlePer; ++e) s_idx[rle_pad(threadIdx.x * kRlePer + e)] = max(pre, loc[e]);
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < kRlePer; ++e) {
-            const uint32_t j = threadIdx.x + e * kDThreads;
-            if (j < nb) {
-                const uint32_t rel = s_idx[rle_pad(j)];
-                // more than kRleRows runs start in the tile only with empty runs
-                const T x = rel < kRleRows ? s_val[rel] : __ldg(values + k0 + rel);
-                out[blk * kRleRows + j] = row0 + j < total ? x : T(0);
+            for (int k = 0; k < kRleRunsPerThread; ++k) {
+                s_start[run_pad(threadIdx.x * kRleRunsPerThread + k)] = st;
+                s_val[run_pad(threadIdx.x * kRleRunsPerThread + k)] = val[k];
+                st += len[k];
             }
+            if (threadIdx.x == kDThreads - 1) s_start[run_pad(kRleTileRuns)] = st;  // runs past nruns are empty
         }
-        if (threadIdx.x == 0) {  // the next tile's first row: from the run covering this tile's last row
-            uint64_t k = k0 + s_idx[rle_pad(nb - 1)];
-            const uint64_t next = row0 + nb;
-            while (k + 1 < nruns && __ldg(starts + k + 1) <= next) ++k;
-            s_k0 = k;
+        __syncthreads();
+        const uint64_t base = s_base, trows = s_start[run_pad(kRleTileRuns)];
+        const uint64_t lo = base > offset ? base : offset;
+        const uint64_t hi = base + trows < end ? base + trows : end;
+        for (uint64_t cs = lo + static_cast<uint64_t>(warp) * kRleStepRows; cs < hi;
+             cs += static_cast<uint64_t>(kRleWarps) * kRleStepRows) {
+            const uint32_t nb = static_cast<uint32_t>(hi - cs < kRleStepRows ? hi - cs : kRleStepRows);
+            const uint64_t x0 = cs - base;  // the step's first row, local: below trows
+            // the last run beginning at or before x0 (non-empty: an empty run
+            // shares its first row with the run after it, or begins at trows)
+            int ka = 0, kb = nin;
+            while (kb - ka > 1) {
+                const int m = (ka + kb) >> 1;
+                if (s_start[run_pad(m)] <= x0) ka = m;
+                else kb = m;
+            }
+            const int k0 = ka;
+#pragma unroll
+            for (int e = 0; e < kRleStepRows / 32; ++e) mark[rle_pad(lane * (kRleStepRows / 32) + e)] = 0;
+            __syncwarp();
+            for (int k = k0 + 1 + lane; k < nin; k += 32) {
+                const uint64_t sk = s_start[run_pad(k)];
+                if (sk >= x0 + nb) break;  // starts are non-decreasing
+                if (s_start[run_pad(k + 1)] > sk)
+                    mark[rle_pad(static_cast<uint32_t>(sk - x0))] = static_cast<uint32_t>(k - k0);
+            }
+            __syncwarp();
+            uint32_t loc[kRleStepRows / 32], m = 0;
+#pragma unroll
+            for (int e = 0; e < kRleStepRows / 32; ++e) {
+                m = max(m, mark[rle_pad(lane * (kRleStepRows / 32) + e)]);
+                loc[e] = m;
+            }
+            uint32_t incl = m;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl = max(incl, y);
+            }
+            uint32_t pre = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) pre = 0;
+            __syncwarp();
+#pragma unroll
+            for (int e = 0; e < kRleStepRows / 32; ++e)
+                mark[rle_pad(lane * (kRleStepRows / 32) + e)] = max(pre, loc[e]);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < kRleStepRows / 32; ++i) {
+                const uint32_t j = lane + 32 * i;
+                if (j < nb) out[cs + j - offset] = s_val[run_pad(k0 + static_cast<int>(mark[rle_pad(j)]))];
+            }
+            __syncwarp();  // the marks are cleared for the next step
+        }
+        if (tile == ntiles - 1) {  // requested rows past the last run
+            const uint64_t past = base + trows > offset ? base + trows : offset;
+            for (uint64_t r = past + threadIdx.x; r < end; r += kDThreads) out[r - offset] = T(0);
         }
         __syncthreads();
     }
@@ -382,8 +383,8 @@ int launch_dict_gather(int dtype, const void* dict, uint32_t card, const uint32_
 }
 
 size_t rle_scratch_bytes(uint64_t nruns) {
-    uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
-    return (nruns + 1) * 8 + (ntiles + 1) * 8 + 64;
+    uint64_t ntiles = (nruns + kRleTileRuns - 1) / kRleTileRuns;
+    return (ntiles + 1) * 8 + 64;  // look-back statuses, then the tile counter
 }
 
 int launch_rle_decode_i64(const int64_t* values, const uint32_t* runs, uint64_t nruns, uint64_t offset,
@@ -393,19 +394,15 @@ int launch_rle_decode_i64(const int64_t* values, const uint32_t* runs, uint64_t 
         VX_CUDA(cudaMemsetAsync(out, 0, count * 8, s));
         return kOk;
     }
-    uint64_t ntiles = (nruns + kRunsPerTile - 1) / kRunsPerTile;
-    uint64_t* starts = static_cast<uint64_t*>(scratch);
-    unsigned long long* status = reinterpret_cast<unsigned long long*>(starts + nruns + 1);
+    const uint64_t ntiles = (nruns + kRleTileRuns - 1) / kRleTileRuns;
+    unsigned long long* status = static_cast<unsigned long long*>(scratch);
     unsigned int* ctr = reinterpret_cast<unsigned int*>(status + ntiles);
     VX_CUDA(cudaMemsetAsync(status, 0, (ntiles + 1) * 8, s));
-    int sms = sm_count() > 0 ? sm_count() : 148;
-    uint64_t b = ntiles < static_cast<uint64_t>(sms) * 4 ? ntiles : static_cast<uint64_t>(sms) * 4;
-    run_starts_kernel<<<static_cast<unsigned>(b), kDThreads, 0, s>>>(runs, nruns, starts, status, ctr, err);
-    VX_CUDA(cudaGetLastError());
-    uint64_t blocks = (count + kRleRows - 1) / kRleRows;
-    if (blocks > static_cast<uint64_t>(sms) * 8) blocks = static_cast<uint64_t>(sms) * 8;
-    rle_expand_kernel<int64_t><<<static_cast<unsigned>(blocks), kDThreads, 0, s>>>(values, starts, nruns, offset,
-                                                                                  count, out);
+    const int sms = sm_count() > 0 ? sm_count() : 148;
+    const uint64_t cap = static_cast<uint64_t>(sms) * 4;
+    const uint64_t blocks = ntiles < cap ? ntiles : cap;
+    rle_decode_kernel<int64_t><<<static_cast<unsigned>(blocks), kDThreads, 0, s>>>(values, runs, nruns, offset, count,
+                                                                                  out, status, ctr, err);
     VX_CUDA(cudaGetLastError());
     return kOk;
 }
