@@ -161,9 +161,10 @@ __global__ void __launch_bounds__(kDThreads) dict_gather_kernel(const T* __restr
 // holding the last run writes 0 to the requested rows past the data.
 constexpr int kRleRunsPerThread = 8;
 constexpr int kRleTileRuns = kDThreads * kRleRunsPerThread;  // 2048 runs per tile
-constexpr int kRleStepRows = 256;                             // rows per warp step, 8 per lane
+constexpr int kRleStepRows = 512;                             // rows per warp step, 16 per lane
 constexpr int kRleWarps = kDThreads / 32;
-__device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + (j >> 3); }  // lanes 9 words apart
+// 16-bit marks, two pad entries per 16: a lane's 16 marks sit 9 words after its neighbour's
+__device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + ((j >> 4) << 1); }
 // runs' starts and values: one pad word per 8 runs, so a thread's 8 runs and
 // its neighbour's sit 9 words apart (conflict-free stores)
 __device__ __forceinline__ int run_pad(int r) { return r + (r >> 3); }
@@ -177,13 +178,13 @@ __global__ void __launch_bounds__(kDThreads, 4) rle_decode_kernel(const T* __res
                                                                int* err) {
     __shared__ uint64_t s_start[kRlePadRuns];  // local first row of each run (run_pad); run kRleTileRuns: tile rows
     __shared__ T s_val[kRlePadRuns];
-    __shared__ uint32_t s_mark[kRleWarps][kRleStepRows + kRleStepRows / 8];
+    __shared__ uint16_t s_mark[kRleWarps][kRleStepRows + kRleStepRows / 8];  // run index - k0 (< 2^11)
     __shared__ uint64_t s_warp[kRleWarps];
     __shared__ uint64_t s_tile, s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t ntiles = (nruns + kRleTileRuns - 1) / kRleTileRuns;
     const uint64_t end = offset + count;
-    uint32_t* const mark = s_mark[warp];
+    uint16_t* const mark = s_mark[warp];
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
         __syncthreads();
@@ -269,13 +270,13 @@ __global__ void __launch_bounds__(kDThreads, 4) rle_decode_kernel(const T* __res
                 const uint64_t sk = s_start[run_pad(k)];
                 if (sk >= x0 + nb) break;  // starts are non-decreasing
                 if (s_start[run_pad(k + 1)] > sk)
-                    mark[rle_pad(static_cast<uint32_t>(sk - x0))] = static_cast<uint32_t>(k - k0);
+                    mark[rle_pad(static_cast<uint32_t>(sk - x0))] = static_cast<uint16_t>(k - k0);
             }
             __syncwarp();
             uint32_t loc[kRleStepRows / 32], m = 0;
 #pragma unroll
             for (int e = 0; e < kRleStepRows / 32; ++e) {
-                m = max(m, mark[rle_pad(lane * (kRleStepRows / 32) + e)]);
+                m = max(m, static_cast<uint32_t>(mark[rle_pad(lane * (kRleStepRows / 32) + e)]));
                 loc[e] = m;
             }
             uint32_t incl = m;
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(kDThreads, 4) rle_decode_kernel(const T* __res
             __syncwarp();
 #pragma unroll
             for (int e = 0; e < kRleStepRows / 32; ++e)
-                mark[rle_pad(lane * (kRleStepRows / 32) + e)] = max(pre, loc[e]);
+                mark[rle_pad(lane * (kRleStepRows / 32) + e)] = static_cast<uint16_t>(max(pre, loc[e]));
             __syncwarp();
 #pragma unroll
             for (int i = 0; i < kRleStepRows / 32; ++i) {
