@@ -1287,8 +1287,10 @@ __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
 #pragma unroll
             for (int k = 0; k < kWords - 1; ++k)
                 if (const uint32_t w = s_w[kWords * i + k]) atomicAdd(&e[k], static_cast<unsigned long long>(w));
-            if (const uint32_t w = s_w[kWords * i + kWords - 1])
-                atomicAdd(&e[kWords - 1], static_cast<unsigned long long>(static_cast<long long>(static_cast<int32_t>(w))));
+            if (const uint32_t w = s_w[kWords * i + kWords - 1]) {
+                const long long top = static_cast<int32_t>(w);  // the sign word
+                atomicAdd(&e[kWords - 1], static_cast<unsigned long long>(top));
+            }
             atomicAdd(&e[5], static_cast<unsigned long long>(c));
             atomicMin(&e[6], s_mn[i]);
             atomicMax(&e[7], s_mx[i]);
@@ -1363,11 +1365,9 @@ __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
             if (a2) atomicAdd(&eb[w.k0 + 2], neg ? 0ull - a2 : a2);
         }
         atomicAdd(&eb[5], 1ull);
-        // screen MIN / MAX with one read of both keys: a stale read only costs
-        // an atomic that changes nothing
-        const ulonglong2 mm = __ldcg(reinterpret_cast<const ulonglong2*>(eb + 6));
-        if (key < mm.x) atomicMin(&eb[6], key);
-        if (key > mm.y) atomicMax(&eb[7], key);
+        // MIN / MAX as reductions too: no read of the current keys to wait on
+        atomicMin(&eb[6], key);
+        atomicMax(&eb[7], key);
     };
 
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
