@@ -307,9 +307,10 @@ int       voxel_dict_decode_dev(int dtype, const void* d_dict, size_t card, cons
  * Additive: fused scan + group-by (decode key, two predicates, group SUM of a
  * product, COUNT, MIN, MAX).  Groups come out sorted by key; returns the
  * group count or (size_t)-1.  Dictionaries of up to 4,096 entries aggregate
- * in shared-memory tables; larger ones (up to 2^26 entries) add straight into
- * the HBM table with atomics and compact the groups with a second kernel
- * (the same exact integers: identical results).
+ * in shared-memory tables; larger ones (up to 2^26 entries) keep their
+ * frequent groups in per-block shared-memory slot caches, send the other rows
+ * to an HBM table with reductions, and compact the groups with a second
+ * kernel (the same exact integers: identical results).
  *   key = dict[unpack(packed_key)], WHERE price > price_gt AND
  *   qty BETWEEN qty_lo AND qty_hi, GROUP BY key:
  *   SUM(price*qty) (one rounded multiply), COUNT(*), MIN(price), MAX(price)
@@ -340,8 +341,8 @@ size_t    voxel_scan_groupby(const uint64_t* packed_key, size_t nwords, uint32_t
  * All but 0 give bit-identical results; the autotuner also times 7.
  * voxel_scan_groupby_last_variant reports the kernel the last call ran: 0
  * warp-merged, 1 TMA-fed, 2 word table with queue, 3 word table direct, 4
- * word table fed by bulk copies, 5 lean word table, 6 the HBM table of
- * dictionaries above 4096 entries, 7 the prefetching word table. */
+ * word table fed by bulk copies, 5 lean word table, 6 the slot caches and
+ * HBM table of dictionaries above 4096 entries, 7 the prefetching word table. */
 int       voxel_scan_groupby_tune(int variant);
 int       voxel_scan_groupby_last_variant(void);
 /* the calling thread's current variant id (as passed to voxel_scan_groupby_tune) */
