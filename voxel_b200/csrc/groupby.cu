@@ -1236,9 +1236,9 @@ __global__ void __launch_bounds__(kGbThreads, 3) scan_groupby_lean_kernel(
 // frequent groups of a skewed column settle in every block's cache.  Rows whose
 // group finds no slot go to the HBM table: per group five signed 64-bit limbs
 // (limb k weighs 2^(32k) units of 2^-76), the count and the MIN / MAX order
-// keys.  Every addition to the HBM table is a reduction whose result is never
-// read (no carry crosses a limb; each added piece is below 2^32), so no thread
-// waits on an HBM atomic.  A scan kernel covers at most kSpillChunk rows; the
+// keys.  Every update of the HBM table (sums, count, min, max) is a reduction
+// whose result is never read (no carry crosses a limb; each added piece is
+// below 2^32), so no thread waits on an HBM atomic.  A scan kernel covers at most kSpillChunk rows; the
 // limbs are normalised between chunks, which keeps each below 2^61.  A
 // separate kernel then compacts the non-empty groups in key order (tiles of
 // groups claimed in launch order, output offsets by decoupled look-back) and
