@@ -1254,7 +1254,9 @@ constexpr int kSpillMaxLog2 = 11;
 // shared memory of the slot cache: min, max keys, five words, count, tag per slot
 size_t spill_smem_bytes(int slots_log2) { return (static_cast<size_t>(1) << slots_log2) * 44; }
 
-template <int RPT, int MINB>
+// B32: queue entries hold the row's 32-bit bit offset in the packed column
+// (rows x width < 2^32), else its 64-bit index
+template <int RPT, int MINB, bool B32>
 __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
     const uint64_t* __restrict__ packed, uint32_t width, uint32_t card, const double* __restrict__ price,
     const int32_t* __restrict__ qty, uint64_t row0, uint64_t n, double pthr, int32_t qlo, int32_t qhi,
@@ -1307,12 +1309,15 @@ __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
     bool bad_value = false, bad_key = false;
     uint64_t since_flush = 0;
 
-    __shared__ WarpQueue<false> s_queue[kGbThreads / 32];
+    __shared__ WarpQueue<B32> s_queue[kGbThreads / 32];
     const int lane = threadIdx.x & 31;
     const unsigned lanemask_lt = (1u << lane) - 1;
-    WarpQueue<false>& Q = s_queue[threadIdx.x >> 5];
+    WarpQueue<B32>& Q = s_queue[threadIdx.x >> 5];
     int qn = 0, qh = 0;
     volatile uint32_t* const v_tag = s_tag;
+    const uint32_t* const p32 = reinterpret_cast<const uint32_t*>(packed);
+    const uint32_t nw32 = B32 ? static_cast<uint32_t>(((row0 + n) * width + 63) / 64 * 2) : 0u;
+    const uint32_t mask32 = static_cast<uint32_t>(mask);
 
     auto consume = [&](int cnt) {
         const bool valid = lane < cnt;
@@ -1322,7 +1327,9 @@ __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
         // one warp-uniform test picks the add-only path of the slot words
         const bool mayneg = __any_sync(0xffffffffu, v < 0.0);
         if (!valid) return;
-        const uint32_t gi = key_bits(packed, Q.pos[e], width, mask);
+        uint32_t gi;
+        if constexpr (B32) gi = key_bits32(p32, Q.pos[e], nw32, mask32);
+        else gi = key_bits(packed, Q.pos[e], width, mask);
         if (gi >= card) {
             bad_key = true;
             return;
@@ -1412,7 +1419,8 @@ __global__ void __launch_bounds__(kGbThreads, MINB) scan_groupby_spill_kernel(
             const unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
                 const int pos = (qh + qn + __popc(m & lanemask_lt)) & (kQueue - 1);
-                Q.pos[pos] = r0 + k;
+                if constexpr (B32) Q.pos[pos] = static_cast<uint32_t>((r0 + k) * width);  // < 2^32 by the launch check
+                else Q.pos[pos] = r0 + k;
                 Q.price[pos] = p;
                 Q.qty[pos] = q;
             }
@@ -1734,15 +1742,25 @@ int launch_spill(ScanGroupBy& S, int slots_log2, const uint64_t* packed, uint32_
     unsigned long long* const hbm = S.g_limb;
     int* const status = static_cast<int*>(S.status.p);
     const size_t smem = spill_smem_bytes(slots_log2);
-    // the smaller cache leaves room for a third block per SM: registers capped to match
-    auto* const kern =
-        slots_log2 < kSpillMaxLog2 ? scan_groupby_spill_kernel<kRpt, 3> : scan_groupby_spill_kernel<kRpt, 2>;
+    // the smaller cache leaves room for a third block per SM: registers capped
+    // to match; 32-bit bit offsets in the queue when rows x width < 2^32
+    const bool b32 = n * static_cast<uint64_t>(width) < (1ull << 32);
+    const bool small = slots_log2 < kSpillMaxLog2;
+    auto* const kern = small ? (b32 ? scan_groupby_spill_kernel<kRpt, 3, true>
+                                    : scan_groupby_spill_kernel<kRpt, 3, false>)
+                             : (b32 ? scan_groupby_spill_kernel<kRpt, 2, true>
+                                    : scan_groupby_spill_kernel<kRpt, 2, false>);
     static thread_local bool attr_set = false;
     if (!attr_set) {
-        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(spill_smem_bytes(kSpillMaxLog2))));
-        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(spill_smem_bytes(kSpillMaxLog2))));
+        const int bytes = static_cast<int>(spill_smem_bytes(kSpillMaxLog2));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 2, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 3, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 2, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VX_CUDA(cudaFuncSetAttribute(scan_groupby_spill_kernel<kRpt, 3, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr_set = true;
     }
     int per_sm = 0;
