@@ -165,8 +165,8 @@ constexpr int kRleStepRows = 512;                             // rows per warp s
 constexpr int kRleWarps = kDThreads / 32;
 // 16-bit marks, two pad entries per 16: a lane's 16 marks sit 9 words after its neighbour's
 __device__ __forceinline__ uint32_t rle_pad(uint32_t j) { return j + ((j >> 4) << 1); }
-// runs' starts and values: one pad word per 8 runs, so a thread's 8 runs and
-// its neighbour's sit 9 words apart (conflict-free stores)
+// runs' starts and values: one pad entry per 8 runs, so a thread's 8 runs and
+// its neighbour's sit 9 entries apart (conflict-free stores)
 __device__ __forceinline__ int run_pad(int r) { return r + (r >> 3); }
 constexpr int kRlePadRuns = kRleTileRuns + kRleTileRuns / 8 + 1;
 
